@@ -1,0 +1,265 @@
+/*
+ * stophys_b200.h — C ABI of the B200 ensemble SDE engine.
+ *
+ * The engine replaces the reference's per-particle simulation loop for a whole
+ * ensemble.  In the reference every particle gets its own
+ * SingleParticleSimulator<Solver,Field>, created and run by
+ * SimulationManager::singleSimulationTask
+ *   (Particle_Simulation/Simulator/SimulationManager.h:126-160)
+ * which calls doSimulation -> startSimulation
+ *   (Particle_Simulation/Simulator/SingleParticleSimulator.h:109-159,221-227)
+ * and folds each particle's window-mean trajectory into the moment-weighted
+ * ensemble mean (Particle_Simulation/Results/MeanSimulationResult.h:87-119).
+ * The reference's binary plug-in point is the per-ISA shared library exporting
+ * SimulationManager<PREC,ISA> (Particle_Simulation/app/StoPhys_arch.cpp.in:4,
+ * selected in Particle_Simulation/app/StoPhysApp_MultiArch.cpp:27-75); this ABI
+ * is the B200 backend a maintainer registers beside AVX/AVX2/AVX512.
+ *
+ * Conventions
+ *  - Every call returns sp_status; no C++ exception crosses the ABI.  The text
+ *    of the last error on the calling thread is returned by sp_last_error().
+ *  - All arrays passed in are HOST pointers owned by the caller.  The library
+ *    copies what it needs to the device and owns all device memory.
+ *  - Units and signs follow the reference's .ini contract: SI units, fields in
+ *    tesla, gyromagnetic ratio positive for the electron, and the reference's
+ *    anisotropy sign (uniaxial H = (-2K/Ms)(m.n)n, so K < 0 is an easy axis).
+ */
+#ifndef STOPHYS_B200_H
+#define STOPHYS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SP_ABI_VERSION 1u
+
+typedef enum sp_status {
+    SP_OK = 0,
+    SP_ERR_INVALID_ARG = 1,       /* malformed or out-of-range description */
+    SP_ERR_UNSUPPORTED_COMBO = 2, /* e.g. ImplicitMidpoint on a problem without Jacobian */
+    SP_ERR_OUT_OF_MEMORY = 3,
+    SP_ERR_ADMISSION_REFUSED = 4, /* request larger than the server's memory budget */
+    SP_ERR_DEVICE_TIMEOUT = 5,
+    SP_ERR_NUMERIC_FAULT = 6,     /* non-finite state detected (see sp_stats) */
+    SP_ERR_CUDA = 7,
+    SP_ERR_NOT_READY = 8,
+    SP_ERR_NOT_FOUND = 9,
+    SP_ERR_CANCELLED = 10,
+    SP_ERR_NO_DEVICE = 11
+} sp_status;
+
+/* Problems the reference registers (Particle_Simulation/Problems/Problems.h:6-9,
+ * enum IProblem in Particle_Simulation/Settings/ProblemSettings.h). */
+typedef enum sp_problem {
+    SP_PROBLEM_NEEL = 0,                          /* NeelRelaxation: m in R^3         */
+    SP_PROBLEM_NEEL_SPHERICAL = 1,                /* NeelRelaxationSpherical: (theta, phi) */
+    SP_PROBLEM_BROWN_AND_NEEL_EULER_SPHERICAL = 2,/* Euler ZXZ (phi,theta,psi) + Neel (theta,phi) */
+    SP_PROBLEM_BROWN_AND_NEEL = 3                 /* BrownAndNeelRelaxation: (n, m) in R^6 */
+} sp_problem;
+
+/* Particle_Simulation/Problems/Anisotropy/AnisotropyList.h:45 */
+typedef enum sp_anisotropy {
+    SP_ANISOTROPY_UNIAXIAL = 0,
+    SP_ANISOTROPY_CUBIC = 1
+} sp_anisotropy;
+
+/* Particle_Simulation/Fields/FieldList.h:48 */
+typedef enum sp_field_type {
+    SP_FIELD_ZERO = 0,
+    SP_FIELD_CONSTANT = 1,
+    SP_FIELD_SINUSOIDAL = 2,
+    SP_FIELD_LISSAJOUS = 3
+} sp_field_type;
+
+/* Particle_Simulation/Settings/SolverSettings.h:39 (ISolver) */
+typedef enum sp_solver {
+    SP_SOLVER_EULER_MARUYAMA = 0,
+    SP_SOLVER_HEUN_STRONG = 1,
+    SP_SOLVER_MILLSTEIN = 2,
+    SP_SOLVER_IMPLICIT_MIDPOINT = 3
+} sp_solver;
+
+typedef enum sp_precision {
+    SP_PRECISION_FP64 = 0, /* plain drop-in: FP64 throughout                         */
+    SP_PRECISION_FP32 = 1  /* FP32 stepping; FP64 time, field phase, ensemble sums,
+                              Newton acceptance test                                 */
+} sp_precision;
+
+typedef enum sp_noise {
+    SP_NOISE_PHILOX = 0,   /* counter-based Philox4x32-10 + Box-Muller, in-kernel    */
+    SP_NOISE_INJECTED = 1  /* Wiener increments supplied by the caller (parity mode) */
+} sp_noise;
+
+/* Per-particle physical properties, host structure-of-arrays of length
+ * n_particles each.  Keys mirror Magnetic_Properties / Hydrodynamic_Properties
+ * (Particle_Simulation/Properties/MagneticProperties.h:207-216,
+ *  Particle_Simulation/Properties/HydrodynamicProperties.h:52-56) and the
+ * initialisation settings (Particle_Simulation/Settings/ParticleSimulationInitSettings.h:30-38)
+ * with Use_random_initial_* = false: orientation and magnetisation are given. */
+typedef struct sp_particles {
+    const double* magnetic_radius;          /* m                                  */
+    const double* saturation_magnetisation; /* A/m                                */
+    const double* damping_constant;         /* alpha                              */
+    const double* gyromagnetic_ratio;       /* rad/(s T)                          */
+    const double* anisotropy_constant;      /* K_uniaxial or K1_cubic, J/m^3      */
+    const double* hydrodynamic_radius;      /* m; Brown problems only (else NULL) */
+    const double* viscosity;                /* Pa s; Brown problems only          */
+    const double* orientation;              /* [n][3] Euler angles phi,theta,psi (ZXZ) */
+    const double* magnetisation;            /* [n][3] initial magnetisation direction  */
+} sp_particles;
+
+/* External field B(t) in tesla.
+ *   ZERO:       B = 0
+ *   CONSTANT:   B = offset                                  (ConstantField.h:43)
+ *   SINUSOIDAL: B = amplitude*sin(2 pi frequency[0] t + phase[0]) + offset
+ *                                                           (SinusoidalField.h:47-51)
+ *   LISSAJOUS:  B_i = offset_i + amplitude_i*sin(2 pi frequency_i t + phase_i)
+ *                                                           (LissajousField.h:98-101) */
+typedef struct sp_field_desc {
+    int32_t type; /* sp_field_type */
+    int32_t reserved;
+    double offset[3];
+    double amplitude[3];
+    double frequency[3];
+    double phase[3];
+} sp_field_desc;
+
+/* Problem_Settings (Particle_Simulation/Settings/ProblemSettings.h:119-206). */
+typedef struct sp_problem_settings {
+    int32_t use_coordinate_transformation;            /* NeelSpherical             */
+    int32_t use_euler_coordinate_transformation;      /* BrownAndNeelEulerSpherical */
+    int32_t use_spherical_coordinate_transformation;  /* BrownAndNeelEulerSpherical */
+    int32_t use_simple_model;                         /* BrownAndNeel (Cartesian)   */
+    double min_angle_before_transformation;           /* rad                        */
+    double brown_min_angle_before_transformation;     /* rad                        */
+    double neel_min_angle_before_transformation;      /* rad                        */
+} sp_problem_settings;
+
+typedef struct sp_ensemble_desc {
+    uint32_t abi_version; /* SP_ABI_VERSION */
+    int32_t problem;      /* sp_problem     */
+    int32_t anisotropy;   /* sp_anisotropy  */
+    int32_t solver;       /* sp_solver      */
+    int32_t precision;    /* sp_precision   */
+    int32_t noise;        /* sp_noise       */
+    sp_problem_settings problem_settings;
+    int32_t max_iteration;       /* Solver_Settings Max_Iterations (ImplicitMidpoint) */
+    int32_t reserved0;
+    double accuracy_goal;        /* Solver_Settings Accuracy_Goal (ImplicitMidpoint)  */
+    uint64_t number_of_steps;    /* Simulation_Settings Number_of_steps               */
+    uint64_t oversampling;       /* Simulation_Settings OverSampling (window W)       */
+    double timestep;             /* Simulation_Settings Timestep (s)                  */
+    double temperature;          /* K                                                 */
+    sp_field_desc field;
+    uint64_t n_particles;
+    sp_particles particles;
+    uint64_t seed;               /* Philox key                                        */
+    uint64_t particle_id_offset; /* global id of particle 0 (shards keep one stream)  */
+    /* SP_NOISE_INJECTED only: Wiener increments dW (already scaled by sqrt(dt)),
+     * layout [integrated_steps][noise_dim][n_particles] with
+     * integrated_steps = (number_of_steps/oversampling - 1) * oversampling. */
+    const double* injected_dw;
+} sp_ensemble_desc;
+
+/* Outputs.  n_samples = number_of_steps / oversampling (SingleParticleSimulator.h:125);
+ * sample 0 is the initial state, sample k>=1 the Kahan mean over window k.
+ * Any pointer may be NULL to skip that output. */
+typedef struct sp_result {
+    double* mean;         /* [n_samples][out_dim] moment-weighted ensemble mean           */
+    double* weight;       /* [out_dim] summed weights (Ms*V per component)                */
+    double* time;         /* [n_samples] window-centre times (SingleParticleSimulator.h:236-273) */
+    double* field;        /* [n_samples][3] window-mean field                             */
+    double* trajectories; /* [n_particles][n_samples][out_dim] per-particle window means  */
+    double* final_state;  /* [n_particles][state_dim] state after the last step           */
+} sp_result;
+
+typedef struct sp_stats {
+    uint64_t particle_steps;      /* integrated particle-steps                       */
+    uint64_t nonfinite_particles; /* particles whose state became NaN/Inf            */
+    uint64_t newton_iterations;   /* ImplicitMidpoint: total Newton iterations       */
+    uint64_t newton_unconverged;  /* ImplicitMidpoint: steps that hit Max_Iterations */
+    uint64_t kernel_launches;     /* device kernels launched for this ensemble       */
+    double device_ms;             /* device time of the stepping kernels             */
+} sp_stats;
+
+typedef struct sp_context sp_context;
+typedef struct sp_ensemble sp_ensemble;
+typedef struct sp_server sp_server;
+
+/* ---- metadata --------------------------------------------------------- */
+const char* sp_last_error(void);
+uint32_t sp_abi_version(void);
+/* State / noise / output dimensions of a problem (GeneralSDEDimension of each
+ * problem: NeelRelaxation.h:24-25, NeelRelaxationSpherical.h:29-30,
+ * BrownAndNeelRelaxationEulerSpherical.h:36-37, BrownAndNeelRelaxation.h:68-69). */
+sp_status sp_query_dims(int32_t problem, int32_t* state_dim, int32_t* noise_dim, int32_t* out_dim);
+/* Validates a description without touching the device. */
+sp_status sp_validate(const sp_ensemble_desc* desc);
+/* Total kernels this process launched through the library. */
+uint64_t sp_kernel_launch_count(void);
+
+/* ---- context ----------------------------------------------------------- */
+sp_status sp_create(sp_context** ctx, int32_t device);
+sp_status sp_destroy(sp_context* ctx);
+
+/* ---- synchronous drop-in ----------------------------------------------
+ * Runs the whole ensemble: replaces SimulationManager::StartSimulationManager's
+ * fan-out of singleSimulationTask over all particles
+ * (Particle_Simulation/Simulator/SimulationManager.h:549-574) and the
+ * MeanSimulationResult accumulation.  Host in, host out. */
+sp_status sp_simulate(sp_context* ctx, const sp_ensemble_desc* desc, sp_result* out, sp_stats* stats);
+
+/* ---- device-resident ensembles ----------------------------------------
+ * sp_ensemble_create copies inputs to the device and builds the initial
+ * state; sp_ensemble_advance integrates further steps (in chunks, on the
+ * given CUDA stream, NULL = the context's stream); sp_ensemble_read waits and
+ * copies results out.  State stays on the device between calls. */
+sp_status sp_ensemble_create(sp_context* ctx, const sp_ensemble_desc* desc, sp_ensemble** ens);
+sp_status sp_ensemble_advance(sp_ensemble* ens, uint64_t n_steps, void* cuda_stream);
+sp_status sp_ensemble_steps_done(const sp_ensemble* ens, uint64_t* steps_done, uint64_t* steps_total);
+sp_status sp_ensemble_read(sp_ensemble* ens, sp_result* out, sp_stats* stats);
+sp_status sp_ensemble_destroy(sp_ensemble* ens);
+/* Bytes of device memory an ensemble of this description holds. */
+sp_status sp_ensemble_footprint(const sp_ensemble_desc* desc, uint64_t* bytes);
+
+/* ---- continuous-batching server ----------------------------------------- */
+typedef struct sp_server_config {
+    uint64_t memory_budget_bytes; /* admission limit on device bytes of admitted requests */
+    uint64_t chunk_steps;         /* steps per scheduling chunk (0 = autotuned default)   */
+    int32_t max_active;           /* cap on concurrently admitted requests (0 = none)     */
+    int32_t reserved;
+} sp_server_config;
+
+typedef enum sp_request_state {
+    SP_REQUEST_QUEUED = 0,
+    SP_REQUEST_RUNNING = 1,
+    SP_REQUEST_DONE = 2,
+    SP_REQUEST_FAILED = 3,
+    SP_REQUEST_CANCELLED = 4
+} sp_request_state;
+
+sp_status sp_server_create(sp_context* ctx, const sp_server_config* cfg, sp_server** srv);
+/* The description (and every array it points to) is copied at submit. */
+sp_status sp_server_submit(sp_server* srv, const sp_ensemble_desc* desc, uint64_t* request_id);
+sp_status sp_server_poll(sp_server* srv, uint64_t request_id, int32_t* state);
+/* Blocks up to timeout_ms (<0: forever) and copies results of a finished request. */
+sp_status sp_server_wait(sp_server* srv, uint64_t request_id, double timeout_ms, sp_result* out,
+                         sp_stats* stats, double* latency_ms);
+sp_status sp_server_cancel(sp_server* srv, uint64_t request_id);
+sp_status sp_server_destroy(sp_server* srv);
+
+/* ---- test hooks ------------------------------------------------------------
+ * Writes the unit normals the kernels draw for particles
+ * [particle_id, particle_id+n) and steps [step0, step0+n_steps) into
+ * out[n_steps][noise_dim][n] (FP64 values; FP32 draws are widened). */
+sp_status sp_debug_philox_normals(sp_context* ctx, uint64_t seed, uint64_t particle_id, uint64_t n,
+                                  uint64_t step0, uint64_t n_steps, int32_t noise_dim,
+                                  int32_t precision, double* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* STOPHYS_B200_H */
