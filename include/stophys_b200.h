@@ -36,6 +36,12 @@ extern "C" {
 
 #define SP_ABI_VERSION 1u
 
+#if defined(_WIN32)
+#define SP_API __declspec(dllexport)
+#else
+#define SP_API __attribute__((visibility("default")))
+#endif
+
 typedef enum sp_status {
     SP_OK = 0,
     SP_ERR_INVALID_ARG = 1,       /* malformed or out-of-range description */
@@ -147,7 +153,8 @@ typedef struct sp_ensemble_desc {
     int32_t noise;        /* sp_noise       */
     sp_problem_settings problem_settings;
     int32_t max_iteration;       /* Solver_Settings Max_Iterations (ImplicitMidpoint) */
-    int32_t reserved0;
+    int32_t record_trajectories; /* keep per-particle window means on the device (parity
+                                    runs; the reference's per-particle result vectors) */
     double accuracy_goal;        /* Solver_Settings Accuracy_Goal (ImplicitMidpoint)  */
     uint64_t number_of_steps;    /* Simulation_Settings Number_of_steps               */
     uint64_t oversampling;       /* Simulation_Settings OverSampling (window W)       */
@@ -190,40 +197,40 @@ typedef struct sp_ensemble sp_ensemble;
 typedef struct sp_server sp_server;
 
 /* ---- metadata --------------------------------------------------------- */
-const char* sp_last_error(void);
-uint32_t sp_abi_version(void);
+SP_API const char* sp_last_error(void);
+SP_API uint32_t sp_abi_version(void);
 /* State / noise / output dimensions of a problem (GeneralSDEDimension of each
  * problem: NeelRelaxation.h:24-25, NeelRelaxationSpherical.h:29-30,
  * BrownAndNeelRelaxationEulerSpherical.h:36-37, BrownAndNeelRelaxation.h:68-69). */
-sp_status sp_query_dims(int32_t problem, int32_t* state_dim, int32_t* noise_dim, int32_t* out_dim);
+SP_API sp_status sp_query_dims(int32_t problem, int32_t* state_dim, int32_t* noise_dim, int32_t* out_dim);
 /* Validates a description without touching the device. */
-sp_status sp_validate(const sp_ensemble_desc* desc);
+SP_API sp_status sp_validate(const sp_ensemble_desc* desc);
 /* Total kernels this process launched through the library. */
-uint64_t sp_kernel_launch_count(void);
+SP_API uint64_t sp_kernel_launch_count(void);
 
 /* ---- context ----------------------------------------------------------- */
-sp_status sp_create(sp_context** ctx, int32_t device);
-sp_status sp_destroy(sp_context* ctx);
+SP_API sp_status sp_create(sp_context** ctx, int32_t device);
+SP_API sp_status sp_destroy(sp_context* ctx);
 
 /* ---- synchronous drop-in ----------------------------------------------
  * Runs the whole ensemble: replaces SimulationManager::StartSimulationManager's
  * fan-out of singleSimulationTask over all particles
  * (Particle_Simulation/Simulator/SimulationManager.h:549-574) and the
  * MeanSimulationResult accumulation.  Host in, host out. */
-sp_status sp_simulate(sp_context* ctx, const sp_ensemble_desc* desc, sp_result* out, sp_stats* stats);
+SP_API sp_status sp_simulate(sp_context* ctx, const sp_ensemble_desc* desc, sp_result* out, sp_stats* stats);
 
 /* ---- device-resident ensembles ----------------------------------------
  * sp_ensemble_create copies inputs to the device and builds the initial
  * state; sp_ensemble_advance integrates further steps (in chunks, on the
  * given CUDA stream, NULL = the context's stream); sp_ensemble_read waits and
  * copies results out.  State stays on the device between calls. */
-sp_status sp_ensemble_create(sp_context* ctx, const sp_ensemble_desc* desc, sp_ensemble** ens);
-sp_status sp_ensemble_advance(sp_ensemble* ens, uint64_t n_steps, void* cuda_stream);
-sp_status sp_ensemble_steps_done(const sp_ensemble* ens, uint64_t* steps_done, uint64_t* steps_total);
-sp_status sp_ensemble_read(sp_ensemble* ens, sp_result* out, sp_stats* stats);
-sp_status sp_ensemble_destroy(sp_ensemble* ens);
+SP_API sp_status sp_ensemble_create(sp_context* ctx, const sp_ensemble_desc* desc, sp_ensemble** ens);
+SP_API sp_status sp_ensemble_advance(sp_ensemble* ens, uint64_t n_steps, void* cuda_stream);
+SP_API sp_status sp_ensemble_steps_done(const sp_ensemble* ens, uint64_t* steps_done, uint64_t* steps_total);
+SP_API sp_status sp_ensemble_read(sp_ensemble* ens, sp_result* out, sp_stats* stats);
+SP_API sp_status sp_ensemble_destroy(sp_ensemble* ens);
 /* Bytes of device memory an ensemble of this description holds. */
-sp_status sp_ensemble_footprint(const sp_ensemble_desc* desc, uint64_t* bytes);
+SP_API sp_status sp_ensemble_footprint(const sp_ensemble_desc* desc, uint64_t* bytes);
 
 /* ---- continuous-batching server ----------------------------------------- */
 typedef struct sp_server_config {
@@ -241,21 +248,21 @@ typedef enum sp_request_state {
     SP_REQUEST_CANCELLED = 4
 } sp_request_state;
 
-sp_status sp_server_create(sp_context* ctx, const sp_server_config* cfg, sp_server** srv);
+SP_API sp_status sp_server_create(sp_context* ctx, const sp_server_config* cfg, sp_server** srv);
 /* The description (and every array it points to) is copied at submit. */
-sp_status sp_server_submit(sp_server* srv, const sp_ensemble_desc* desc, uint64_t* request_id);
-sp_status sp_server_poll(sp_server* srv, uint64_t request_id, int32_t* state);
+SP_API sp_status sp_server_submit(sp_server* srv, const sp_ensemble_desc* desc, uint64_t* request_id);
+SP_API sp_status sp_server_poll(sp_server* srv, uint64_t request_id, int32_t* state);
 /* Blocks up to timeout_ms (<0: forever) and copies results of a finished request. */
-sp_status sp_server_wait(sp_server* srv, uint64_t request_id, double timeout_ms, sp_result* out,
+SP_API sp_status sp_server_wait(sp_server* srv, uint64_t request_id, double timeout_ms, sp_result* out,
                          sp_stats* stats, double* latency_ms);
-sp_status sp_server_cancel(sp_server* srv, uint64_t request_id);
-sp_status sp_server_destroy(sp_server* srv);
+SP_API sp_status sp_server_cancel(sp_server* srv, uint64_t request_id);
+SP_API sp_status sp_server_destroy(sp_server* srv);
 
 /* ---- test hooks ------------------------------------------------------------
  * Writes the unit normals the kernels draw for particles
  * [particle_id, particle_id+n) and steps [step0, step0+n_steps) into
  * out[n_steps][noise_dim][n] (FP64 values; FP32 draws are widened). */
-sp_status sp_debug_philox_normals(sp_context* ctx, uint64_t seed, uint64_t particle_id, uint64_t n,
+SP_API sp_status sp_debug_philox_normals(sp_context* ctx, uint64_t seed, uint64_t particle_id, uint64_t n,
                                   uint64_t step0, uint64_t n_steps, int32_t noise_dim,
                                   int32_t precision, double* out);
 

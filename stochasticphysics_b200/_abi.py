@@ -134,7 +134,7 @@ class sp_ensemble_desc(C.Structure):
         ("noise", C.c_int32),
         ("problem_settings", sp_problem_settings),
         ("max_iteration", C.c_int32),
-        ("reserved0", C.c_int32),
+        ("record_trajectories", C.c_int32),
         ("accuracy_goal", C.c_double),
         ("number_of_steps", C.c_uint64),
         ("oversampling", C.c_uint64),
@@ -267,6 +267,7 @@ class EnsembleSpec:
     neel_min_angle_before_transformation: float = 0.0
     use_simple_model: bool = False
     injected_dw: Optional[np.ndarray] = None
+    record_trajectories: bool = False
 
     @property
     def dims(self):
@@ -329,6 +330,7 @@ class DescHolder:
         ps.brown_min_angle_before_transformation = float(spec.brown_min_angle_before_transformation)
         ps.neel_min_angle_before_transformation = float(spec.neel_min_angle_before_transformation)
         d.max_iteration = int(spec.max_iteration)
+        d.record_trajectories = int(bool(spec.record_trajectories))
         d.accuracy_goal = float(spec.accuracy_goal)
         d.number_of_steps = int(spec.number_of_steps)
         d.oversampling = int(spec.oversampling)

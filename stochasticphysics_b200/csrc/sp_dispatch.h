@@ -1,0 +1,40 @@
+// sp_dispatch.h — host-side table of the instantiated kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "sp_types.h"
+
+namespace sp {
+
+struct KernelSet {
+    bool valid = false;
+    int D = 0, Mn = 0, OUT = 0, P = 0, real_bytes = 0;
+    void (*init)(const EnsDev* e, const RawParticles& rp, unsigned long long Np, cudaStream_t s) = nullptr;
+    void (*step)(const EnsDev* e, const TileDesc* t, int ntiles, int grid, int block, cudaStream_t s) = nullptr;
+    void (*reduce)(const EnsDev* e, int n_ens, int max_slots, int mode, cudaStream_t s) = nullptr;
+    void (*field)(const EnsDev* e, int n_ens, unsigned long long chunk, int midpoint, cudaStream_t s) = nullptr;
+    const void* step_fn = nullptr;  // for cudaFuncGetAttributes / occupancy queries
+};
+
+// index: problem, anisotropy, solver, precision (0 FP64, 1 FP32), injected noise
+const KernelSet& kernel_set(int problem, int aniso, int solver, int precision, int inject);
+inline int kernel_index(int aniso, int solver, int precision, int inject) {
+    return ((aniso * 4 + solver) * 2 + precision) * 2 + inject;
+}
+constexpr int kKernelsPerProblem = 32;
+
+void fill_neel(KernelSet* tab);
+void fill_neel_spherical(KernelSet* tab);
+void fill_brown_neel_euler(KernelSet* tab);
+void fill_brown_neel(KernelSet* tab);
+
+void launch_commit(const EnsDev* e, int n_ens, cudaStream_t s);
+void launch_set_target(EnsCtl* ctl, unsigned long long target, cudaStream_t s);
+void launch_field_window(const FieldParams& f, double dt, unsigned long long W, unsigned long long K, double* out,
+                         cudaStream_t s);
+void launch_debug_normals(unsigned long long seed, unsigned long long pid0, unsigned long long n,
+                          unsigned long long step0, unsigned long long nsteps, int noise_dim, int precision, double* out,
+                          cudaStream_t s);
+
+}  // namespace sp

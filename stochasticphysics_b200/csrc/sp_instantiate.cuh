@@ -1,0 +1,65 @@
+// sp_instantiate.cuh — builds the KernelSet entries of one problem.
+#pragma once
+
+#include "sp_dispatch.h"
+#include "sp_kernels.cuh"
+
+namespace sp {
+
+template <int PROB, class R, int A, int SOLVER, bool INJ>
+void launch_step_t(const EnsDev* e, const TileDesc* t, int ntiles, int grid, int block, cudaStream_t s) {
+    step_kernel<PROB, R, A, SOLVER, INJ><<<grid, block, 0, s>>>(e, t, ntiles);
+}
+template <int PROB, class R, int A>
+void launch_init_t(const EnsDev* e, const RawParticles& rp, unsigned long long Np, cudaStream_t s) {
+    init_kernel<PROB, R, A><<<static_cast<unsigned>(Np / kPad), kPad, 0, s>>>(e, rp);
+}
+template <class R>
+void launch_field_chunk_t(const EnsDev* e, int n_ens, unsigned long long chunk, int midpoint, cudaStream_t s) {
+    field_chunk_kernel<R><<<dim3(static_cast<unsigned>((chunk + 255) / 256), static_cast<unsigned>(n_ens)), 256, 0, s>>>(e, midpoint);
+}
+template <int OUT>
+void launch_reduce_t(const EnsDev* e, int n_ens, int max_slots, int mode, cudaStream_t s) {
+    reduce_kernel<OUT><<<dim3(static_cast<unsigned>(max_slots * OUT), static_cast<unsigned>(n_ens)), kReduceThreads, 0, s>>>(e, mode);
+}
+
+template <int PROB, class R, int A, int SOLVER, bool INJ>
+KernelSet make_set() {
+    using Prob = typename ProblemOf<PROB, R, A>::type;
+    KernelSet k;
+    if constexpr (SOLVER == kImplicitMidpoint && !Prob::kHasJacobian) {
+        return k;  // not supported by the reference either
+    } else {
+        k.valid = true;
+        k.D = Prob::D; k.Mn = Prob::Mn; k.OUT = Prob::OUT; k.P = ProblemOf<PROB, R, A>::P;
+        k.real_bytes = static_cast<int>(sizeof(R));
+        k.init = &launch_init_t<PROB, R, A>;
+        k.step = &launch_step_t<PROB, R, A, SOLVER, INJ>;
+        k.reduce = &launch_reduce_t<Prob::OUT>;
+        k.field = &launch_field_chunk_t<R>;
+        k.step_fn = reinterpret_cast<const void*>(&step_kernel<PROB, R, A, SOLVER, INJ>);
+        return k;
+    }
+}
+
+template <int PROB, int A, int SOLVER>
+void fill_solver(KernelSet* tab) {
+    tab[kernel_index(A, SOLVER, 0, 0)] = make_set<PROB, double, A, SOLVER, false>();
+    tab[kernel_index(A, SOLVER, 0, 1)] = make_set<PROB, double, A, SOLVER, true>();
+    tab[kernel_index(A, SOLVER, 1, 0)] = make_set<PROB, float, A, SOLVER, false>();
+    tab[kernel_index(A, SOLVER, 1, 1)] = make_set<PROB, float, A, SOLVER, true>();
+}
+template <int PROB, int A>
+void fill_aniso(KernelSet* tab) {
+    fill_solver<PROB, A, kEulerMaruyama>(tab);
+    fill_solver<PROB, A, kHeun>(tab);
+    fill_solver<PROB, A, kMillstein>(tab);
+    fill_solver<PROB, A, kImplicitMidpoint>(tab);
+}
+template <int PROB>
+void fill_problem(KernelSet* tab) {
+    fill_aniso<PROB, kUniaxial>(tab);
+    fill_aniso<PROB, kCubic>(tab);
+}
+
+}  // namespace sp

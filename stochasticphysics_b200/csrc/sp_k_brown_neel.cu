@@ -1,0 +1,6 @@
+// Kernel instantiations for one problem (split per problem for parallel builds).
+#include "sp_instantiate.cuh"
+
+namespace sp {
+void fill_brown_neel(KernelSet* tab) { fill_problem<kBrownNeel>(tab); }
+}  // namespace sp

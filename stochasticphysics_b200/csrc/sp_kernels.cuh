@@ -1,0 +1,373 @@
+// sp_kernels.cuh — kernel templates of the ensemble engine (sm_100a).
+//
+//  init_kernel      per-particle prefactors (FP64 formulas of
+//                   Problems/Helpers/ParameterCalculator{Neel,Brown}.h), the
+//                   initial state (getStart of each problem), sample 0 and the
+//                   weights (getWeighting), reduced per warp
+//  step_kernel      one chunk of steps for a list of particle tiles: the state
+//                   lives in registers, B(t) is computed once per step per CTA
+//                   into shared memory, the Wiener increments come from
+//                   in-kernel Philox (or from HBM in injection mode), each
+//                   window's Kahan mean is reduced per warp in FP64
+//                   (SingleParticleSimulator.h:129-159, MeanSimulationResult.h:87-119)
+//  reduce_kernel    per-warp window partials -> ensemble sums, fixed order
+//  commit_kernel    advances the device step counter (graph replay)
+//  field_window_kernel  window-mean field of the Results contract
+//                   (SingleParticleSimulator.h:236-273)
+#pragma once
+
+#include "sp_physics.cuh"
+
+namespace sp {
+
+// ------------------------------------------------------------------ problem traits
+template <int PROB, class R, int A> struct ProblemOf;
+template <class R, int A> struct ProblemOf<kNeel, R, A> { using type = NeelCart<R, A>; static constexpr int P = kParamsNeel; };
+template <class R, int A> struct ProblemOf<kNeelSpherical, R, A> { using type = NeelSph<R, A>; static constexpr int P = kParamsNeelSph; };
+template <class R, int A> struct ProblemOf<kBrownNeelEuler, R, A> { using type = BrownNeelEuler<R, A>; static constexpr int P = kParamsBrownNeelEuler; };
+template <class R, int A> struct ProblemOf<kBrownNeel, R, A> { using type = BrownNeelCart<R, A>; static constexpr int P = kParamsBrownNeel; };
+
+// ------------------------------------------------------------------ FP64 parameter formulas
+constexpr double kBoltzmann = 1.3806485279E-23;  // ParameterCalculatorNeel.h:43
+constexpr double kPiD = 3.14159265358979323846;
+
+__device__ __forceinline__ double sphere_volume(double r) { return 4.0 / 3.0 * kPiD * r * r * r; }
+
+struct NeelP { double NF1, NF2, Dp, DN; };
+// ParameterCalculatorNeel.h:44-92
+__device__ __forceinline__ NeelP neel_params(double r, double Ms, double alpha, double gamma, double T) {
+    NeelP p;
+    const double moment = sphere_volume(r) * Ms;
+    double diffsquare = 2.0 * alpha * kBoltzmann * T / (gamma * moment);
+    if (isinf(diffsquare) || isnan(diffsquare)) diffsquare = 0.0;
+    if (isinf(alpha)) { p.NF1 = 0.0; p.NF2 = 0.0; }
+    else { p.NF1 = -gamma / (1.0 + alpha * alpha); p.NF2 = fabs(p.NF1) * alpha; }
+    p.Dp = (diffsquare == 0.0) ? 0.0 : -1.0 * (p.NF1 * p.NF1) * (1.0 + alpha * alpha) * diffsquare;
+    p.DN = sqrt(diffsquare);
+    return p;
+}
+struct BrownP { double c, DB, cF; };
+// ParameterCalculatorBrown.h:39-58
+__device__ __forceinline__ BrownP brown_params(double rh, double eta, double T) {
+    BrownP p;
+    const double vh = sphere_volume(rh);
+    p.c = 1.0 / (6.0 * eta * vh);
+    p.DB = sqrt(2.0 * kBoltzmann * T * (6.0 * eta * vh));
+    if (isinf(p.DB) || isnan(p.DB)) p.DB = 0.0;
+    if (isnan(p.c)) p.c = 0.0;
+    p.cF = p.c * p.DB;
+    return p;
+}
+// NeelRelaxation.h:240-260 / ParticleStateInitializer.h:64-105
+__device__ __forceinline__ void euler_axes(const double* e, double* x, double* y, double* z) {
+    double sphi, cphi, stheta, ctheta, spsi, cpsi;
+    sincos(e[0], &sphi, &cphi);
+    sincos(e[1], &stheta, &ctheta);
+    sincos(e[2], &spsi, &cpsi);
+    const double cphicpsi = cphi * cpsi, sphicpsi = sphi * cpsi, cphispsi = cphi * spsi, sphispsi = sphi * spsi;
+    x[0] = cphicpsi - ctheta * sphispsi; x[1] = -sphicpsi - ctheta * cphispsi; x[2] = stheta * spsi;
+    y[0] = ctheta * sphicpsi + cphispsi; y[1] = ctheta * cphicpsi - sphispsi; y[2] = -stheta * cpsi;
+    z[0] = stheta * sphi; z[1] = stheta * cphi; z[2] = ctheta;
+}
+
+// Fills params[k] (FP64) and the initial state y (FP64) of particle p.
+template <int PROB>
+__device__ __forceinline__ void particle_setup(const RawParticles& rp, unsigned long long p, double* prm, double* y,
+                                               double& moment) {
+    const double r = rp.radius[p], Ms = rp.Ms[p], alpha = rp.alpha[p], gamma = rp.gamma[p], K = rp.K[p];
+    const double V = sphere_volume(r);
+    moment = V * Ms;
+    const double e[3] = {rp.euler[3 * p], rp.euler[3 * p + 1], rp.euler[3 * p + 2]};
+    const double mg[3] = {rp.mag[3 * p], rp.mag[3 * p + 1], rp.mag[3 * p + 2]};
+    const NeelP np = neel_params(r, Ms, alpha, gamma, rp.temperature);
+    const double pF = -2.0 * K / Ms;  // UniaxialAnisotropy.h:71-77, CubicAnisotropy.h:93
+    if constexpr (PROB == kNeel || PROB == kNeelSpherical) {
+        double x[3], yy[3], z[3];
+        euler_axes(e, x, yy, z);
+        if constexpr (PROB == kNeel) {
+            prm[0] = np.NF1; prm[1] = np.NF2; prm[2] = np.Dp; prm[3] = np.NF1 * np.DN; prm[4] = np.NF2 * np.DN;
+            prm[5] = pF; prm[6] = 2.0 * alpha;
+            for (int i = 0; i < 3; ++i) { prm[7 + i] = z[i]; prm[10 + i] = x[i]; prm[13 + i] = yy[i]; }
+            const double n = sqrt(mg[0] * mg[0] + mg[1] * mg[1] + mg[2] * mg[2]);  // NeelRelaxation.h:283
+            y[0] = mg[0] / n; y[1] = mg[1] / n; y[2] = mg[2] / n;
+        } else {
+            prm[0] = np.NF1; prm[1] = np.NF2; prm[2] = np.Dp; prm[3] = np.DN; prm[4] = pF; prm[5] = 2.0 * alpha;
+            for (int i = 0; i < 3; ++i) { prm[6 + i] = z[i]; prm[9 + i] = x[i]; prm[12 + i] = yy[i]; }
+            y[0] = acos(mg[2]); y[1] = atan2(mg[1], mg[0]);  // ParticleStateInitializer.h:132-144
+        }
+    } else {
+        const BrownP bp = brown_params(rp.rh[p], rp.viscosity[p], rp.temperature);
+        const double a = np.NF1, b = np.NF2, DN = np.DN;
+        const double d = bp.c * moment;  // BrownAndNeelRelaxationEulerSpherical.h:390
+        const double bpd = b + d;
+        const double cT = bp.c * (-2.0 * K * V);  // c * torque prefactor (UniaxialAnisotropy.h:79-85)
+        if constexpr (PROB == kBrownNeelEuler) {
+            prm[0] = a; prm[1] = bpd; prm[2] = d; prm[3] = cT; prm[4] = pF; prm[5] = bp.cF;
+            prm[6] = d * DN; prm[7] = bpd * DN; prm[8] = a * DN;
+            prm[9] = a * d * (DN * DN); prm[10] = 0.25 * (d * DN) * (d * DN); prm[11] = 0.5 * bp.cF * bp.cF;
+            prm[12] = 0.5 * bp.cF * bp.cF + 0.5 * (a * a + bpd * bpd) * (DN * DN);
+            y[0] = e[0]; y[1] = e[1]; y[2] = e[2];  // BrownAndNeelRelaxationEulerSpherical.h:741-753
+            y[3] = acos(mg[2]); y[4] = atan2(mg[1], mg[0]);
+        } else {
+            const bool simple = rp.simple_model != 0;
+            prm[0] = a; prm[1] = bpd; prm[2] = d; prm[3] = cT; prm[4] = pF; prm[5] = bp.cF;
+            prm[6] = simple ? 0.0 : d * DN;
+            prm[7] = (simple ? b : bpd) * DN;
+            prm[8] = a * DN;
+            prm[9] = bp.cF * bp.cF;
+            prm[10] = simple ? 0.0 : d * a * (DN * DN);
+            prm[11] = simple ? 0.0 : 0.5 * d * d * (DN * DN);
+            prm[12] = simple ? (a * a + b * b) * (DN * DN) : bp.cF * bp.cF + (a * a + bpd * bpd) * (DN * DN);
+            prm[13] = simple ? 0.0 : bp.cF;
+            // BrownAndNeelRelaxation.inl:278-324 with given orientation and magnetisation
+            double sa, ca, sb, cb, sg, cg;
+            sincos(e[0], &sa, &ca); sincos(e[1], &sb, &cb); sincos(e[2], &sg, &cg);
+            double n[3] = {ca * cg - sa * cb * sg, -ca * sg - sa * cb * cg, sa * sb};
+            const double nn = sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+            const double mm = sqrt(mg[0] * mg[0] + mg[1] * mg[1] + mg[2] * mg[2]);
+            for (int i = 0; i < 3; ++i) { y[i] = n[i] / nn; y[3 + i] = mg[i] / mm; }
+        }
+    }
+}
+
+template <int PROB>
+__device__ __forceinline__ double weight_of(int c, double moment) {
+    if constexpr (PROB == kBrownNeel) return c < 3 ? 1.0 : moment;  // BrownAndNeelRelaxation.h:152-159
+    else return moment;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// ------------------------------------------------------------------ init
+// partial slot 0 <- weighted sample 0, slot 1 <- weights (per warp)
+template <int PROB, class R, int A>
+__global__ void __launch_bounds__(kMaxBlock) init_kernel(const EnsDev* __restrict__ ens, RawParticles rp) {
+    using Prob = typename ProblemOf<PROB, R, A>::type;
+    constexpr int D = Prob::D, OUT = Prob::OUT, P = ProblemOf<PROB, R, A>::P;
+    const EnsDev& e = *ens;
+    const unsigned long long p = static_cast<unsigned long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const unsigned long long Np = e.Np;
+    if (p >= Np) return;
+    const bool active = p < e.n;
+    R* state = static_cast<R*>(e.state);
+    R* ks = static_cast<R*>(e.ksum);
+    R* kc = static_cast<R*>(e.kcomp);
+    R* prm = const_cast<R*>(static_cast<const R*>(e.params));
+    double yd[D], pd[P > 0 ? P : 1], moment = 0.0;
+    if (active) {
+        particle_setup<PROB>(rp, p, pd, yd, moment);
+    } else {
+        for (int i = 0; i < D; ++i) yd[i] = 0.0;
+        for (int i = 0; i < P; ++i) pd[i] = 0.0;
+    }
+    R y[D];
+    for (int i = 0; i < D; ++i) { y[i] = static_cast<R>(yd[i]); state[i * Np + p] = y[i]; }
+    for (int i = 0; i < P; ++i) prm[i * Np + p] = static_cast<R>(pd[i]);
+    const_cast<double*>(e.moment)[p] = moment;
+    for (int c = 0; c < OUT; ++c) { ks[c * Np + p] = R(0); kc[c * Np + p] = R(0); }
+    e.status[p] = 0;
+    R o[OUT];
+    Prob::out(y, o);
+    const unsigned long long warp = p >> 5;
+    const int lane = threadIdx.x & 31;
+    for (int c = 0; c < OUT; ++c) {
+        const double w = active ? weight_of<PROB>(c, moment) : 0.0;
+        const double vo = active ? static_cast<double>(o[c]) : 0.0;
+        if (e.traj && active) e.traj[static_cast<unsigned long long>(c) * Np + p] = vo;
+        const double s0 = warp_sum(w * vo), s1 = warp_sum(w);
+        if (lane == 0) {
+            e.partial[(warp * e.slots + 0) * OUT + c] = s0;
+            e.partial[(warp * e.slots + 1) * OUT + c] = s1;
+        }
+    }
+}
+
+// ------------------------------------------------------------------ step
+template <int PROB, class R, int A, int SOLVER, bool INJECT>
+__global__ void __launch_bounds__(kMaxBlock) step_kernel(const EnsDev* __restrict__ ensembles,
+                                                         const TileDesc* __restrict__ tiles, int ntiles) {
+    using Prob = typename ProblemOf<PROB, R, A>::type;
+    using St = Stepper<Prob, R, SOLVER>;
+    constexpr int D = Prob::D, Mn = Prob::Mn, OUT = Prob::OUT;
+    __shared__ R sB[kFieldTile][3];
+
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const TileDesc td = tiles[t];
+        const EnsDev& e = ensembles[td.ens];
+        const unsigned long long s0 = e.ctl->step_done, tgt = e.ctl->step_target;
+        const unsigned long long nsteps = tgt > s0 ? min(e.chunk, tgt - s0) : 0ull;
+        if (nsteps == 0) continue;  // uniform across the CTA
+        const unsigned long long Np = e.Np, W = e.W;
+        const unsigned long long p = td.first + threadIdx.x;
+        const bool active = p < e.n;
+        const double dt_d = e.dt;
+        const R dt = static_cast<R>(dt_d);
+        const R sqdt = static_cast<R>(e.sqrt_dt);
+        const unsigned long long seed = e.seed, pid = e.pid_offset + p;
+        const int slots = e.slots;
+        const R* ftab = static_cast<const R*>(e.ftab);
+        Rot<R> rot;
+        rot.rb = e.rot_brown != 0; rot.rn = e.rot_neel != 0;
+        rot.min1 = static_cast<R>(e.min1); rot.max1 = static_cast<R>(e.max1);
+        rot.min2 = static_cast<R>(e.min2); rot.max2 = static_cast<R>(e.max2);
+
+        R* state = static_cast<R*>(e.state);
+        R* ks = static_cast<R*>(e.ksum);
+        R* kc = static_cast<R*>(e.kcomp);
+        const R* prm = static_cast<const R*>(e.params);
+        R y[D], sum[OUT], comp[OUT];
+        typename Prob::Par q;
+        double moment = 0.0;
+        if (active) {
+#pragma unroll
+            for (int i = 0; i < D; ++i) y[i] = state[i * Np + p];
+#pragma unroll
+            for (int c = 0; c < OUT; ++c) { sum[c] = ks[c * Np + p]; comp[c] = kc[c * Np + p]; }
+            q = Prob::load(prm, Np, p);
+            moment = e.moment[p];
+        } else {
+#pragma unroll
+            for (int i = 0; i < D; ++i) y[i] = R(0);
+#pragma unroll
+            for (int c = 0; c < OUT; ++c) { sum[c] = R(0); comp[c] = R(0); }
+            q = Prob::load(prm, Np, td.first);  // any valid slot; results are discarded
+        }
+        NewtonCount nc{0u, 0u};
+        unsigned long long wpos = s0 % W;
+        const unsigned long long kbase = s0 / W;  // windows completed before this chunk
+        const unsigned long long warp = p >> 5;
+        const int lane = threadIdx.x & 31;
+        const R* dwp = static_cast<const R*>(e.dw);
+        double* const traj = e.traj;
+        double* const partial = e.partial;
+
+        for (unsigned long long t0 = 0; t0 < nsteps; t0 += kFieldTile) {
+            const int len = static_cast<int>(min(static_cast<unsigned long long>(kFieldTile), nsteps - t0));
+            __syncthreads();
+            for (int i = threadIdx.x; i < 3 * len; i += blockDim.x) (&sB[0][0])[i] = ftab[3 * t0 + i];
+            __syncthreads();
+            for (int i = 0; i < len; ++i) {
+                const unsigned long long g = s0 + t0 + i;
+                if (active) {
+                    R w[Mn];
+                    if constexpr (INJECT) {
+#pragma unroll
+                        for (int j = 0; j < Mn; ++j) w[j] = dwp[(g * Mn + j) * Np + p];
+                    } else {
+                        philox_normals<R, Mn>(seed, pid, g, w);
+#pragma unroll
+                        for (int j = 0; j < Mn; ++j) w[j] = w[j] * sqdt;
+                    }
+                    const R B[3] = {sB[i][0], sB[i][1], sB[i][2]};
+                    St::step(q, rot, y, B, w, dt, e.max_iter, e.tol, nc);
+                    R o[OUT];
+                    Prob::out(y, o);
+#pragma unroll
+                    for (int c = 0; c < OUT; ++c) {  // Kahan summation (SingleParticleSimulator.h:148-153)
+                        const R yv = o[c] - comp[c];
+                        const R tv = sum[c] + yv;
+                        comp[c] = (tv - sum[c]) - yv;
+                        sum[c] = tv;
+                    }
+                }
+                if (++wpos == W) {  // window end: uniform across the CTA
+                    wpos = 0;
+                    const unsigned long long k = (g + 1) / W;
+                    const int slot = static_cast<int>(k - kbase - 1);
+#pragma unroll
+                    for (int c = 0; c < OUT; ++c) {
+                        const R v = active ? sum[c] / static_cast<R>(static_cast<double>(W)) : R(0);
+                        sum[c] = R(0);
+                        const double vd = static_cast<double>(v);
+                        if (traj && active) traj[(k * OUT + c) * Np + p] = vd;
+                        const double ws = warp_sum(active ? weight_of<PROB>(c, moment) * vd : 0.0);
+                        if (lane == 0) partial[(warp * slots + slot) * OUT + c] = ws;
+                    }
+                }
+            }
+        }
+        if (active) {
+            bool finite = true;
+#pragma unroll
+            for (int i = 0; i < D; ++i) { state[i * Np + p] = y[i]; finite = finite && M<R>::finite(y[i]); }
+#pragma unroll
+            for (int c = 0; c < OUT; ++c) { ks[c * Np + p] = sum[c]; kc[c * Np + p] = comp[c]; }
+            if (!finite) e.status[p] = 1;
+        }
+        if constexpr (SOLVER == kImplicitMidpoint) {
+            unsigned int it = nc.iterations, un = nc.unconverged;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) { it += __shfl_xor_sync(0xffffffffu, it, o); un += __shfl_xor_sync(0xffffffffu, un, o); }
+            if (lane == 0) {
+                atomicAdd(&e.ctl->newton_iterations, static_cast<unsigned long long>(it));
+                atomicAdd(&e.ctl->newton_unconverged, static_cast<unsigned long long>(un));
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------------ reductions
+// grid (slots*OUT, n_ens); block kReduceThreads.  mode 0: windows completed in
+// the current chunk -> msum[k]; mode 1 (after init): slot 0 -> msum[0], slot 1 -> wsum.
+template <int OUT>
+__global__ void __launch_bounds__(kReduceThreads) reduce_kernel(const EnsDev* __restrict__ ensembles, int mode) {
+    const EnsDev& e = ensembles[blockIdx.y];
+    const int slot = blockIdx.x / OUT, c = blockIdx.x % OUT;
+    if (slot >= e.slots) return;
+    double* dst;
+    if (mode == 0) {
+        const unsigned long long s0 = e.ctl->step_done, tgt = e.ctl->step_target;
+        const unsigned long long nsteps = tgt > s0 ? min(e.chunk, tgt - s0) : 0ull;
+        const unsigned long long nwin = (s0 + nsteps) / e.W - s0 / e.W;
+        if (static_cast<unsigned long long>(slot) >= nwin) return;
+        dst = e.msum + (s0 / e.W + 1 + slot) * OUT + c;
+    } else {
+        if (slot > 1) return;
+        dst = (slot == 0) ? e.msum + c : e.wsum + c;
+    }
+    const unsigned long long nwarps = e.Np >> 5;
+    double acc = 0.0;
+    for (unsigned long long w = threadIdx.x; w < nwarps; w += blockDim.x) acc += e.partial[(w * e.slots + slot) * OUT + c];
+    __shared__ double red[kReduceThreads];
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s = kReduceThreads / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *dst = red[0];
+}
+
+// B(t) for every step of the current chunk of each ensemble (grid.y = ensemble):
+// t = (n+1) dt (SingleParticleSimulator.h:145), + dt/2 for ImplicitMidpoint
+// (Implicit_Midpoint.inl:59); phase and sine in FP64, stored as Real.
+template <class R>
+__global__ void field_chunk_kernel(const EnsDev* __restrict__ ensembles, int midpoint) {
+    const EnsDev& e = ensembles[blockIdx.y];
+    const unsigned long long s0 = e.ctl->step_done, tgt = e.ctl->step_target;
+    const unsigned long long nsteps = tgt > s0 ? min(e.chunk, tgt - s0) : 0ull;
+    const unsigned long long i = static_cast<unsigned long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= nsteps) return;
+    const double t = e.dt * static_cast<double>(s0 + i + 1) + (midpoint ? 0.5 * e.dt : 0.0);
+    double B[3];
+    field_eval(e.field, t, B);
+    R* f = static_cast<R*>(e.ftab) + 3 * i;
+    f[0] = static_cast<R>(B[0]); f[1] = static_cast<R>(B[1]); f[2] = static_cast<R>(B[2]);
+}
+
+template <class R, int Mn>
+__global__ void debug_normals_kernel(unsigned long long seed, unsigned long long pid0, unsigned long long n,
+                                     unsigned long long step0, unsigned long long nsteps, double* out) {
+    const unsigned long long idx = static_cast<unsigned long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (idx >= n * nsteps) return;
+    const unsigned long long s = idx / n, p = idx % n;
+    R z[Mn];
+    philox_normals<R, Mn>(seed, pid0 + p, step0 + s, z);
+    for (int j = 0; j < Mn; ++j) out[(s * Mn + j) * n + p] = static_cast<double>(z[j]);
+}
+
+}  // namespace sp

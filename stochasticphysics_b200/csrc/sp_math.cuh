@@ -1,0 +1,169 @@
+// sp_math.cuh — precision-generic device math, 3-vectors and the Philox noise source.
+//
+// FP64 instantiations call the IEEE double routines.  FP32 instantiations use
+// the SFU approximations (__sincosf, __logf) where the stepping tolerates
+// them; the field phase, time and ensemble sums never pass through here in
+// FP32 (they are computed in double by the kernels).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "sp_types.h"
+
+namespace sp {
+
+template <class R> struct M;
+
+template <> struct M<double> {
+    static __device__ __forceinline__ double sin(double x) { return ::sin(x); }
+    static __device__ __forceinline__ double cos(double x) { return ::cos(x); }
+    static __device__ __forceinline__ void sincos(double x, double* s, double* c) { ::sincos(x, s, c); }
+    static __device__ __forceinline__ double acos(double x) { return ::acos(x); }
+    static __device__ __forceinline__ double atan2(double y, double x) { return ::atan2(y, x); }
+    static __device__ __forceinline__ double fmod(double x, double y) { return ::fmod(x, y); }
+    static __device__ __forceinline__ double sqrt(double x) { return ::sqrt(x); }
+    static __device__ __forceinline__ double rcp(double x) { return 1.0 / x; }
+    static __device__ __forceinline__ double abs(double x) { return ::fabs(x); }
+    static __device__ __forceinline__ bool isinf(double x) { return ::isinf(x); }
+    static __device__ __forceinline__ bool finite(double x) { return ::isfinite(x); }
+    static constexpr double two_pi = 6.283185307179586;
+    static constexpr double eps = 2.220446049250313e-16;
+};
+
+template <> struct M<float> {
+    static __device__ __forceinline__ float sin(float x) { return __sinf(x); }
+    static __device__ __forceinline__ float cos(float x) { return __cosf(x); }
+    static __device__ __forceinline__ void sincos(float x, float* s, float* c) { __sincosf(x, s, c); }
+    static __device__ __forceinline__ float acos(float x) { return ::acosf(x); }
+    static __device__ __forceinline__ float atan2(float y, float x) { return ::atan2f(y, x); }
+    static __device__ __forceinline__ float fmod(float x, float y) { return ::fmodf(x, y); }
+    static __device__ __forceinline__ float sqrt(float x) { return ::sqrtf(x); }
+    static __device__ __forceinline__ float rcp(float x) { return __frcp_rn(x); }
+    static __device__ __forceinline__ float abs(float x) { return ::fabsf(x); }
+    static __device__ __forceinline__ bool isinf(float x) { return ::isinf(x); }
+    static __device__ __forceinline__ bool finite(float x) { return ::isfinite(x); }
+    static constexpr float two_pi = 6.283185307179586f;
+    static constexpr float eps = 1.1920929e-7f;
+};
+
+template <class R>
+struct V3 {
+    R x, y, z;
+};
+template <class R> __device__ __forceinline__ V3<R> v3(R a, R b, R c) { return V3<R>{a, b, c}; }
+template <class R> __device__ __forceinline__ V3<R> operator+(V3<R> a, V3<R> b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+template <class R> __device__ __forceinline__ V3<R> operator-(V3<R> a, V3<R> b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+template <class R> __device__ __forceinline__ V3<R> operator*(R s, V3<R> a) { return {s * a.x, s * a.y, s * a.z}; }
+template <class R> __device__ __forceinline__ R dot(V3<R> a, V3<R> b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+template <class R> __device__ __forceinline__ V3<R> cross(V3<R> a, V3<R> b) {
+    return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+
+// ------------------------------------------------------------------ Philox4x32-10
+// Counter-based generator of Salmon, Moraes, Dror and Shaw (SC'11).  Particle p
+// at integrated step n draws
+//   counter = {n_lo, n_hi, pid_lo, (pid_hi & 0xFFFFFF) | call << 24}, key = seed
+// so the stream depends on neither launch shape, chunking nor co-scheduling.
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint32_t k0, uint32_t k1) {
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const uint32_t hi0 = __umulhi(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
+        const uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
+        c = make_uint4(hi1 ^ c.y ^ k0, lo1, hi0 ^ c.w ^ k1, lo0);
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    return c;
+}
+
+__device__ __forceinline__ uint4 philox_block(unsigned long long seed, unsigned long long pid, unsigned long long step,
+                                              uint32_t call) {
+    const uint4 c = make_uint4(static_cast<uint32_t>(step), static_cast<uint32_t>(step >> 32),
+                               static_cast<uint32_t>(pid),
+                               (static_cast<uint32_t>(pid >> 32) & 0xFFFFFFu) | (call << 24));
+    return philox4x32_10(c, static_cast<uint32_t>(seed), static_cast<uint32_t>(seed >> 32));
+}
+
+// Box-Muller on u = (w + 1/2) 2^-32.  npairs = 1 or 2 pairs of normals.
+__device__ __forceinline__ void box_muller(uint4 w, int npairs, double* z) {
+    const double inv = 2.3283064365386963e-10, half = 1.1641532182693481e-10;  // 2^-32, 2^-33
+    {
+        const double u0 = fma(static_cast<double>(w.x), inv, half), u1 = fma(static_cast<double>(w.y), inv, half);
+        const double r = ::sqrt(-2.0 * ::log(u0));
+        double s, c;
+        ::sincospi(2.0 * u1, &s, &c);
+        z[0] = r * c;
+        z[1] = r * s;
+    }
+    if (npairs > 1) {
+        const double u2 = fma(static_cast<double>(w.z), inv, half), u3 = fma(static_cast<double>(w.w), inv, half);
+        const double r = ::sqrt(-2.0 * ::log(u2));
+        double s, c;
+        ::sincospi(2.0 * u3, &s, &c);
+        z[2] = r * c;
+        z[3] = r * s;
+    }
+}
+__device__ __forceinline__ void box_muller(uint4 w, int npairs, float* z) {
+    const float inv = 2.3283064e-10f, half = 1.1641532e-10f;
+    {
+        const float u0 = fmaf(__uint2float_rn(w.x), inv, half), u1 = fmaf(__uint2float_rn(w.y), inv, half);
+        const float r = ::sqrtf(-2.0f * __logf(u0));
+        float s, c;
+        __sincosf(6.2831853f * u1, &s, &c);
+        z[0] = r * c;
+        z[1] = r * s;
+    }
+    if (npairs > 1) {
+        const float u2 = fmaf(__uint2float_rn(w.z), inv, half), u3 = fmaf(__uint2float_rn(w.w), inv, half);
+        const float r = ::sqrtf(-2.0f * __logf(u2));
+        float s, c;
+        __sincosf(6.2831853f * u3, &s, &c);
+        z[2] = r * c;
+        z[3] = r * s;
+    }
+}
+
+// m unit normals (m = 3 or 6) for (seed, pid, step)
+template <class R, int Mdim>
+__device__ __forceinline__ void philox_normals(unsigned long long seed, unsigned long long pid, unsigned long long step,
+                                               R* z) {
+    R t[4];
+    box_muller(philox_block(seed, pid, step, 0u), 2, t);
+    z[0] = t[0];
+    z[1] = t[1];
+    z[2] = t[2];
+    if (Mdim > 3) {
+        z[3] = t[3];
+        R u[4];
+        box_muller(philox_block(seed, pid, step, 1u), 1, u);
+        z[4] = u[0];
+        z[5] = u[1];
+    }
+}
+
+// B(t) in double: SinusoidalField.h:47-51 / LissajousField.h:98-101.  The phase
+// products are rounded separately (no fused multiply-add) like the host code.
+__device__ __forceinline__ void field_eval(const FieldParams& f, double t, double* B) {
+    switch (f.type) {
+        case 0:
+            B[0] = B[1] = B[2] = 0.0;
+            break;
+        case 1:
+            B[0] = f.offset[0]; B[1] = f.offset[1]; B[2] = f.offset[2];
+            break;
+        case 2: {
+            const double s = ::sin(__dadd_rn(__dmul_rn(f.omega[0], t), f.phase[0]));
+#pragma unroll
+            for (int i = 0; i < 3; ++i) B[i] = __dadd_rn(__dmul_rn(f.amplitude[i], s), f.offset[i]);
+            break;
+        }
+        default:
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+                B[i] = __dadd_rn(f.offset[i], __dmul_rn(f.amplitude[i], ::sin(__dadd_rn(__dmul_rn(f.omega[i], t), f.phase[i]))));
+    }
+}
+
+}  // namespace sp

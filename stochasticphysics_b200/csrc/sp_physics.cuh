@@ -1,0 +1,666 @@
+// sp_physics.cuh — per-particle SDE right-hand sides and steppers (device code).
+//
+// One thread integrates one particle; every function works on registers.  The
+// stochastic term is applied as b(y)·dW directly (the D x M matrix is never
+// formed).  Reference formulas, by problem:
+//   Neel (Cartesian LLG)      Problems/NeelRelaxation.h:92-190
+//   Neel spherical            Problems/NeelRelaxationSpherical.h:124-516
+//   Brown+Neel Euler/sph.     Problems/BrownAndNeelRelaxationEulerSpherical.h:141-735
+//   Brown+Neel Cartesian      Problems/BrownAndNeelRelaxation.inl:40-270
+//   uniaxial / cubic          Problems/Anisotropy/{Uniaxial,Cubic}Anisotropy.h
+// and by solver (Stratonovich forms):
+//   EulerMaruyama             SDEFramework/Solver/EulerMaruyama.inl:42-72
+//   Heun_Strong               SDEFramework/Solver/Heun_Strong.inl:37-47
+//   Millstein                 SDEFramework/Solver/Millstein.inl:35-44
+//   Implicit_Midpoint         SDEFramework/Solver/Implicit_Midpoint.inl:40-105,175
+// Per-particle prefactors are precomputed in FP64 by the init kernel and
+// grouped so that FP32 never forms an overflowing product (c^2 ~ 1e48).
+#pragma once
+
+#include "sp_math.cuh"
+#include "sp_types.h"
+
+namespace sp {
+
+template <class R>
+struct Rot {
+    bool rb, rn;          // rotation enabled (Neel spherical uses rb)
+    R min1, max1, min2, max2;
+};
+
+// ------------------------------------------------------------------ anisotropy
+template <class R, int A>
+struct Aniso {
+    // effective anisotropy field + external field
+    static __device__ __forceinline__ V3<R> heff(R pF, V3<R> m, V3<R> x, V3<R> y, V3<R> z, V3<R> B) {
+        if constexpr (A == kUniaxial) {
+            return (pF * dot(m, z)) * z + B;  // UniaxialAnisotropy.h:140-144
+        } else {                              // CubicAnisotropy.h:133-146
+            const R c1 = dot(m, x), c2 = dot(m, y), c3 = dot(m, z);
+            const R c1s = c1 * c1, c2s = c2 * c2, c3s = c3 * c3;
+            return pF * (((c2s + c3s) * c1) * x + ((c1s + c3s) * c2) * y + ((c1s + c2s) * c3) * z) + B;
+        }
+    }
+};
+
+// ======================================================================= Neel (Cartesian)
+template <class R, int A>
+struct NeelCart {
+    static constexpr int D = 3, Mn = 3, OUT = 3;
+    static constexpr bool kHasJacobian = true;
+    struct Par {
+        R NF1, NF2, Dp, pre1, pre2, pF, twoalpha;
+        V3<R> z, x, y;
+    };
+    struct Cache {};
+    static __device__ __forceinline__ Par load(const R* P, unsigned long long Np, unsigned long long p) {
+        Par q;
+        q.NF1 = P[0 * Np + p]; q.NF2 = P[1 * Np + p]; q.Dp = P[2 * Np + p];
+        q.pre1 = P[3 * Np + p]; q.pre2 = P[4 * Np + p]; q.pF = P[5 * Np + p]; q.twoalpha = P[6 * Np + p];
+        q.z = v3(P[7 * Np + p], P[8 * Np + p], P[9 * Np + p]);
+        if constexpr (A == kCubic) {
+            q.x = v3(P[10 * Np + p], P[11 * Np + p], P[12 * Np + p]);
+            q.y = v3(P[13 * Np + p], P[14 * Np + p], P[15 * Np + p]);
+        } else {
+            q.x = q.y = v3(R(0), R(0), R(0));
+        }
+        return q;
+    }
+    static __device__ __forceinline__ void prepare(const Par&, const Rot<R>&, R*, Cache&) {}
+    static __device__ __forceinline__ void recompute(const Par&, const R*, Cache&) {}
+    static __device__ __forceinline__ void finish(const Rot<R>&, R*, const Cache&) {}
+    static __device__ __forceinline__ void det(const Par& q, const R* y, const Cache&, const R* B, R* a) {
+        const V3<R> m = v3(y[0], y[1], y[2]);
+        const V3<R> H = Aniso<R, A>::heff(q.pF, m, q.x, q.y, q.z, v3(B[0], B[1], B[2]));
+        const V3<R> mxH = cross(m, H);
+        const V3<R> r = q.NF1 * mxH - q.NF2 * cross(m, mxH);
+        a[0] = r.x; a[1] = r.y; a[2] = r.z;
+    }
+    static __device__ __forceinline__ void drift(const Par& q, const R* y, const Cache&, R* d) {
+        d[0] = q.Dp * y[0]; d[1] = q.Dp * y[1]; d[2] = q.Dp * y[2];
+    }
+    // b(m)·w = pre2 (w - m (m·w)) + pre1 (m x w)          NeelRelaxation.h:92-109
+    static __device__ __forceinline__ void bdw(const Par& q, const R* y, const Cache&, const R* w, R* r) {
+        const V3<R> m = v3(y[0], y[1], y[2]), W = v3(w[0], w[1], w[2]);
+        const V3<R> o = q.pre2 * (W - dot(m, W) * m) + q.pre1 * cross(m, W);
+        r[0] = o.x; r[1] = o.y; r[2] = o.z;
+    }
+    static __device__ __forceinline__ void out(const R* y, R* o) { o[0] = y[0]; o[1] = y[1]; o[2] = y[2]; }
+    // S = -I + dt/2 J_det + 1/2 J_sto with the reference Jacobians (NeelRelaxation.h:134-190):
+    // J_det = NF1([m]x J_H - [H]x) - (2 alpha/dt)[m]x, J_sto = -pre1 [dW]x, J_H = pF z z^T (cubic: I)
+    static __device__ __forceinline__ void newton_matrix(const Par& q, const R* y, const Cache&, const R* B, const R* w,
+                                                         R dt, R S[D][D]) {
+        const V3<R> m = v3(y[0], y[1], y[2]);
+        const V3<R> H = Aniso<R, A>::heff(q.pF, m, q.x, q.y, q.z, v3(B[0], B[1], B[2]));
+        R JH[3][3];
+        const R zz[3] = {q.z.x, q.z.y, q.z.z};
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) JH[i][j] = (A == kUniaxial) ? (q.pF * zz[i]) * zz[j] : R(i == j ? 1 : 0);
+        const R mx[3][3] = {{R(0), -m.z, m.y}, {m.z, R(0), -m.x}, {-m.y, m.x, R(0)}};
+        const R hx[3][3] = {{R(0), -H.z, H.y}, {H.z, R(0), -H.x}, {-H.y, H.x, R(0)}};
+        const R wx[3][3] = {{R(0), -w[2], w[1]}, {w[2], R(0), -w[0]}, {-w[1], w[0], R(0)}};
+        const R damp = q.twoalpha / dt;
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) {
+                R mj = mx[i][0] * JH[0][j] + mx[i][1] * JH[1][j] + mx[i][2] * JH[2][j];
+                const R jdet = q.NF1 * (mj - hx[i][j]) - damp * mx[i][j];
+                const R jsto = -q.pre1 * wx[i][j];
+                S[i][j] = (i == j ? R(-1) : R(0)) + (R(0.5) * dt) * jdet + R(0.5) * jsto;
+            }
+    }
+};
+
+// ======================================================================= Neel (spherical)
+template <class R, int A>
+struct NeelSph {
+    static constexpr int D = 2, Mn = 3, OUT = 3;
+    static constexpr bool kHasJacobian = true;
+    struct Par {
+        R NF1, NF2, Dp, DN, pF, twoalpha;
+        V3<R> z, x, y;
+    };
+    struct Cache {
+        bool rot;
+        R odst, st, ct;
+        V3<R> md, eth, eph;
+        V3<R> P0, P1;
+    };
+    static __device__ __forceinline__ Par load(const R* P, unsigned long long Np, unsigned long long p) {
+        Par q;
+        q.NF1 = P[0 * Np + p]; q.NF2 = P[1 * Np + p]; q.Dp = P[2 * Np + p]; q.DN = P[3 * Np + p];
+        q.pF = P[4 * Np + p]; q.twoalpha = P[5 * Np + p];
+        q.z = v3(P[6 * Np + p], P[7 * Np + p], P[8 * Np + p]);
+        if constexpr (A == kCubic) {
+            q.x = v3(P[9 * Np + p], P[10 * Np + p], P[11 * Np + p]);
+            q.y = v3(P[12 * Np + p], P[13 * Np + p], P[14 * Np + p]);
+        } else {
+            q.x = q.y = v3(R(0), R(0), R(0));
+        }
+        return q;
+    }
+    // NeelRelaxationSpherical.h:568-602
+    static __device__ __forceinline__ void rotate(R* y) {
+        R st, ct, sp, cp;
+        M<R>::sincos(y[0], &st, &ct);
+        M<R>::sincos(y[1], &sp, &cp);
+        const R t = M<R>::acos(-cp * st), p = M<R>::atan2(sp * st, ct);
+        y[0] = t; y[1] = p;
+    }
+    static __device__ __forceinline__ void unrotate(R* y) {
+        R st, ct, sp, cp;
+        M<R>::sincos(y[0], &st, &ct);
+        M<R>::sincos(y[1], &sp, &cp);
+        const R t = M<R>::acos(cp * st), p = M<R>::atan2(sp * st, -ct);
+        y[0] = t; y[1] = p;
+    }
+    // :124-237
+    static __device__ __forceinline__ void prepare(const Par& q, const Rot<R>& r, R* y, Cache& c) {
+        c.rot = r.rb && (y[0] < r.min1 || y[0] > r.max1);
+        if (c.rot) rotate(y);
+        recompute(q, y, c);
+    }
+    static __device__ __forceinline__ void recompute(const Par& q, const R* y, Cache& c) {
+        R st, ct, sp, cp;
+        M<R>::sincos(y[0], &st, &ct);
+        M<R>::sincos(y[1], &sp, &cp);
+        c.st = st; c.ct = ct;
+        R odst = R(1) / st;
+        if (M<R>::isinf(odst)) odst = R(0);
+        c.odst = odst;
+        if (!c.rot) {
+            c.md = v3(st * cp, st * sp, ct);
+            c.eth = v3(ct * cp, ct * sp, -st);
+            c.eph = v3(-sp, cp, R(0));
+        } else {
+            c.md = v3(-ct, st * sp, st * cp);
+            c.eth = v3(st, ct * sp, ct * cp);
+            c.eph = v3(R(0), cp, -sp);
+        }
+        c.P0 = (-q.NF1) * c.eph + q.NF2 * c.eth;
+        c.P1 = odst * (q.NF1 * c.eth + q.NF2 * c.eph);
+        if (odst == R(0)) {
+            if (!c.rot) c.P1.z = q.NF1;
+            else c.P1.x = -q.NF1;
+        }
+    }
+    static __device__ __forceinline__ void finish(const Rot<R>&, R* y, const Cache& c) {
+        if (c.rot) unrotate(y);
+        else { y[0] = M<R>::fmod(y[0], M<R>::two_pi); y[1] = M<R>::fmod(y[1], M<R>::two_pi); }
+    }
+    static __device__ __forceinline__ void det(const Par& q, const R*, const Cache& c, const R* B, R* a) {
+        const V3<R> H = Aniso<R, A>::heff(q.pF, c.md, q.x, q.y, q.z, v3(B[0], B[1], B[2]));
+        a[0] = dot(c.P0, H);
+        a[1] = dot(c.P1, H);
+    }
+    static __device__ __forceinline__ void drift(const Par& q, const R*, const Cache& c, R* d) {
+        const R cos_t = c.rot ? -c.md.x : c.md.z;
+        d[0] = R(-0.5) * q.Dp * cos_t * c.odst;
+        d[1] = R(0);
+    }
+    static __device__ __forceinline__ void bdw(const Par& q, const R*, const Cache& c, const R* w, R* r) {
+        const V3<R> W = v3(w[0], w[1], w[2]);
+        r[0] = q.DN * dot(c.P0, W);
+        r[1] = q.DN * dot(c.P1, W);
+    }
+    static __device__ __forceinline__ void out(const R* y, R* o) {
+        R st, ct, sp, cp;
+        M<R>::sincos(y[0], &st, &ct);
+        M<R>::sincos(y[1], &sp, &cp);
+        o[0] = st * cp; o[1] = st * sp; o[2] = ct;
+    }
+    // NeelRelaxationSpherical.h:312-432 and finishJacobiCalculations :473-497
+    static __device__ __forceinline__ void newton_matrix(const Par& q, const R*, const Cache& c, const R* B, const R* w,
+                                                         R dt, R S[D][D]) {
+        const R cos_t = c.rot ? -c.md.x : c.md.z;
+        const R sin_t = c.rot ? c.eth.x : -c.eth.z;
+        const V3<R> Jer0 = c.eth, Jer1 = sin_t * c.eph;
+        const V3<R> Jth0 = (R(-1)) * c.md, Jth1 = cos_t * c.eph;
+        const V3<R> Jph0 = v3(R(0), R(0), R(0));
+        const V3<R> Jph1 = c.rot ? v3(R(0), c.eph.z, -c.eph.y) : v3(-c.eph.y, c.eph.x, R(0));
+        const V3<R> H = Aniso<R, A>::heff(q.pF, c.md, q.x, q.y, q.z, v3(B[0], B[1], B[2]));
+        const R a = q.NF1, b = q.NF2;
+        // J_H J_er^T columns (3-vectors), c = 0, 1
+        V3<R> HJer[2];
+        const V3<R> Jer[2] = {Jer0, Jer1};
+        for (int k = 0; k < 2; ++k) {
+            if constexpr (A == kUniaxial) HJer[k] = (q.pF * dot(q.z, Jer[k])) * q.z;
+            else HJer[k] = Jer[k];
+        }
+        const V3<R> A0[2] = {(-a) * Jph0 + b * Jth0, (-a) * Jph1 + b * Jth1};  // rows of (-a J_phi + b J_theta)
+        const V3<R> B1[2] = {c.odst * (a * Jth0 + b * Jph0), c.odst * (a * Jth1 + b * Jph1)};
+        const V3<R> ab = a * c.eth + b * c.eph;
+        const R jst = c.odst * c.odst * cos_t;
+        const V3<R> W = v3(w[0], w[1], w[2]);
+        R Jd[2][2], Js[2][2];
+        for (int k = 0; k < 2; ++k) {
+            Jd[0][k] = dot(A0[k], H) + dot(c.P0, HJer[k]);
+            Js[0][k] = q.DN * dot(A0[k], W);
+            const V3<R> rowk = (k == 0) ? B1[0] - jst * ab : B1[1];
+            // (P1 J_H) J_er^T
+            V3<R> P1JH;
+            if constexpr (A == kUniaxial) P1JH = (q.pF * dot(c.P1, q.z)) * q.z;
+            else P1JH = c.P1;
+            Jd[1][k] = dot(H, rowk) + dot(P1JH, Jer[k]);
+            Js[1][k] = q.DN * dot(W, rowk);
+        }
+        for (int i = 0; i < 2; ++i)
+            for (int k = 0; k < 2; ++k) S[i][k] = (i == k ? R(-1) : R(0)) + (R(0.5) * dt) * Jd[i][k] + R(0.5) * Js[i][k];
+        if (c.rot) {
+            const R m_cos_t = c.md.x, sin_t2 = c.eth.x, cos_p = c.eph.y, m_sin_p = c.eph.z;
+            const R factor = R(1) / M<R>::sqrt(R(1) - sin_t2 * sin_t2 * cos_p * cos_p);
+            const R J00 = factor * m_cos_t * cos_p, J01 = m_sin_p;
+            const R J10 = -factor * c.odst * m_sin_p, J11 = c.odst * m_cos_t * cos_p;
+            for (int i = 0; i < 2; ++i) {
+                const R s0 = S[i][0], s1 = S[i][1];
+                S[i][0] = s0 * J00 + s1 * J10;
+                S[i][1] = s0 * J01 + s1 * J11;
+            }
+        }
+    }
+};
+
+// ======================================================================= Brown + Neel, Euler/spherical
+template <class R, int A>
+struct BrownNeelEuler {
+    static constexpr int D = 5, Mn = 6, OUT = 9;
+    static constexpr bool kHasJacobian = false;  // assert(false) in the reference (:605-626)
+    struct Par {
+        R a, bpd, d, cT, pF, cF, dDN, bpdDN, aDN, adDN2, d2fDN2, cF2h, nd;
+    };
+    struct Cache {
+        bool br, nr;
+        R S[5], C[5];
+        R csc, odst;
+        V3<R> md;
+    };
+    static __device__ __forceinline__ Par load(const R* P, unsigned long long Np, unsigned long long p) {
+        Par q;
+        q.a = P[0 * Np + p]; q.bpd = P[1 * Np + p]; q.d = P[2 * Np + p]; q.cT = P[3 * Np + p];
+        q.pF = P[4 * Np + p]; q.cF = P[5 * Np + p]; q.dDN = P[6 * Np + p]; q.bpdDN = P[7 * Np + p];
+        q.aDN = P[8 * Np + p]; q.adDN2 = P[9 * Np + p]; q.d2fDN2 = P[10 * Np + p]; q.cF2h = P[11 * Np + p];
+        q.nd = P[12 * Np + p];
+        return q;
+    }
+    // :859-899
+    static __device__ __forceinline__ void euler_rotate(R* e) {
+        R S0, C0, S1, C1, S2, C2;
+        M<R>::sincos(e[0], &S0, &C0); M<R>::sincos(e[1], &S1, &C1); M<R>::sincos(e[2], &S2, &C2);
+        const R np = M<R>::atan2(-C2 * C0 + C1 * S0 * S2, S0 * C2 + C1 * C0 * S2);
+        const R nt = M<R>::acos(-S1 * S2);
+        const R ns = M<R>::atan2(C1, C2 * S1);
+        e[0] = np; e[1] = nt; e[2] = ns;
+    }
+    static __device__ __forceinline__ void euler_unrotate(R* e) {
+        R S0, C0, S1, C1, S2, C2;
+        M<R>::sincos(e[0], &S0, &C0); M<R>::sincos(e[1], &S1, &C1); M<R>::sincos(e[2], &S2, &C2);
+        const R np = M<R>::atan2(C0 * C2 - C1 * S0 * S2, -C2 * S0 - C1 * C0 * S2);
+        const R nt = M<R>::acos(S1 * S2);
+        const R ns = M<R>::atan2(-C1, C2 * S1);
+        e[0] = np; e[1] = nt; e[2] = ns;
+    }
+    static __device__ __forceinline__ void neel_rotate(R* y) { NeelSph<R, A>::rotate(y); }
+    static __device__ __forceinline__ void neel_unrotate(R* y) { NeelSph<R, A>::unrotate(y); }
+    // :141-361
+    static __device__ __forceinline__ void prepare(const Par& q, const Rot<R>& r, R* y, Cache& c) {
+        const R tb = M<R>::abs(y[1]);
+        c.br = r.rb && (tb < r.min1 || tb > r.max1);
+        if (c.br) euler_rotate(y);
+        const R tn = M<R>::abs(y[3]);
+        c.nr = r.rn && (tn < r.min2 || tn > r.max2);
+        if (c.nr) neel_rotate(y + 3);
+        recompute(q, y, c);
+    }
+    static __device__ __forceinline__ void recompute(const Par&, const R* y, Cache& c) {
+#pragma unroll
+        for (int i = 0; i < 5; ++i) M<R>::sincos(y[i], &c.S[i], &c.C[i]);
+        R csc = R(1) / c.S[1];
+        if (M<R>::isinf(csc)) csc = R(0);
+        c.csc = csc;
+        R odst = R(1) / c.S[3];
+        if (M<R>::isinf(odst)) odst = R(0);
+        c.odst = odst;
+        const R ct = c.C[3], cp = c.C[4], st = c.S[3], sp = c.S[4];
+        c.md = c.nr ? v3(-ct, st * sp, st * cp) : v3(st * cp, st * sp, ct);
+    }
+    // body axes (columns of the cached Euler rotation matrix, :183-304)
+    static __device__ __forceinline__ void axes(const Cache& c, V3<R>& x, V3<R>& y, V3<R>& z) {
+        const R cphi = c.C[0], ctheta = c.C[1], cpsi = c.C[2], sphi = c.S[0], stheta = c.S[1], spsi = c.S[2];
+        const R cphicpsi = cphi * cpsi, sphicpsi = sphi * cpsi, cphispsi = cphi * spsi, sphispsi = sphi * spsi;
+        if (!c.br) {
+            x = v3(cphicpsi - ctheta * sphispsi, ctheta * sphicpsi + cphispsi, stheta * sphi);
+            y = v3(-sphicpsi - ctheta * cphispsi, ctheta * cphicpsi - sphispsi, stheta * cphi);
+            z = v3(stheta * spsi, -stheta * cpsi, ctheta);
+        } else {
+            x = v3(-stheta * sphi, ctheta * sphicpsi + cphispsi, cphicpsi - ctheta * sphispsi);
+            y = v3(-stheta * cphi, ctheta * cphicpsi - sphispsi, -sphicpsi - ctheta * cphispsi);
+            z = v3(-ctheta, -stheta * cpsi, stheta * spsi);
+        }
+    }
+    // E313^-1 applied to v (EulerProjectionMatrix, :228-237 and :293-302)
+    static __device__ __forceinline__ V3<R> eproj(const Cache& c, V3<R> v) {
+        const R ctheta = c.C[1], cpsi = c.C[2], spsi = c.S[2], csc = c.csc;
+        if (!c.br)
+            return v3(spsi * csc * v.x - cpsi * csc * v.y, cpsi * v.x + spsi * v.y,
+                      -(ctheta * spsi) * csc * v.x + (ctheta * cpsi) * csc * v.y + v.z);
+        return v3(-cpsi * csc * v.y + spsi * csc * v.z, spsi * v.y + cpsi * v.z,
+                  -v.x + (ctheta * cpsi) * csc * v.y - (ctheta * spsi) * csc * v.z);
+    }
+    // spherical projection (:324-329 and :354-359), 2 rows applied to v
+    static __device__ __forceinline__ void sproj(const Cache& c, V3<R> v, R* o) {
+        const R ct = c.C[3], cp = c.C[4], sp = c.S[4], od = c.odst;
+        if (!c.nr) {
+            o[0] = -sp * v.x + cp * v.y;
+            o[1] = -(cp * ct * od) * v.x - (sp * ct * od) * v.y + v.z;
+        } else {
+            o[0] = cp * v.y - sp * v.z;
+            o[1] = -v.x - (sp * ct * od) * v.y - (cp * ct * od) * v.z;
+        }
+    }
+    // c*Teff: uniaxial (UniaxialAnisotropy.h:146-150) or cubic (CubicAnisotropy.h:162-193)
+    static __device__ __forceinline__ V3<R> ctorque(const Par& q, const Cache& c, V3<R> m, V3<R> x, V3<R> y, V3<R> z) {
+        if constexpr (A == kUniaxial) {
+            return (q.cT * dot(m, z)) * cross(z, m);
+        } else {
+            const R c1 = dot(m, x), c2 = dot(m, y), c3 = dot(m, z);
+            const R c1s = c1 * c1, c2s = c2 * c2;
+            const R ctheta = c.C[1], cpsi = c.C[2], stheta = c.S[1], spsi = c.S[2];
+            const V3<R> th = v3(ctheta * spsi, -ctheta * cpsi, -stheta);
+            const V3<R> sym = cross(z, (c3 * (c1s + c2s)) * m);
+            const V3<R> asdir = (ctheta / stheta) * th + z;
+            return q.cT * (sym + (c1 * c2 * (c2s - c1s)) * asdir);
+        }
+    }
+    static __device__ __forceinline__ void finish(const Rot<R>&, R* y, const Cache& c) {
+        if (c.br) euler_unrotate(y);
+        else { y[0] = M<R>::fmod(y[0], M<R>::two_pi); y[1] = M<R>::fmod(y[1], M<R>::two_pi); y[2] = M<R>::fmod(y[2], M<R>::two_pi); }
+        if (c.nr) neel_unrotate(y + 3);
+        else { y[3] = M<R>::fmod(y[3], M<R>::two_pi); y[4] = M<R>::fmod(y[4], M<R>::two_pi); }
+    }
+    // :363-425
+    static __device__ __forceinline__ void det(const Par& q, const R*, const Cache& c, const R* B, R* a) {
+        V3<R> x, y, z;
+        axes(c, x, y, z);
+        const V3<R> H = Aniso<R, A>::heff(q.pF, c.md, x, y, z, v3(B[0], B[1], B[2]));
+        const V3<R> cTe = ctorque(q, c, c.md, x, y, z);
+        const V3<R> mxH = cross(c.md, H);
+        const V3<R> wb = eproj(c, cTe + q.d * mxH);
+        a[0] = wb.x; a[1] = wb.y; a[2] = wb.z;
+        sproj(c, (-q.a) * H + q.bpd * mxH + cTe, a + 3);
+    }
+    // :427-497 applied to w = (wA, wB)
+    static __device__ __forceinline__ void bdw(const Par& q, const R*, const Cache& c, const R* w, R* r) {
+        const V3<R> wA = v3(w[0], w[1], w[2]), wB = v3(w[3], w[4], w[5]);
+        const V3<R> cwA = q.cF * wA;
+        const V3<R> b = eproj(c, cwA + cross(q.dDN * c.md, wB));
+        r[0] = b.x; r[1] = b.y; r[2] = b.z;
+        sproj(c, cwA + q.bpdDN * cross(c.md, wB) - q.aDN * wB, r + 3);
+    }
+    // :499-601 with the prefactors grouped: adDN2 = a d DN^2, d2fDN2 = d^2 DN^2 / 4, cF2h = (c DB)^2 / 2
+    static __device__ __forceinline__ void drift(const Par& q, const R* y, const Cache& c, R* r) {
+        const R ctheta = c.C[1], cpsi = c.C[2], spsi = c.S[2];
+        const R cos_t = c.C[3], cos_p = c.C[4], sin_t = c.S[3], sin_p = c.S[4];
+        const R csc = c.csc;
+        const R cotb = csc * ctheta;
+        if (c.br == c.nr) {
+            const R cos_2t = cos_t * cos_t - sin_t * sin_t;
+            const R sin_2t = R(2) * cos_t * sin_t;
+            const R sin_t_2 = sin_t * sin_t;
+            const R cph = cos_p * cpsi + spsi * sin_p;
+            const R sph = cpsi * sin_p - cos_p * spsi;
+            R s2, c2;
+            M<R>::sincos(R(2) * (y[4] - y[2]), &s2, &c2);
+            r[0] = csc * sin_t * (q.adDN2 * sph - R(2) * q.d2fDN2 * (cos_t * cph + cotb * sin_t * s2));
+            r[1] = q.cF2h * cotb - q.adDN2 * (cph * sin_t) +
+                   q.d2fDN2 * (R(0.5) * (R(3) + cos_2t + R(2) * c2 * sin_t_2) * cotb - sin_2t * sph);
+            r[2] = -(q.adDN2 * (cos_t + sin_t * cotb * sph) -
+                     q.d2fDN2 * sin_t * (R(2) * cos_t * cotb * cph + (R(-1) + R(2) * csc * csc) * sin_t * s2));
+        } else {
+            const R sin_2t = R(2) * cos_t * sin_t;
+            const R sin_t_2 = sin_t * sin_t;
+            const R cpsi_2 = cpsi * cpsi, spsi_2 = spsi * spsi;
+            const R c2psi = cpsi_2 - spsi_2, s2psi = R(2) * cpsi * spsi;
+            const R sin_2p = R(2) * cos_p * sin_p;
+            const R cos_t_2 = cos_t * cos_t, sin_p_2 = sin_p * sin_p, cos_p_2 = cos_p * cos_p;
+            if (c.br) {  // :559-576
+                r[0] = csc * (q.adDN2 * (-spsi * cos_t + sin_p * cpsi * sin_t) +
+                              R(2) * q.d2fDN2 * (-c2psi * cotb * sin_2t * sin_p + cos_p * sin_t * (cos_t * cpsi + sin_t * sin_p * spsi) +
+                                                 cotb * s2psi * (cos_t_2 - sin_t_2 * sin_p_2)));
+                r[1] = q.cF2h * cotb + q.adDN2 * (-cos_t * cpsi - spsi * sin_t * sin_p) +
+                       q.d2fDN2 * (R(2) * cpsi_2 * cotb * (cos_t_2 + cos_p_2 * sin_t_2) + cpsi * sin_t_2 * sin_2p +
+                                   R(2) * spsi * (-sin_t * cos_t * cos_p + cotb * sin_t_2 * spsi) + cotb * sin_2t * sin_p * s2psi);
+                r[2] = q.adDN2 * (sin_t * cos_p - cpsi * cotb * sin_t * sin_p + cotb * cos_t * spsi) -
+                       q.d2fDN2 * (cos_t * cpsi + sin_t * sin_p * spsi) *
+                           (R(2) * cos_p * cotb * sin_t - (R(3) + c2psi) * csc * csc * (cpsi * sin_t * sin_p - cos_t * spsi));
+            } else {  // only Neel rotated, :577-594
+                r[0] = csc * (q.adDN2 * (spsi * cos_t + sin_p * cpsi * sin_t) +
+                              R(2) * q.d2fDN2 * (c2psi * cotb * sin_2t * sin_p + cos_p * sin_t * (cos_t * cpsi - sin_t * sin_p * spsi) +
+                                                 cotb * s2psi * (cos_t_2 - sin_t_2 * sin_p_2)));
+                r[1] = q.cF2h * cotb + q.adDN2 * (cos_t * cpsi - spsi * sin_t * sin_p) +
+                       q.d2fDN2 * (R(2) * cpsi_2 * cotb * (cos_t_2 + cos_p_2 * sin_t_2) - cpsi * sin_t_2 * sin_2p +
+                                   R(2) * spsi * (-sin_t * cos_t * cos_p + cotb * sin_t_2 * spsi) - cotb * sin_2t * sin_p * s2psi);
+                r[2] = q.adDN2 * (-sin_t * cos_p - cpsi * cotb * sin_t * sin_p - cotb * cos_t * spsi) -
+                       q.d2fDN2 * (cos_t * cpsi - sin_t * sin_p * spsi) *
+                           (R(2) * cos_p * cotb * sin_t + (R(3) + c2psi) * csc * csc * (cpsi * sin_t * sin_p + cos_t * spsi));
+            }
+        }
+        r[3] = q.nd * c.odst * cos_t;  // :597
+        r[4] = R(0);
+    }
+    // :673-735: x-axis, y-axis, magnetisation
+    static __device__ __forceinline__ void out(const R* y, R* o) {
+        R s[5], c[5];
+#pragma unroll
+        for (int i = 0; i < 5; ++i) M<R>::sincos(y[i], &s[i], &c[i]);
+        const R cphicpsi = c[0] * c[2], sphicpsi = s[0] * c[2], cphispsi = c[0] * s[2], sphispsi = s[0] * s[2];
+        o[0] = cphicpsi - c[1] * sphispsi; o[1] = c[1] * sphicpsi + cphispsi; o[2] = s[1] * s[0];
+        o[3] = -sphicpsi - c[1] * cphispsi; o[4] = c[1] * cphicpsi - sphispsi; o[5] = s[1] * c[0];
+        o[6] = s[3] * c[4]; o[7] = s[3] * s[4]; o[8] = c[3];
+    }
+    static __device__ __forceinline__ void newton_matrix(const Par&, const R*, const Cache&, const R*, const R*, R,
+                                                         R S[D][D]) {
+        for (int i = 0; i < D; ++i) for (int j = 0; j < D; ++j) S[i][j] = R(i == j ? -1 : 0);
+    }
+};
+
+// ======================================================================= Brown + Neel (Cartesian)
+template <class R, int A>
+struct BrownNeelCart {
+    static constexpr int D = 6, Mn = 6, OUT = 6;
+    static constexpr bool kHasJacobian = true;  // both Jacobians are zero in the reference (.h:119-128)
+    struct Par {
+        R a, bpd, d, cT, pF, cF, dDN, bpdDN, aDN, cF2, adDN2, hd2DN2, ndrift, cFe;
+    };
+    struct Cache {};
+    static __device__ __forceinline__ Par load(const R* P, unsigned long long Np, unsigned long long p) {
+        Par q;
+        q.a = P[0 * Np + p]; q.bpd = P[1 * Np + p]; q.d = P[2 * Np + p]; q.cT = P[3 * Np + p];
+        q.pF = P[4 * Np + p]; q.cF = P[5 * Np + p]; q.dDN = P[6 * Np + p]; q.bpdDN = P[7 * Np + p];
+        q.aDN = P[8 * Np + p]; q.cF2 = P[9 * Np + p]; q.adDN2 = P[10 * Np + p]; q.hd2DN2 = P[11 * Np + p];
+        q.ndrift = P[12 * Np + p]; q.cFe = P[13 * Np + p];
+        return q;
+    }
+    static __device__ __forceinline__ void prepare(const Par&, const Rot<R>&, R*, Cache&) {}
+    static __device__ __forceinline__ void recompute(const Par&, const R*, Cache&) {}
+    static __device__ __forceinline__ void finish(const Rot<R>&, R*, const Cache&) {}
+    // .inl:222-271 (the reference returns zero for cubic anisotropy, .inl:225-229)
+    static __device__ __forceinline__ void det(const Par& q, const R* y, const Cache&, const R* B, R* a) {
+        if constexpr (A == kCubic) {
+            for (int i = 0; i < 6; ++i) a[i] = R(0);
+        } else {
+            const V3<R> n = v3(y[0], y[1], y[2]), e = v3(y[3], y[4], y[5]);
+            const R en = dot(e, n);
+            const V3<R> H = (q.pF * en) * n + v3(B[0], B[1], B[2]);
+            const V3<R> cTe = (q.cT * en) * cross(n, e);
+            const V3<R> mxH = cross(e, H);
+            const V3<R> br = cross(cTe + q.d * mxH, n);
+            const V3<R> ne = cross((-q.a) * H + q.bpd * mxH + cTe, e);
+            a[0] = br.x; a[1] = br.y; a[2] = br.z; a[3] = ne.x; a[4] = ne.y; a[5] = ne.z;
+        }
+    }
+    // .inl:40-170 applied to w = (wA, wB)
+    static __device__ __forceinline__ void bdw(const Par& q, const R* y, const Cache&, const R* w, R* r) {
+        const V3<R> n = v3(y[0], y[1], y[2]), e = v3(y[3], y[4], y[5]);
+        const V3<R> wA = v3(w[0], w[1], w[2]), wB = v3(w[3], w[4], w[5]);
+        const V3<R> br = (-q.cF) * cross(n, wA) + q.dDN * (dot(n, e) * wB - dot(n, wB) * e);
+        const V3<R> ne = (-q.cFe) * cross(e, wA) + q.bpdDN * (wB - dot(e, wB) * e) + q.aDN * cross(e, wB);
+        r[0] = br.x; r[1] = br.y; r[2] = br.z; r[3] = ne.x; r[4] = ne.y; r[5] = ne.z;
+    }
+    // .inl:179-219
+    static __device__ __forceinline__ void drift(const Par& q, const R* y, const Cache&, R* r) {
+        const V3<R> n = v3(y[0], y[1], y[2]), e = v3(y[3], y[4], y[5]);
+        const V3<R> br = (-q.cF2) * n + q.adDN2 * cross(n, e) - q.hd2DN2 * (dot(e, e) * n - n);
+        const V3<R> ne = (-q.ndrift) * e;
+        r[0] = br.x; r[1] = br.y; r[2] = br.z; r[3] = ne.x; r[4] = ne.y; r[5] = ne.z;
+    }
+    static __device__ __forceinline__ void out(const R* y, R* o) {
+#pragma unroll
+        for (int i = 0; i < 6; ++i) o[i] = y[i];
+    }
+    static __device__ __forceinline__ void newton_matrix(const Par&, const R*, const Cache&, const R*, const R*, R,
+                                                         R S[D][D]) {
+        for (int i = 0; i < D; ++i) for (int j = 0; j < D; ++j) S[i][j] = R(i == j ? -1 : 0);
+    }
+};
+
+// ======================================================================= steppers
+struct NewtonCount {
+    unsigned int iterations, unconverged;
+};
+
+// Gaussian elimination with partial pivoting (D <= 3; larger systems here are -I)
+template <class R, int D>
+__device__ __forceinline__ bool solve_small(R A[D][D], R* b, R* x) {
+#pragma unroll
+    for (int k = 0; k < D; ++k) {
+        int piv = k;
+#pragma unroll
+        for (int i = k + 1; i < D; ++i)
+            if (M<R>::abs(A[i][k]) > M<R>::abs(A[piv][k])) piv = i;
+        if (A[piv][k] == R(0)) return false;
+        if (piv != k) {
+#pragma unroll
+            for (int j = 0; j < D; ++j) { const R t = A[k][j]; A[k][j] = A[piv][j]; A[piv][j] = t; }
+            const R t = b[k]; b[k] = b[piv]; b[piv] = t;
+        }
+#pragma unroll
+        for (int i = k + 1; i < D; ++i) {
+            const R f = A[i][k] / A[k][k];
+#pragma unroll
+            for (int j = k; j < D; ++j) A[i][j] = A[i][j] - f * A[k][j];
+            b[i] = b[i] - f * b[k];
+        }
+    }
+#pragma unroll
+    for (int i = D - 1; i >= 0; --i) {
+        R s = b[i];
+#pragma unroll
+        for (int j = i + 1; j < D; ++j) s = s - A[i][j] * x[j];
+        x[i] = s / A[i][i];
+    }
+    return true;
+}
+
+template <class P, class R, int SOLVER>
+struct Stepper {
+    static constexpr int D = P::D, Mn = P::Mn;
+    using Par = typename P::Par;
+    using Cache = typename P::Cache;
+
+    static __device__ __forceinline__ void step(const Par& q, const Rot<R>& rot, R* y, const R* B, const R* w, R dt,
+                                                int max_iter, double tol, NewtonCount& nc) {
+        if constexpr (SOLVER == kEulerMaruyama) {
+            Cache c;
+            P::prepare(q, rot, y, c);
+            R a[D], d[D], bw[D];
+            P::det(q, y, c, B, a);
+            P::drift(q, y, c, d);
+            P::bdw(q, y, c, w, bw);
+#pragma unroll
+            for (int i = 0; i < D; ++i) y[i] = y[i] + ((a[i] + d[i]) * dt + bw[i]);
+            P::finish(rot, y, c);
+        } else if constexpr (SOLVER == kHeun) {
+            Cache c;
+            P::prepare(q, rot, y, c);
+            R a1[D], d[D], bw[D], s[D];
+            P::det(q, y, c, B, a1);
+            P::drift(q, y, c, d);
+            P::bdw(q, y, c, w, bw);
+#pragma unroll
+            for (int i = 0; i < D; ++i) {
+                a1[i] = a1[i] + d[i];
+                s[i] = (y[i] + a1[i] * dt) + bw[i];
+            }
+            P::recompute(q, s, c);  // second stage in the chart chosen for y_n
+            R a2[D];
+            P::det(q, s, c, B, a2);
+            P::drift(q, s, c, d);
+#pragma unroll
+            for (int i = 0; i < D; ++i) y[i] = (y[i] + (R(0.5) * ((a2[i] + d[i]) + a1[i])) * dt) + bw[i];
+            P::finish(rot, y, c);
+        } else if constexpr (SOLVER == kMillstein) {
+            Cache c;
+            P::prepare(q, rot, y, c);
+            R a[D], d[D], bw[D];
+            P::det(q, y, c, B, a);
+            P::drift(q, y, c, d);
+            P::bdw(q, y, c, w, bw);
+            R ww = R(0);
+#pragma unroll
+            for (int j = 0; j < Mn; ++j) ww = ww + w[j] * w[j];
+#pragma unroll
+            for (int i = 0; i < D; ++i) y[i] = ((y[i] + a[i] * dt) + bw[i]) + d[i] * ww;
+            P::finish(rot, y, c);
+        } else {
+            if constexpr (P::kHasJacobian) {
+                // Newton on f(yj) = finish(prepare((yj+yn)/2) + a dt + b dW) + yn/2 - 3yj/2,
+                // accepted when |dy| <= tol, evaluated in FP64 (FP32: tol raised to what
+                // the FP32 state can resolve)
+                R yn[D], yj[D];
+#pragma unroll
+                for (int i = 0; i < D; ++i) { yn[i] = y[i]; yj[i] = y[i]; }
+                bool conv = false;
+                for (int it = 0; it < max_iter; ++it) {
+                    R r[D];
+#pragma unroll
+                    for (int i = 0; i < D; ++i) r[i] = (yj[i] + yn[i]) * R(0.5);
+                    Cache c;
+                    P::prepare(q, rot, r, c);
+                    R a[D], bw[D], S[D][D];
+                    P::det(q, r, c, B, a);
+                    P::bdw(q, r, c, w, bw);
+                    P::newton_matrix(q, r, c, B, w, dt, S);
+#pragma unroll
+                    for (int i = 0; i < D; ++i) r[i] = r[i] + (a[i] * dt + bw[i]);
+                    P::finish(rot, r, c);
+                    R rhs[D], dx[D];
+#pragma unroll
+                    for (int i = 0; i < D; ++i) rhs[i] = -(r[i] + (yn[i] * R(0.5) - yj[i] * R(1.5)));
+                    ++nc.iterations;
+                    bool ok;
+                    if constexpr (D > 3) {  // S == -I for the coupled Cartesian problem
+#pragma unroll
+                        for (int i = 0; i < D; ++i) dx[i] = -rhs[i];
+                        ok = true;
+                    } else {
+                        ok = solve_small<R, D>(S, rhs, dx);
+                    }
+                    if (!ok) break;
+                    double n2 = 0.0, y2 = 0.0;
+#pragma unroll
+                    for (int i = 0; i < D; ++i) {
+                        yj[i] = yj[i] + dx[i];
+                        n2 += static_cast<double>(dx[i]) * static_cast<double>(dx[i]);
+                        y2 += static_cast<double>(yj[i]) * static_cast<double>(yj[i]);
+                    }
+                    const double tol_eff = (sizeof(R) == 4) ? fmax(tol, 8.0 * 1.1920929e-7 * ::sqrt(y2)) : tol;
+                    if (::sqrt(n2) <= tol_eff) { conv = true; break; }
+                }
+                if (!conv) ++nc.unconverged;
+#pragma unroll
+                for (int i = 0; i < D; ++i) y[i] = yj[i];
+            }
+        }
+    }
+};
+
+}  // namespace sp

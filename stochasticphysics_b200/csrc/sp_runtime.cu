@@ -1,0 +1,564 @@
+// sp_runtime.cu — host runtime behind include/stophys_b200.h (ensembles, context, C ABI).
+//
+// Host code only; the kernels live in sp_k_*.cu / sp_misc.cu.  Every C entry
+// point catches all C++ exceptions and turns them into an sp_status plus the
+// thread-local text returned by sp_last_error().
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/stophys_b200.h"
+#include "sp_dispatch.h"
+#include "sp_runtime.h"
+
+namespace sp {
+
+thread_local std::string g_last_error;
+std::atomic<unsigned long long> g_launch_count{0};
+
+Error::Error(sp_status s, const std::string& m) : std::runtime_error(m), status(s) {}
+
+void check_cuda(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return;
+    const sp_status s = (e == cudaErrorMemoryAllocation) ? SP_ERR_OUT_OF_MEMORY : SP_ERR_CUDA;
+    throw Error(s, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+sp_status fail(sp_status s, const std::string& msg) {
+    g_last_error = msg;
+    return s;
+}
+
+int state_dim(int p) { return p == 0 ? 3 : p == 1 ? 2 : p == 2 ? 5 : 6; }
+int noise_dim(int p) { return (p == 0 || p == 1) ? 3 : 6; }
+int out_dim(int p) { return p == 0 ? 3 : p == 1 ? 3 : p == 2 ? 9 : 6; }
+int param_count(int p) {
+    return p == 0 ? kParamsNeel : p == 1 ? kParamsNeelSph : p == 2 ? kParamsBrownNeelEuler : kParamsBrownNeel;
+}
+
+// ------------------------------------------------------------------ validation
+sp_status validate_desc(const sp_ensemble_desc* d, std::string& why) {
+    auto bad = [&](const std::string& m) { why = m; return SP_ERR_INVALID_ARG; };
+    if (!d) return bad("description is NULL");
+    if (d->abi_version != SP_ABI_VERSION) return bad("abi_version mismatch");
+    if (d->problem < 0 || d->problem > 3) return bad("unknown problem");
+    if (d->anisotropy < 0 || d->anisotropy > 1) return bad("unknown anisotropy");
+    if (d->solver < 0 || d->solver > 3) return bad("unknown solver");
+    if (d->precision < 0 || d->precision > 1) return bad("unknown precision");
+    if (d->noise < 0 || d->noise > 1) return bad("unknown noise mode");
+    if (d->field.type < 0 || d->field.type > 3) return bad("unknown field type");
+    if (d->n_particles == 0) return bad("n_particles must be > 0");
+    if (d->n_particles > (1ull << 31)) return bad("n_particles exceeds 2^31");
+    if (d->oversampling == 0) return bad("oversampling must be > 0");
+    if (d->number_of_steps < d->oversampling) return bad("number_of_steps must be >= oversampling");
+    if (!(d->timestep > 0.0) || !std::isfinite(d->timestep)) return bad("timestep must be finite and > 0");
+    if (!(d->temperature >= 0.0) || !std::isfinite(d->temperature)) return bad("temperature must be finite and >= 0");
+    const sp_particles& q = d->particles;
+    if (!q.magnetic_radius || !q.saturation_magnetisation || !q.damping_constant || !q.gyromagnetic_ratio ||
+        !q.anisotropy_constant || !q.orientation || !q.magnetisation)
+        return bad("a required per-particle array is NULL");
+    if ((d->problem == SP_PROBLEM_BROWN_AND_NEEL || d->problem == SP_PROBLEM_BROWN_AND_NEEL_EULER_SPHERICAL) &&
+        (!q.hydrodynamic_radius || !q.viscosity))
+        return bad("Brown problems need hydrodynamic_radius and viscosity");
+    if (d->noise == SP_NOISE_INJECTED && !d->injected_dw) return bad("injected noise mode needs injected_dw");
+    if (d->solver == SP_SOLVER_IMPLICIT_MIDPOINT) {
+        if (d->problem == SP_PROBLEM_BROWN_AND_NEEL_EULER_SPHERICAL) {
+            why = "ImplicitMidpoint needs Jacobians, which BrownAndNeelEulerSpherical does not provide";
+            return SP_ERR_UNSUPPORTED_COMBO;
+        }
+        if (d->max_iteration < 1 || d->max_iteration > 1000) return bad("ImplicitMidpoint needs 1 <= max_iteration <= 1000");
+        if (!(d->accuracy_goal > 0.0)) return bad("ImplicitMidpoint needs accuracy_goal > 0");
+    }
+    const unsigned long long K = d->number_of_steps / d->oversampling;
+    if (K > (1ull << 31)) return bad("too many samples");
+    return SP_OK;
+}
+
+// ------------------------------------------------------------------ launch heuristics
+LaunchConfig default_launch(const sp_context* ctx, const sp_ensemble_desc& d) {
+    LaunchConfig c;
+    const int sms = ctx ? ctx->sms : 148;
+    int block = 256;
+    const unsigned long long n = d.n_particles;
+    while (block > 32 && (n + block - 1) / block < static_cast<unsigned long long>(2 * sms)) block >>= 1;
+    c.block = block;
+    c.persistent = 0;
+    const unsigned long long W = d.oversampling;
+    const unsigned long long target = 10000;
+    c.chunk = W >= target ? W : (target / W) * W;
+    return c;
+}
+
+// ------------------------------------------------------------------ ensemble
+static unsigned long long round_up(unsigned long long x, unsigned long long m) { return (x + m - 1) / m * m; }
+
+EnsembleLayout layout_of(const sp_ensemble_desc& d, const LaunchConfig& lc) {
+    EnsembleLayout L;
+    L.D = state_dim(d.problem);
+    L.Mn = noise_dim(d.problem);
+    L.OUT = out_dim(d.problem);
+    L.P = param_count(d.problem);
+    L.real = d.precision == SP_PRECISION_FP32 ? 4 : 8;
+    L.n = d.n_particles;
+    L.Np = round_up(L.n, kPad);
+    L.W = d.oversampling;
+    L.K = d.number_of_steps / d.oversampling;
+    L.S = (L.K - 1) * L.W;
+    L.chunk = std::max<unsigned long long>(1, std::min<unsigned long long>(lc.chunk, std::max<unsigned long long>(L.S, 1)));
+    L.slots = static_cast<int>(L.chunk / L.W + 2);
+    const unsigned long long nw = L.Np / 32;
+    L.bytes = L.Np * (L.D + 2ull * L.OUT + L.P) * L.real + L.Np * 8 + L.Np + nw * L.slots * L.OUT * 8 +
+              L.K * L.OUT * 8 + L.OUT * 8 + L.K * 3 * 8 + L.chunk * 3 * L.real + sizeof(EnsCtl) + sizeof(EnsDev) +
+              ((L.Np + 31) / 32 + 1) * sizeof(TileDesc);
+    if (d.record_trajectories) L.bytes += L.K * L.OUT * L.Np * 8;
+    if (d.noise == SP_NOISE_INJECTED) L.bytes += L.S * L.Mn * L.Np * L.real;
+    return L;
+}
+
+void* Ensemble::dalloc(size_t bytes) {
+    void* p = nullptr;
+    check_cuda(cudaMalloc(&p, std::max<size_t>(bytes, 16)), "cudaMalloc");
+    allocs.push_back(p);
+    return p;
+}
+
+Ensemble::Ensemble(sp_context* c, const sp_ensemble_desc& d, const LaunchConfig& lc) : ctx(c), desc(d), launch(lc) {
+    ks = &kernel_set(d.problem, d.anisotropy, d.solver, d.precision, d.noise == SP_NOISE_INJECTED ? 1 : 0);
+    if (!ks->valid) throw Error(SP_ERR_UNSUPPORTED_COMBO, "no kernel for this problem/solver combination");
+    L = layout_of(d, lc);
+    check_cuda(cudaSetDevice(ctx->device), "cudaSetDevice");
+    check_cuda(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    check_cuda(cudaEventCreate(&ev0), "cudaEventCreate");
+    check_cuda(cudaEventCreate(&ev1), "cudaEventCreate");
+
+    const size_t R = L.real;
+    d_state = dalloc(L.Np * L.D * R);
+    d_ksum = dalloc(L.Np * L.OUT * R);
+    d_kcomp = dalloc(L.Np * L.OUT * R);
+    d_params = dalloc(L.Np * L.P * R);
+    d_moment = static_cast<double*>(dalloc(L.Np * 8));
+    d_status = static_cast<unsigned char*>(dalloc(L.Np));
+    d_partial = static_cast<double*>(dalloc((L.Np / 32) * L.slots * L.OUT * 8));
+    d_msum = static_cast<double*>(dalloc(L.K * L.OUT * 8));
+    d_wsum = static_cast<double*>(dalloc(L.OUT * 8));
+    d_field = static_cast<double*>(dalloc(L.K * 3 * 8));
+    d_ftab = dalloc(L.chunk * 3 * R);
+    d_ctl = static_cast<EnsCtl*>(dalloc(sizeof(EnsCtl)));
+    d_ens = static_cast<EnsDev*>(dalloc(sizeof(EnsDev)));
+    if (d.record_trajectories) d_traj = static_cast<double*>(dalloc(L.K * L.OUT * L.Np * 8));
+    check_cuda(cudaMemsetAsync(d_msum, 0, L.K * L.OUT * 8, stream), "memset");
+    check_cuda(cudaMemsetAsync(d_ctl, 0, sizeof(EnsCtl), stream), "memset");
+
+    // injected increments: [S][M][n] FP64 host -> [S][M][Np] Real device
+    if (d.noise == SP_NOISE_INJECTED && L.S > 0) {
+        d_dw = dalloc(L.S * L.Mn * L.Np * R);
+        const size_t rows = L.S * L.Mn;
+        std::vector<unsigned char> host(rows * L.Np * R, 0);
+        for (size_t r = 0; r < rows; ++r) {
+            const double* src = d.injected_dw + r * L.n;
+            if (R == 8) {
+                std::memcpy(host.data() + r * L.Np * 8, src, L.n * 8);
+            } else {
+                float* dst = reinterpret_cast<float*>(host.data() + r * L.Np * 4);
+                for (size_t i = 0; i < L.n; ++i) dst[i] = static_cast<float>(src[i]);
+            }
+        }
+        check_cuda(cudaMemcpyAsync(d_dw, host.data(), host.size(), cudaMemcpyHostToDevice, stream), "upload dW");
+        check_cuda(cudaStreamSynchronize(stream), "sync");
+    }
+
+    // device descriptor
+    EnsDev& e = hdev;
+    std::memset(&e, 0, sizeof(e));
+    e.n = L.n; e.Np = L.Np; e.K = L.K; e.W = L.W; e.S = L.S; e.chunk = L.chunk;
+    e.seed = d.seed; e.pid_offset = d.particle_id_offset;
+    e.dt = d.timestep; e.sqrt_dt = std::sqrt(d.timestep);
+    e.field = field_params(d.field);
+    e.max_iter = d.max_iteration; e.tol = d.accuracy_goal;
+    const double kPi = 3.14159265358979323846;
+    if (d.problem == SP_PROBLEM_NEEL_SPHERICAL) {
+        e.rot_brown = d.problem_settings.use_coordinate_transformation;
+        e.min1 = d.problem_settings.min_angle_before_transformation;
+        e.max1 = kPi - e.min1;
+    } else if (d.problem == SP_PROBLEM_BROWN_AND_NEEL_EULER_SPHERICAL) {
+        e.rot_brown = d.problem_settings.use_euler_coordinate_transformation;
+        e.rot_neel = d.problem_settings.use_spherical_coordinate_transformation;
+        e.min1 = d.problem_settings.brown_min_angle_before_transformation;
+        e.max1 = kPi - e.min1;
+        e.min2 = d.problem_settings.neel_min_angle_before_transformation;
+        e.max2 = kPi - e.min2;
+    }
+    e.slots = L.slots;
+    e.state = d_state; e.ksum = d_ksum; e.kcomp = d_kcomp; e.params = d_params; e.moment = d_moment;
+    e.dw = d_dw; e.partial = d_partial; e.msum = d_msum; e.wsum = d_wsum; e.traj = d_traj; e.ftab = d_ftab;
+    e.status = d_status; e.ctl = d_ctl;
+    check_cuda(cudaMemcpyAsync(d_ens, &e, sizeof(EnsDev), cudaMemcpyHostToDevice, stream), "upload EnsDev");
+
+    // tiles
+    block = launch.block;
+    ntiles = static_cast<int>((L.n + block - 1) / block);
+    std::vector<TileDesc> tiles(ntiles);
+    for (int t = 0; t < ntiles; ++t) tiles[t] = TileDesc{0u, static_cast<unsigned>(t * block)};
+    d_tiles = static_cast<TileDesc*>(dalloc(tiles.size() * sizeof(TileDesc)));
+    check_cuda(cudaMemcpyAsync(d_tiles, tiles.data(), tiles.size() * sizeof(TileDesc), cudaMemcpyHostToDevice, stream),
+               "upload tiles");
+    grid = ntiles;
+    if (launch.persistent) {
+        int per_sm = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ks->step_fn, block, 0);
+        grid = std::min(ntiles, std::max(1, per_sm) * ctx->sms);
+    }
+
+    // raw particle properties -> init kernel
+    upload_and_init(d);
+    build_graph();
+    check_cuda(cudaStreamSynchronize(stream), "ensemble init");
+}
+
+FieldParams field_params(const sp_field_desc& f) {
+    FieldParams p;
+    std::memset(&p, 0, sizeof(p));
+    p.type = f.type;
+    const double two_pi = 6.28318530717958647692;  // math::constants::two_pi (SinusoidalField.h:39)
+    for (int i = 0; i < 3; ++i) {
+        p.offset[i] = f.offset[i];
+        p.amplitude[i] = f.amplitude[i];
+        p.omega[i] = two_pi * (f.type == SP_FIELD_SINUSOIDAL ? f.frequency[0] : f.frequency[i]);
+        p.phase[i] = f.type == SP_FIELD_SINUSOIDAL ? f.phase[0] : f.phase[i];
+    }
+    return p;
+}
+
+void Ensemble::upload_and_init(const sp_ensemble_desc& d) {
+    const size_t n = L.n;
+    const sp_particles& q = d.particles;
+    const bool brown = d.problem == SP_PROBLEM_BROWN_AND_NEEL || d.problem == SP_PROBLEM_BROWN_AND_NEEL_EULER_SPHERICAL;
+    // one staging buffer: 7 scalars + 6 vector components per particle
+    std::vector<double> host(n * 13, 0.0);
+    const double* src[7] = {q.magnetic_radius, q.saturation_magnetisation, q.damping_constant, q.gyromagnetic_ratio,
+                            q.anisotropy_constant, brown ? q.hydrodynamic_radius : nullptr, brown ? q.viscosity : nullptr};
+    for (int k = 0; k < 7; ++k)
+        if (src[k]) std::memcpy(host.data() + k * n, src[k], n * 8);
+    std::memcpy(host.data() + 7 * n, q.orientation, n * 24);
+    std::memcpy(host.data() + 10 * n, q.magnetisation, n * 24);
+    double* dev = nullptr;
+    check_cuda(cudaMallocAsync(reinterpret_cast<void**>(&dev), host.size() * 8, stream), "cudaMallocAsync");
+    check_cuda(cudaMemcpyAsync(dev, host.data(), host.size() * 8, cudaMemcpyHostToDevice, stream), "upload particles");
+    h2d_bytes += host.size() * 8;
+    RawParticles rp;
+    rp.radius = dev; rp.Ms = dev + n; rp.alpha = dev + 2 * n; rp.gamma = dev + 3 * n; rp.K = dev + 4 * n;
+    rp.rh = dev + 5 * n; rp.viscosity = dev + 6 * n; rp.euler = dev + 7 * n; rp.mag = dev + 10 * n;
+    rp.temperature = d.temperature;
+    rp.simple_model = d.problem_settings.use_simple_model;
+    ks->init(d_ens, rp, L.Np, stream);
+    ks->reduce(d_ens, 1, 2, 1, stream);
+    launch_field_window(hdev.field, d.timestep, L.W, L.K, d_field, stream);
+    check_cuda(cudaGetLastError(), "init kernels");
+    launches += 3;
+    g_launch_count += 3;
+    check_cuda(cudaFreeAsync(dev, stream), "cudaFreeAsync");
+    // the host staging buffer must outlive the asynchronous copy
+    check_cuda(cudaStreamSynchronize(stream), "init");
+}
+
+void Ensemble::enqueue_chunk(cudaStream_t s) {
+    const int midpoint = desc.solver == SP_SOLVER_IMPLICIT_MIDPOINT ? 1 : 0;
+    ks->field(d_ens, 1, L.chunk, midpoint, s);
+    ks->step(d_ens, d_tiles, ntiles, grid, block, s);
+    ks->reduce(d_ens, 1, L.slots, 0, s);
+    launch_commit(d_ens, 1, s);
+}
+
+void Ensemble::build_graph() {
+    cudaStream_t cs;
+    check_cuda(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking), "capture stream");
+    check_cuda(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal), "begin capture");
+    enqueue_chunk(cs);
+    cudaGraph_t g = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(cs, &g);
+    cudaStreamDestroy(cs);
+    check_cuda(ce, "end capture");
+    graph = g;
+    check_cuda(cudaGraphInstantiate(&gexec, graph, 0), "graph instantiate");
+}
+
+void Ensemble::advance(unsigned long long nsteps, cudaStream_t s) {
+    if (!s) s = stream;
+    const unsigned long long target = std::min(steps_done + nsteps, L.S);
+    if (target <= steps_done) return;
+    launch_set_target(d_ctl, target, s);
+    const unsigned long long nchunks = (target - steps_done + L.chunk - 1) / L.chunk;
+    check_cuda(cudaEventRecord(ev0, s), "event");
+    for (unsigned long long i = 0; i < nchunks; ++i) check_cuda(cudaGraphLaunch(gexec, s), "graph launch");
+    check_cuda(cudaEventRecord(ev1, s), "event");
+    pending_timing = true;
+    launches += 1 + 4 * nchunks;
+    g_launch_count += 1 + 4 * nchunks;
+    particle_steps += (target - steps_done) * L.n;
+    steps_done = target;
+    last_stream = s;
+}
+
+void Ensemble::synchronize() {
+    if (last_stream) check_cuda(cudaStreamSynchronize(last_stream), "synchronize");
+    check_cuda(cudaStreamSynchronize(stream), "synchronize");
+    if (pending_timing) {
+        float ms = 0.f;
+        check_cuda(cudaEventElapsedTime(&ms, ev0, ev1), "event time");
+        device_ms += ms;
+        pending_timing = false;
+    }
+}
+
+// Simulator/SingleParticleSimulator.h:236-273 (times of the samples)
+void reference_times(unsigned long long K, unsigned long long W, double dt, double* times) {
+    if (K == 0) return;
+    double start = 0.0, end = 0.0;
+    const double timeshift = dt * static_cast<double>(W) * 0.5;
+    times[0] = start;
+    unsigned long long counter = 0;
+    for (unsigned long long k = 1; k < K; ++k) {
+        start = end + dt;
+        counter += W;
+        end = dt * static_cast<double>(counter) + start;
+        times[k] = (end - start) - timeshift;
+    }
+}
+
+void Ensemble::read(sp_result* out, sp_stats* st) {
+    synchronize();
+    const int OUT = L.OUT;
+    std::vector<double> msum(L.K * OUT), wsum(OUT);
+    check_cuda(cudaMemcpy(msum.data(), d_msum, msum.size() * 8, cudaMemcpyDeviceToHost), "read msum");
+    check_cuda(cudaMemcpy(wsum.data(), d_wsum, OUT * 8, cudaMemcpyDeviceToHost), "read wsum");
+    d2h_bytes += (msum.size() + OUT) * 8;
+    if (out) {
+        if (out->mean) {
+            // MeanSimulationResult::normalize (Results/MeanSimulationResult.h:63-75)
+            bool allzero = true;
+            for (int c = 0; c < OUT; ++c) allzero = allzero && wsum[c] == 0.0;
+            for (size_t k = 0; k < L.K; ++k)
+                for (int c = 0; c < OUT; ++c) out->mean[k * OUT + c] = allzero ? msum[k * OUT + c] : msum[k * OUT + c] / wsum[c];
+        }
+        if (out->weight) std::memcpy(out->weight, wsum.data(), OUT * 8);
+        if (out->time) reference_times(L.K, L.W, desc.timestep, out->time);
+        if (out->field) {
+            check_cuda(cudaMemcpy(out->field, d_field, L.K * 3 * 8, cudaMemcpyDeviceToHost), "read field");
+            d2h_bytes += L.K * 3 * 8;
+        }
+        if (out->trajectories) {
+            if (!d_traj) throw Error(SP_ERR_INVALID_ARG, "trajectories were not recorded (record_trajectories = 0)");
+            std::vector<double> t(L.K * OUT * L.Np);
+            check_cuda(cudaMemcpy(t.data(), d_traj, t.size() * 8, cudaMemcpyDeviceToHost), "read traj");
+            d2h_bytes += t.size() * 8;
+            for (size_t p = 0; p < L.n; ++p)
+                for (size_t k = 0; k < L.K; ++k)
+                    for (int c = 0; c < OUT; ++c) out->trajectories[(p * L.K + k) * OUT + c] = t[(k * OUT + c) * L.Np + p];
+        }
+        if (out->final_state) {
+            std::vector<unsigned char> s(L.D * L.Np * L.real);
+            check_cuda(cudaMemcpy(s.data(), d_state, s.size(), cudaMemcpyDeviceToHost), "read state");
+            d2h_bytes += s.size();
+            for (size_t p = 0; p < L.n; ++p)
+                for (int i = 0; i < L.D; ++i)
+                    out->final_state[p * L.D + i] =
+                        L.real == 8 ? reinterpret_cast<double*>(s.data())[i * L.Np + p]
+                                    : static_cast<double>(reinterpret_cast<float*>(s.data())[i * L.Np + p]);
+        }
+    }
+    if (st) {
+        std::vector<unsigned char> status(L.Np);
+        check_cuda(cudaMemcpy(status.data(), d_status, L.Np, cudaMemcpyDeviceToHost), "read status");
+        EnsCtl ctl;
+        check_cuda(cudaMemcpy(&ctl, d_ctl, sizeof(ctl), cudaMemcpyDeviceToHost), "read ctl");
+        std::memset(st, 0, sizeof(*st));
+        st->particle_steps = particle_steps;
+        for (size_t p = 0; p < L.n; ++p) st->nonfinite_particles += status[p] != 0;
+        st->newton_iterations = ctl.newton_iterations;
+        st->newton_unconverged = ctl.newton_unconverged;
+        st->kernel_launches = launches;
+        st->device_ms = device_ms;
+    }
+}
+
+Ensemble::~Ensemble() {
+    if (last_stream) cudaStreamSynchronize(last_stream);
+    if (stream) cudaStreamSynchronize(stream);
+    if (gexec) cudaGraphExecDestroy(gexec);
+    if (graph) cudaGraphDestroy(graph);
+    for (void* p : allocs) cudaFree(p);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (stream) cudaStreamDestroy(stream);
+}
+
+}  // namespace sp
+
+using namespace sp;
+
+// ====================================================================== C ABI
+#define SP_GUARD_BEGIN try {
+#define SP_GUARD_END                                                   \
+    }                                                                  \
+    catch (const Error& e) { return fail(e.status, e.what()); }        \
+    catch (const std::bad_alloc&) { return fail(SP_ERR_OUT_OF_MEMORY, "host allocation failed"); } \
+    catch (const std::exception& e) { return fail(SP_ERR_CUDA, e.what()); }
+
+extern "C" {
+
+const char* sp_last_error(void) { return g_last_error.c_str(); }
+uint32_t sp_abi_version(void) { return SP_ABI_VERSION; }
+uint64_t sp_kernel_launch_count(void) { return g_launch_count.load(); }
+
+sp_status sp_query_dims(int32_t problem, int32_t* sd, int32_t* nd, int32_t* od) {
+    if (problem < 0 || problem > 3) return fail(SP_ERR_INVALID_ARG, "unknown problem");
+    if (sd) *sd = state_dim(problem);
+    if (nd) *nd = noise_dim(problem);
+    if (od) *od = out_dim(problem);
+    return SP_OK;
+}
+
+sp_status sp_validate(const sp_ensemble_desc* desc) {
+    std::string why;
+    const sp_status s = validate_desc(desc, why);
+    return s == SP_OK ? SP_OK : fail(s, why);
+}
+
+sp_status sp_create(sp_context** out, int32_t device) {
+    SP_GUARD_BEGIN
+    if (!out) return fail(SP_ERR_INVALID_ARG, "ctx pointer is NULL");
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) return fail(SP_ERR_NO_DEVICE, "no CUDA device");
+    if (device < 0 || device >= count) return fail(SP_ERR_INVALID_ARG, "device index out of range");
+    check_cuda(cudaSetDevice(device), "cudaSetDevice");
+    auto* c = new sp_context();
+    c->device = device;
+    cudaDeviceProp prop;
+    check_cuda(cudaGetDeviceProperties(&prop, device), "cudaGetDeviceProperties");
+    c->sms = prop.multiProcessorCount;
+    c->total_mem = prop.totalGlobalMem;
+    c->cc_major = prop.major;
+    c->cc_minor = prop.minor;
+    check_cuda(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    *out = c;
+    return SP_OK;
+    SP_GUARD_END
+}
+
+sp_status sp_destroy(sp_context* ctx) {
+    SP_GUARD_BEGIN
+    if (!ctx) return SP_OK;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return SP_OK;
+    SP_GUARD_END
+}
+
+sp_status sp_ensemble_footprint(const sp_ensemble_desc* desc, uint64_t* bytes) {
+    SP_GUARD_BEGIN
+    std::string why;
+    const sp_status s = validate_desc(desc, why);
+    if (s != SP_OK) return fail(s, why);
+    if (bytes) *bytes = layout_of(*desc, default_launch(nullptr, *desc)).bytes;
+    return SP_OK;
+    SP_GUARD_END
+}
+
+sp_status sp_ensemble_create(sp_context* ctx, const sp_ensemble_desc* desc, sp_ensemble** ens) {
+    SP_GUARD_BEGIN
+    if (!ctx || !ens) return fail(SP_ERR_INVALID_ARG, "NULL argument");
+    std::string why;
+    const sp_status s = validate_desc(desc, why);
+    if (s != SP_OK) return fail(s, why);
+    auto* e = new Ensemble(ctx, *desc, launch_config_for(ctx, *desc));
+    *ens = reinterpret_cast<sp_ensemble*>(e);
+    return SP_OK;
+    SP_GUARD_END
+}
+
+sp_status sp_ensemble_advance(sp_ensemble* ens, uint64_t n_steps, void* cuda_stream) {
+    SP_GUARD_BEGIN
+    if (!ens) return fail(SP_ERR_INVALID_ARG, "NULL ensemble");
+    auto* e = reinterpret_cast<Ensemble*>(ens);
+    check_cuda(cudaSetDevice(e->ctx->device), "cudaSetDevice");
+    e->advance(n_steps, static_cast<cudaStream_t>(cuda_stream));
+    check_cuda(cudaGetLastError(), "advance");
+    return SP_OK;
+    SP_GUARD_END
+}
+
+sp_status sp_ensemble_steps_done(const sp_ensemble* ens, uint64_t* done, uint64_t* total) {
+    if (!ens) return fail(SP_ERR_INVALID_ARG, "NULL ensemble");
+    auto* e = reinterpret_cast<const Ensemble*>(ens);
+    if (done) *done = e->steps_done;
+    if (total) *total = e->L.S;
+    return SP_OK;
+}
+
+sp_status sp_ensemble_read(sp_ensemble* ens, sp_result* out, sp_stats* stats) {
+    SP_GUARD_BEGIN
+    if (!ens) return fail(SP_ERR_INVALID_ARG, "NULL ensemble");
+    auto* e = reinterpret_cast<Ensemble*>(ens);
+    check_cuda(cudaSetDevice(e->ctx->device), "cudaSetDevice");
+    e->read(out, stats);
+    return SP_OK;
+    SP_GUARD_END
+}
+
+sp_status sp_ensemble_destroy(sp_ensemble* ens) {
+    SP_GUARD_BEGIN
+    if (!ens) return SP_OK;
+    auto* e = reinterpret_cast<Ensemble*>(ens);
+    cudaSetDevice(e->ctx->device);
+    delete e;
+    return SP_OK;
+    SP_GUARD_END
+}
+
+sp_status sp_simulate(sp_context* ctx, const sp_ensemble_desc* desc, sp_result* out, sp_stats* stats) {
+    SP_GUARD_BEGIN
+    if (!ctx) return fail(SP_ERR_INVALID_ARG, "NULL context");
+    std::string why;
+    const sp_status s = validate_desc(desc, why);
+    if (s != SP_OK) return fail(s, why);
+    sp_ensemble_desc d = *desc;
+    if (out && out->trajectories) d.record_trajectories = 1;
+    Ensemble e(ctx, d, launch_config_for(ctx, d));
+    e.advance(e.L.S, nullptr);
+    e.read(out, stats);
+    return SP_OK;
+    SP_GUARD_END
+}
+
+sp_status sp_debug_philox_normals(sp_context* ctx, uint64_t seed, uint64_t pid, uint64_t n, uint64_t step0,
+                                  uint64_t nsteps, int32_t noise_dim, int32_t precision, double* out) {
+    SP_GUARD_BEGIN
+    if (!ctx || !out) return fail(SP_ERR_INVALID_ARG, "NULL argument");
+    if (noise_dim != 3 && noise_dim != 6) return fail(SP_ERR_INVALID_ARG, "noise_dim must be 3 or 6");
+    if (precision != 0 && precision != 1) return fail(SP_ERR_INVALID_ARG, "unknown precision");
+    if (n == 0 || nsteps == 0) return SP_OK;
+    check_cuda(cudaSetDevice(ctx->device), "cudaSetDevice");
+    const size_t bytes = n * nsteps * noise_dim * 8;
+    double* d = nullptr;
+    check_cuda(cudaMalloc(&d, bytes), "cudaMalloc");
+    launch_debug_normals(seed, pid, n, step0, nsteps, noise_dim, precision, d, ctx->stream);
+    g_launch_count += 1;
+    cudaError_t e1 = cudaMemcpyAsync(out, d, bytes, cudaMemcpyDeviceToHost, ctx->stream);
+    cudaError_t e2 = cudaStreamSynchronize(ctx->stream);
+    cudaFree(d);
+    check_cuda(e1, "copy normals");
+    check_cuda(e2, "normals kernel");
+    return SP_OK;
+    SP_GUARD_END
+}
+
+}  // extern "C"

@@ -1,0 +1,414 @@
+// sp_server.cu — continuous batching of ensemble simulations on one GPU.
+//
+// Requests arrive through sp_server_submit at any time.  A scheduler thread
+// admits queued requests while their device footprint (state, Philox
+// counters are implicit, FP64 sample buffers, parameters) fits the memory
+// budget, keeps every admitted ensemble's state on the device between chunks,
+// and advances all of them chunk by chunk: admitted ensembles are grouped by
+// kernel key (problem, anisotropy, solver, precision, noise mode) and each
+// group runs ONE batched launch per chunk over a shared work list of particle
+// tiles (step_kernel reads the tile -> ensemble map), captured once per group
+// membership as a CUDA graph.  Groups run on separate streams so different
+// kernels overlap on the device.  Finished ensembles are read back and freed
+// at the next chunk boundary, which makes room for queued requests.
+//
+// Every particle's arithmetic, noise stream and per-warp reduction order are
+// independent of which other ensembles share the launch, so a request's
+// result is bit-identical alone and in any mix.
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+
+#include "sp_runtime.h"
+
+namespace sp {
+
+void launch_bump_targets(const EnsDev* e, int n_ens, cudaStream_t s);
+
+using Clock = std::chrono::steady_clock;
+
+struct Request {
+    uint64_t id = 0;
+    sp_ensemble_desc desc{};
+    std::vector<double> arrays;  // deep copy of every per-particle array and injected dW
+    std::unique_ptr<Ensemble> ens;
+    int state = SP_REQUEST_QUEUED;
+    bool cancel = false;
+    sp_status error = SP_OK;
+    std::string message;
+    uint64_t bytes = 0;
+    Clock::time_point t_submit, t_done;
+    std::vector<double> mean, weight, time, field;
+    sp_stats stats{};
+};
+
+struct Group {
+    const KernelSet* ks = nullptr;
+    std::vector<Request*> members;
+    EnsDev* d_ens = nullptr;
+    TileDesc* d_tiles = nullptr;
+    int ntiles = 0, max_slots = 2, block = 128;
+    unsigned long long max_chunk = 1;
+    cudaStream_t stream = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    bool dirty = true;
+
+    void release() {
+        if (gexec) cudaGraphExecDestroy(gexec);
+        if (graph) cudaGraphDestroy(graph);
+        if (d_ens) cudaFree(d_ens);
+        if (d_tiles) cudaFree(d_tiles);
+        gexec = nullptr; graph = nullptr; d_ens = nullptr; d_tiles = nullptr;
+    }
+};
+
+}  // namespace sp
+
+using namespace sp;
+
+struct sp_server {
+    sp_context* ctx = nullptr;
+    sp_server_config cfg{};
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::thread worker;
+    bool stop = false;
+    uint64_t next_id = 1;
+    uint64_t used_bytes = 0, budget = 0;
+    std::deque<Request*> queue;
+    std::vector<Request*> active;
+    std::unordered_map<uint64_t, std::unique_ptr<Request>> all;
+    std::map<int, Group> groups;  // key -> group
+
+    static int key_of(const sp_ensemble_desc& d) {
+        return (((d.problem * 2 + d.anisotropy) * 4 + d.solver) * 2 + d.precision) * 2 + (d.noise == SP_NOISE_INJECTED);
+    }
+
+    LaunchConfig launch_for(const sp_ensemble_desc& d) const {
+        LaunchConfig c = launch_config_for(ctx, d);
+        if (cfg.chunk_steps) c.chunk = std::max<unsigned long long>(cfg.chunk_steps, 1);
+        return c;
+    }
+
+    void finish(Request* r, int state, sp_status err, const std::string& msg) {
+        r->state = state;
+        r->error = err;
+        r->message = msg;
+        r->t_done = Clock::now();
+    }
+
+    void retire(Request* r) {
+        if (r->ens) {
+            sp_result out{};
+            r->mean.assign(r->ens->L.K * r->ens->L.OUT, 0.0);
+            r->weight.assign(r->ens->L.OUT, 0.0);
+            r->time.assign(r->ens->L.K, 0.0);
+            r->field.assign(r->ens->L.K * 3, 0.0);
+            out.mean = r->mean.data();
+            out.weight = r->weight.data();
+            out.time = r->time.data();
+            out.field = r->field.data();
+            r->ens->read(&out, &r->stats);
+            r->ens.reset();
+        }
+    }
+
+    void admit_locked() {
+        while (!queue.empty()) {
+            Request* r = queue.front();
+            if (r->cancel) {
+                queue.pop_front();
+                finish(r, SP_REQUEST_CANCELLED, SP_ERR_CANCELLED, "cancelled while queued");
+                cv_done.notify_all();
+                continue;
+            }
+            if (cfg.max_active > 0 && static_cast<int>(active.size()) >= cfg.max_active) break;
+            if (used_bytes + r->bytes > budget) break;
+            queue.pop_front();
+            try {
+                r->ens = std::make_unique<Ensemble>(ctx, r->desc, launch_for(r->desc));
+                r->ens->last_stream = nullptr;
+                r->state = SP_REQUEST_RUNNING;
+                used_bytes += r->bytes;
+                active.push_back(r);
+                Group& g = groups[key_of(r->desc)];
+                g.members.push_back(r);
+                g.dirty = true;
+            } catch (const Error& e) {
+                finish(r, SP_REQUEST_FAILED, e.status, e.what());
+                cv_done.notify_all();
+            }
+        }
+    }
+
+    void rebuild(Group& g) {
+        g.release();
+        if (g.members.empty()) return;
+        if (!g.stream) check_cuda(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking), "group stream");
+        g.ks = g.members.front()->ens->ks;
+        std::vector<EnsDev> ens;
+        std::vector<TileDesc> tiles;
+        g.max_slots = 2;
+        g.max_chunk = 1;
+        g.block = 32;
+        for (Request* r : g.members) g.block = std::max(g.block, r->ens->block);
+        for (size_t i = 0; i < g.members.size(); ++i) {
+            Ensemble* e = g.members[i]->ens.get();
+            ens.push_back(e->hdev);
+            g.max_slots = std::max(g.max_slots, e->L.slots);
+            g.max_chunk = std::max(g.max_chunk, e->L.chunk);
+            for (unsigned long long f = 0; f < e->L.n; f += g.block) tiles.push_back(TileDesc{static_cast<unsigned>(i), static_cast<unsigned>(f)});
+        }
+        g.ntiles = static_cast<int>(tiles.size());
+        check_cuda(cudaMalloc(&g.d_ens, ens.size() * sizeof(EnsDev)), "cudaMalloc");
+        check_cuda(cudaMalloc(&g.d_tiles, tiles.size() * sizeof(TileDesc)), "cudaMalloc");
+        check_cuda(cudaMemcpyAsync(g.d_ens, ens.data(), ens.size() * sizeof(EnsDev), cudaMemcpyHostToDevice, g.stream), "copy");
+        check_cuda(cudaMemcpyAsync(g.d_tiles, tiles.data(), tiles.size() * sizeof(TileDesc), cudaMemcpyHostToDevice, g.stream), "copy");
+        check_cuda(cudaStreamSynchronize(g.stream), "group upload");
+        const int n = static_cast<int>(ens.size());
+        const int midpoint = g.members.front()->desc.solver == SP_SOLVER_IMPLICIT_MIDPOINT ? 1 : 0;
+        cudaStream_t cs;
+        check_cuda(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking), "capture stream");
+        check_cuda(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal), "begin capture");
+        launch_bump_targets(g.d_ens, n, cs);
+        g.ks->field(g.d_ens, n, g.max_chunk, midpoint, cs);
+        g.ks->step(g.d_ens, g.d_tiles, g.ntiles, g.ntiles, g.block, cs);
+        g.ks->reduce(g.d_ens, n, g.max_slots, 0, cs);
+        launch_commit(g.d_ens, n, cs);
+        const cudaError_t ce = cudaStreamEndCapture(cs, &g.graph);
+        cudaStreamDestroy(cs);
+        check_cuda(ce, "end capture");
+        check_cuda(cudaGraphInstantiate(&g.gexec, g.graph, 0), "instantiate");
+        g.dirty = false;
+    }
+
+    void run() {
+        check_cuda(cudaSetDevice(ctx->device), "cudaSetDevice");
+        for (;;) {
+            {
+                std::unique_lock<std::mutex> lk(mu);
+                for (;;) {
+                    admit_locked();
+                    if (stop) return;
+                    if (!active.empty()) break;
+                    cv_work.wait(lk);
+                }
+            }
+            try {
+                // one chunk for every group
+                for (auto& kv : groups) {
+                    Group& g = kv.second;
+                    if (g.members.empty()) continue;
+                    if (g.dirty) rebuild(g);
+                    check_cuda(cudaGraphLaunch(g.gexec, g.stream), "graph launch");
+                    g_launch_count += 5;
+                }
+                for (auto& kv : groups)
+                    if (!kv.second.members.empty()) check_cuda(cudaStreamSynchronize(kv.second.stream), "chunk");
+            } catch (const Error& e) {
+                std::lock_guard<std::mutex> lk(mu);
+                for (Request* r : active) { r->ens.reset(); finish(r, SP_REQUEST_FAILED, e.status, e.what()); }
+                active.clear();
+                used_bytes = 0;
+                for (auto& kv : groups) { kv.second.members.clear(); kv.second.release(); }
+                cv_done.notify_all();
+                continue;
+            }
+            // host mirror of the device counters; retire finished or cancelled ensembles
+            std::lock_guard<std::mutex> lk(mu);
+            std::vector<Request*> still;
+            for (Request* r : active) {
+                Ensemble* e = r->ens.get();
+                const unsigned long long step = std::min(e->L.chunk, e->L.S - e->steps_done);
+                e->steps_done += step;
+                e->particle_steps += step * e->L.n;
+                e->launches += 5;
+                const bool done = e->steps_done >= e->L.S;
+                if (done || r->cancel) {
+                    try {
+                        if (done) retire(r);
+                        else r->ens.reset();
+                        finish(r, done ? SP_REQUEST_DONE : SP_REQUEST_CANCELLED, done ? SP_OK : SP_ERR_CANCELLED,
+                               done ? "" : "cancelled while running");
+                    } catch (const Error& ex) {
+                        r->ens.reset();
+                        finish(r, SP_REQUEST_FAILED, ex.status, ex.what());
+                    }
+                    used_bytes -= r->bytes;
+                    Group& g = groups[key_of(r->desc)];
+                    g.members.erase(std::find(g.members.begin(), g.members.end(), r));
+                    g.dirty = true;
+                } else {
+                    still.push_back(r);
+                }
+            }
+            active.swap(still);
+            cv_done.notify_all();
+        }
+    }
+};
+
+namespace sp {
+void copy_desc_arrays(const sp_ensemble_desc& in, Request& r) {
+    const size_t n = in.n_particles;
+    const bool brown = in.problem == SP_PROBLEM_BROWN_AND_NEEL || in.problem == SP_PROBLEM_BROWN_AND_NEEL_EULER_SPHERICAL;
+    const int M = noise_dim(in.problem);
+    const unsigned long long K = in.number_of_steps / in.oversampling;
+    const size_t ndw = in.noise == SP_NOISE_INJECTED ? (K - 1) * in.oversampling * M * n : 0;
+    r.arrays.assign(n * (5 + (brown ? 2 : 0) + 6) + ndw, 0.0);
+    double* p = r.arrays.data();
+    auto put = [&](const double* src, size_t count) -> const double* {
+        std::memcpy(p, src, count * 8);
+        const double* at = p;
+        p += count;
+        return at;
+    };
+    r.desc = in;
+    sp_particles& q = r.desc.particles;
+    q.magnetic_radius = put(in.particles.magnetic_radius, n);
+    q.saturation_magnetisation = put(in.particles.saturation_magnetisation, n);
+    q.damping_constant = put(in.particles.damping_constant, n);
+    q.gyromagnetic_ratio = put(in.particles.gyromagnetic_ratio, n);
+    q.anisotropy_constant = put(in.particles.anisotropy_constant, n);
+    if (brown) {
+        q.hydrodynamic_radius = put(in.particles.hydrodynamic_radius, n);
+        q.viscosity = put(in.particles.viscosity, n);
+    } else {
+        q.hydrodynamic_radius = nullptr;
+        q.viscosity = nullptr;
+    }
+    q.orientation = put(in.particles.orientation, 3 * n);
+    q.magnetisation = put(in.particles.magnetisation, 3 * n);
+    r.desc.injected_dw = ndw ? put(in.injected_dw, ndw) : nullptr;
+}
+}  // namespace sp
+
+#define SP_GUARD_BEGIN try {
+#define SP_GUARD_END                                                   \
+    }                                                                  \
+    catch (const Error& e) { return fail(e.status, e.what()); }        \
+    catch (const std::bad_alloc&) { return fail(SP_ERR_OUT_OF_MEMORY, "host allocation failed"); } \
+    catch (const std::exception& e) { return fail(SP_ERR_CUDA, e.what()); }
+
+extern "C" {
+
+sp_status sp_server_create(sp_context* ctx, const sp_server_config* cfg, sp_server** out) {
+    SP_GUARD_BEGIN
+    if (!ctx || !out) return fail(SP_ERR_INVALID_ARG, "NULL argument");
+    auto* s = new sp_server();
+    s->ctx = ctx;
+    if (cfg) s->cfg = *cfg;
+    size_t free_b = 0, total_b = 0;
+    check_cuda(cudaSetDevice(ctx->device), "cudaSetDevice");
+    check_cuda(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
+    const uint64_t cap = static_cast<uint64_t>(0.9 * static_cast<double>(free_b));
+    s->budget = s->cfg.memory_budget_bytes ? std::min<uint64_t>(s->cfg.memory_budget_bytes, cap) : cap;
+    s->worker = std::thread([s] {
+        try {
+            s->run();
+        } catch (...) {
+        }
+    });
+    *out = s;
+    return SP_OK;
+    SP_GUARD_END
+}
+
+sp_status sp_server_submit(sp_server* s, const sp_ensemble_desc* desc, uint64_t* id) {
+    SP_GUARD_BEGIN
+    if (!s || !id) return fail(SP_ERR_INVALID_ARG, "NULL argument");
+    std::string why;
+    const sp_status st = validate_desc(desc, why);
+    if (st != SP_OK) return fail(st, why);
+    auto r = std::make_unique<Request>();
+    copy_desc_arrays(*desc, *r);
+    r->bytes = layout_of(r->desc, s->launch_for(r->desc)).bytes;
+    if (r->bytes > s->budget)
+        return fail(SP_ERR_ADMISSION_REFUSED, "request needs " + std::to_string(r->bytes) + " bytes; budget is " +
+                                                   std::to_string(s->budget));
+    r->t_submit = Clock::now();
+    std::lock_guard<std::mutex> lk(s->mu);
+    r->id = s->next_id++;
+    *id = r->id;
+    s->queue.push_back(r.get());
+    s->all[r->id] = std::move(r);
+    s->cv_work.notify_one();
+    return SP_OK;
+    SP_GUARD_END
+}
+
+sp_status sp_server_poll(sp_server* s, uint64_t id, int32_t* state) {
+    if (!s) return fail(SP_ERR_INVALID_ARG, "NULL server");
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->all.find(id);
+    if (it == s->all.end()) return fail(SP_ERR_NOT_FOUND, "unknown request id");
+    if (state) *state = it->second->state;
+    return SP_OK;
+}
+
+sp_status sp_server_wait(sp_server* s, uint64_t id, double timeout_ms, sp_result* out, sp_stats* stats,
+                         double* latency_ms) {
+    SP_GUARD_BEGIN
+    if (!s) return fail(SP_ERR_INVALID_ARG, "NULL server");
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto it = s->all.find(id);
+    if (it == s->all.end()) return fail(SP_ERR_NOT_FOUND, "unknown request id");
+    Request* r = it->second.get();
+    auto terminal = [r] { return r->state >= SP_REQUEST_DONE; };
+    if (timeout_ms < 0) s->cv_done.wait(lk, terminal);
+    else if (!s->cv_done.wait_for(lk, std::chrono::duration<double, std::milli>(timeout_ms), terminal))
+        return fail(SP_ERR_NOT_READY, "request still running");
+    if (r->state != SP_REQUEST_DONE) return fail(r->error, r->message);
+    if (out) {
+        if (out->mean) std::memcpy(out->mean, r->mean.data(), r->mean.size() * 8);
+        if (out->weight) std::memcpy(out->weight, r->weight.data(), r->weight.size() * 8);
+        if (out->time) std::memcpy(out->time, r->time.data(), r->time.size() * 8);
+        if (out->field) std::memcpy(out->field, r->field.data(), r->field.size() * 8);
+        if (out->trajectories || out->final_state)
+            return fail(SP_ERR_INVALID_ARG, "the server returns ensemble results only");
+    }
+    if (stats) *stats = r->stats;
+    if (latency_ms) *latency_ms = std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count();
+    return SP_OK;
+    SP_GUARD_END
+}
+
+sp_status sp_server_cancel(sp_server* s, uint64_t id) {
+    if (!s) return fail(SP_ERR_INVALID_ARG, "NULL server");
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->all.find(id);
+    if (it == s->all.end()) return fail(SP_ERR_NOT_FOUND, "unknown request id");
+    it->second->cancel = true;
+    s->cv_work.notify_one();
+    return SP_OK;
+}
+
+sp_status sp_server_destroy(sp_server* s) {
+    SP_GUARD_BEGIN
+    if (!s) return SP_OK;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+    }
+    s->cv_work.notify_all();
+    if (s->worker.joinable()) s->worker.join();
+    cudaSetDevice(s->ctx->device);
+    for (Request* r : s->active) r->ens.reset();
+    for (auto& kv : s->groups) {
+        kv.second.release();
+        if (kv.second.stream) cudaStreamDestroy(kv.second.stream);
+    }
+    delete s;
+    return SP_OK;
+    SP_GUARD_END
+}
+
+}  // extern "C"

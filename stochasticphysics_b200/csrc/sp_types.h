@@ -1,0 +1,105 @@
+// sp_types.h — data shared by the host runtime and the sm_100a kernels.
+//
+// Device memory of one ensemble (structure of arrays, particle index fastest,
+// Np = n rounded up to a multiple of kPad so every tile is full in memory):
+//   state   [D][Np]      Real   SDE state y (D = 3, 2, 5, 6)
+//   ksum    [OUT][Np]    Real   Kahan running window sum of the outputs
+//   kcomp   [OUT][Np]    Real   Kahan compensation (persists across windows)
+//   params  [P][Np]      Real   derived per-particle prefactors (see kParams*)
+//   moment  [Np]         double Ms*V, the reference's getWeighting
+//   partial [warps][slots][OUT] double  per-warp weighted window means of one chunk
+//   msum    [K][OUT]     double weighted ensemble sums of every sample
+//   traj    [K][OUT][Np] double optional per-particle window means
+//   dw      [S][M][Np]   Real   optional injected Wiener increments
+//   ftab    [chunk][3]   Real   B(t) of each step of the current chunk (FP64 phase, once per ensemble)
+#pragma once
+
+#include <stdint.h>
+
+namespace sp {
+
+constexpr int kPad = 256;           // particle padding = largest block size
+constexpr int kMaxBlock = 256;
+constexpr int kFieldTile = 256;     // steps of B(t) staged in shared memory at a time
+constexpr int kReduceThreads = 256; // threads per (sample, component) in the window reduction
+
+enum ProblemId : int { kNeel = 0, kNeelSpherical = 1, kBrownNeelEuler = 2, kBrownNeel = 3 };
+enum AnisoId : int { kUniaxial = 0, kCubic = 1 };
+enum SolverId : int { kEulerMaruyama = 0, kHeun = 1, kMillstein = 2, kImplicitMidpoint = 3 };
+
+// number of derived parameters per problem
+constexpr int kParamsNeel = 16;
+constexpr int kParamsNeelSph = 15;
+constexpr int kParamsBrownNeelEuler = 13;
+constexpr int kParamsBrownNeel = 14;
+
+struct FieldParams {
+    int type;  // sp_field_type
+    int pad;
+    double offset[3];
+    double amplitude[3];
+    double omega[3];  // 2*pi*frequency
+    double phase[3];
+};
+
+// Control block of one ensemble, advanced by the commit kernel so that a
+// captured chunk graph can be replayed without changing kernel arguments.
+struct EnsCtl {
+    unsigned long long step_done;    // integrated steps completed
+    unsigned long long step_target;  // integrate up to this step
+    unsigned long long newton_iterations;
+    unsigned long long newton_unconverged;
+};
+
+struct EnsDev {
+    // geometry
+    unsigned long long n, Np, K, W, S;  // particles, padded, samples, window, integrated steps
+    unsigned long long chunk;           // steps per chunk
+    unsigned long long seed, pid_offset;
+    double dt, sqrt_dt;
+    FieldParams field;
+    // solver / problem settings
+    int max_iter;
+    int rot_brown;  // NeelSpherical: rotation enabled; BrownNeelEuler: Brown rotation enabled
+    int rot_neel;   // BrownNeelEuler: Neel rotation enabled
+    int slots;      // partial slots per chunk (max windows completing in a chunk)
+    double tol;
+    double min1, max1, min2, max2;  // rotation thresholds
+    // buffers
+    void* state;
+    void* ksum;
+    void* kcomp;
+    const void* params;
+    const double* moment;
+    const void* dw;
+    double* partial;
+    double* msum;   // [K][OUT] weighted ensemble sums
+    double* wsum;   // [OUT] summed weights
+    double* traj;
+    void* ftab;     // [chunk][3] Real: B(t) of every step of the current chunk
+    unsigned char* status;
+    EnsCtl* ctl;
+};
+
+// One CTA's worth of particles of one ensemble.
+struct TileDesc {
+    unsigned int ens;    // index into the EnsDev array
+    unsigned int first;  // first particle of the tile
+};
+
+// raw per-particle properties as uploaded (FP64, [n] or [n][3])
+struct RawParticles {
+    const double* radius;
+    const double* Ms;
+    const double* alpha;
+    const double* gamma;
+    const double* K;
+    const double* rh;
+    const double* viscosity;
+    const double* euler;  // [n][3]
+    const double* mag;    // [n][3]
+    double temperature;
+    int simple_model;
+};
+
+}  // namespace sp

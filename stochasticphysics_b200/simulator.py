@@ -1,0 +1,194 @@
+"""Host-side mirror of the reference's simulation interface, over the C ABI.
+
+``Context.simulate`` is the drop-in for the reference's per-particle loop
+(SimulationManager::StartSimulationManager fanning out singleSimulationTask,
+Particle_Simulation/Simulator/SimulationManager.h:549-574, plus the
+MeanSimulationResult accumulation): one call integrates the whole ensemble
+and returns the Results contract {Time, Field, Results (mean), Weight}
+(Particle_Simulation/Results/MeanSimulationResult.h:131-141).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import Optional
+
+import numpy as np
+
+from ._abi import DescHolder, EnsembleSpec, ResultBuffers, sp_result, sp_server_config, sp_stats, RequestState
+from .lib import check, load
+
+
+@dataclass
+class SimulationResult:
+    time: np.ndarray
+    field: np.ndarray
+    mean: np.ndarray
+    weight: np.ndarray
+    trajectories: Optional[np.ndarray] = None
+    final_state: Optional[np.ndarray] = None
+    stats: dict = field(default_factory=dict)
+
+
+def _stats_dict(st: sp_stats) -> dict:
+    return {"particle_steps": st.particle_steps, "nonfinite_particles": st.nonfinite_particles,
+            "newton_iterations": st.newton_iterations, "newton_unconverged": st.newton_unconverged,
+            "kernel_launches": st.kernel_launches, "device_ms": st.device_ms}
+
+
+def _result(buf: ResultBuffers, st: sp_stats) -> SimulationResult:
+    return SimulationResult(time=buf.time, field=buf.field, mean=buf.mean, weight=buf.weight,
+                            trajectories=buf.trajectories, final_state=buf.final_state, stats=_stats_dict(st))
+
+
+class Context:
+    """One CUDA device.  Owns a library context (sp_create/sp_destroy)."""
+
+    def __init__(self, device: int = 0):
+        self._lib = load()
+        h = C.c_void_p()
+        check(self._lib.sp_create(C.byref(h), device))
+        self.handle = h
+        self.device = device
+
+    def close(self):
+        if self.handle:
+            check(self._lib.sp_destroy(self.handle))
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001 - interpreter shutdown
+            pass
+
+    # -------------------------------------------------------------- synchronous drop-in
+    def simulate(self, spec: EnsembleSpec, trajectories: bool = False, final_state: bool = False) -> SimulationResult:
+        h = DescHolder(spec)
+        buf = ResultBuffers(spec, trajectories=trajectories, final_state=final_state)
+        st = sp_stats()
+        check(self._lib.sp_simulate(self.handle, h.byref(), C.byref(buf.c), C.byref(st)))
+        return _result(buf, st)
+
+    def ensemble(self, spec: EnsembleSpec) -> "DeviceEnsemble":
+        return DeviceEnsemble(self, spec)
+
+    def server(self, memory_budget_bytes: int = 0, chunk_steps: int = 0, max_active: int = 0) -> "Server":
+        return Server(self, memory_budget_bytes, chunk_steps, max_active)
+
+    def philox_normals(self, seed: int, pid0: int, n: int, step0: int, nsteps: int, noise_dim: int,
+                       precision: int = 0) -> np.ndarray:
+        out = np.zeros((nsteps, noise_dim, n))
+        check(self._lib.sp_debug_philox_normals(self.handle, seed, pid0, n, step0, nsteps, noise_dim, precision,
+                                                out.ctypes.data_as(C.POINTER(C.c_double))))
+        return out
+
+    @staticmethod
+    def footprint(spec: EnsembleSpec) -> int:
+        h = DescHolder(spec)
+        v = C.c_uint64()
+        check(load().sp_ensemble_footprint(h.byref(), C.byref(v)))
+        return int(v.value)
+
+
+class DeviceEnsemble:
+    """A device-resident ensemble: inputs uploaded once, advanced chunk by chunk."""
+
+    def __init__(self, ctx: Context, spec: EnsembleSpec):
+        self.ctx, self.spec = ctx, spec
+        self._lib = ctx._lib
+        self._holder = DescHolder(spec)
+        h = C.c_void_p()
+        check(self._lib.sp_ensemble_create(ctx.handle, self._holder.byref(), C.byref(h)))
+        self.handle = h
+
+    def advance(self, n_steps: int, stream: Optional[int] = None) -> None:
+        check(self._lib.sp_ensemble_advance(self.handle, int(n_steps), C.c_void_p(stream or 0)))
+
+    def steps(self):
+        d, t = C.c_uint64(), C.c_uint64()
+        check(self._lib.sp_ensemble_steps_done(self.handle, C.byref(d), C.byref(t)))
+        return int(d.value), int(t.value)
+
+    def read(self, trajectories: bool = False, final_state: bool = False) -> SimulationResult:
+        buf = ResultBuffers(self.spec, trajectories=trajectories, final_state=final_state)
+        st = sp_stats()
+        check(self._lib.sp_ensemble_read(self.handle, C.byref(buf.c), C.byref(st)))
+        return _result(buf, st)
+
+    def close(self):
+        if self.handle:
+            check(self._lib.sp_ensemble_destroy(self.handle))
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # noqa: BLE001
+            pass
+
+
+class Server:
+    """Continuous-batching server (sp_server_*): submit at any time, wait for results."""
+
+    def __init__(self, ctx: Context, memory_budget_bytes: int = 0, chunk_steps: int = 0, max_active: int = 0):
+        self.ctx = ctx
+        self._lib = ctx._lib
+        cfg = sp_server_config()
+        cfg.memory_budget_bytes = int(memory_budget_bytes)
+        cfg.chunk_steps = int(chunk_steps)
+        cfg.max_active = int(max_active)
+        h = C.c_void_p()
+        check(self._lib.sp_server_create(ctx.handle, C.byref(cfg), C.byref(h)))
+        self.handle = h
+        self._specs = {}
+
+    def submit(self, spec: EnsembleSpec) -> int:
+        holder = DescHolder(spec)
+        rid = C.c_uint64()
+        check(self._lib.sp_server_submit(self.handle, holder.byref(), C.byref(rid)))
+        self._specs[int(rid.value)] = spec
+        return int(rid.value)
+
+    def poll(self, rid: int) -> RequestState:
+        s = C.c_int32()
+        check(self._lib.sp_server_poll(self.handle, rid, C.byref(s)))
+        return RequestState(s.value)
+
+    def wait(self, rid: int, timeout_ms: float = -1.0):
+        spec = self._specs[rid]
+        buf = ResultBuffers(spec)
+        st = sp_stats()
+        lat = C.c_double()
+        check(self._lib.sp_server_wait(self.handle, rid, float(timeout_ms), C.byref(buf.c), C.byref(st), C.byref(lat)))
+        return _result(buf, st), float(lat.value)
+
+    def cancel(self, rid: int) -> None:
+        check(self._lib.sp_server_cancel(self.handle, rid))
+
+    def close(self):
+        if self.handle:
+            check(self._lib.sp_server_destroy(self.handle))
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def kernel_launch_count() -> int:
+    return int(load().sp_kernel_launch_count())

@@ -1,0 +1,201 @@
+"""GPU parity: the sm_100a kernels, called through the C ABI, against the CPU oracle.
+
+Bars (stated per test):
+  injection mode (same Wiener increments on both sides), FP64:
+      per-trajectory window means within 1e-9 relative (floor 1e-3 absolute scale),
+      ensemble mean within 1e-10 absolute (the mean magnetisation is O(1))
+  in-kernel Philox, FP64: the same 32-bit Philox words as the oracle; normals
+      within 1e-14 relative, trajectories within 1e-9
+  FP32 form: ensemble mean within 1e-3 of the FP64 kernel on the same noise
+"""
+import dataclasses
+import math
+
+import numpy as np
+import pytest
+
+import oracle
+import stochasticphysics_b200 as sp
+from stochasticphysics_b200 import provider
+from stochasticphysics_b200._abi import Anisotropy, Noise, Precision, Problem, Solver
+
+pytestmark = pytest.mark.gpu
+
+REL_TRAJ = 1e-9
+ABS_MEAN = 1e-10
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = sp.Context(0)
+    yield c
+    c.close()
+
+
+def small_spec(problem, solver, aniso=Anisotropy.Uniaxial, n=67, steps=1000, W=50, seed=11, **kw):
+    """Small ensemble of the given kind with config-like parameters."""
+    if problem == Problem.BrownAndNeelEulerSpherical:
+        base = provider.brown_neel_relaxation(n=n, steps=steps, oversampling=W, seed=seed)
+    elif problem == Problem.BrownAndNeel:
+        base = provider.brown_neel_relaxation(n=n, steps=steps, oversampling=W, seed=seed)
+        base = dataclasses.replace(base, problem=Problem.BrownAndNeel,
+                                   magnetisation=provider.along_axis_random_sign(
+                                       np.random.default_rng(seed), provider.easy_axis(Problem.BrownAndNeel, base.orientation)))
+    elif problem == Problem.NeelSpherical:
+        base = provider.neel_relaxation(n=n, steps=steps, oversampling=W, seed=seed)
+        base = dataclasses.replace(base, problem=Problem.NeelSpherical, use_coordinate_transformation=True,
+                                   min_angle_before_transformation=math.pi / 36)
+    else:
+        base = provider.neel_relaxation(n=n, steps=steps, oversampling=W, seed=seed)
+    if aniso == Anisotropy.Cubic:
+        base = dataclasses.replace(base, anisotropy=Anisotropy.Cubic, anisotropy_constant=np.full(n, -1.1e4))
+    return dataclasses.replace(base, solver=solver, **kw)
+
+
+def compare(gpu, ref, rel=REL_TRAJ, mean_abs=ABS_MEAN):
+    t_err = np.max(np.abs(gpu.trajectories - ref["trajectories"]) / np.maximum(np.abs(ref["trajectories"]), 1e-3))
+    m_err = np.max(np.abs(gpu.mean - ref["mean"]))
+    assert t_err < rel, f"per-trajectory relative error {t_err:.3e}"
+    assert m_err < mean_abs, f"ensemble-mean error {m_err:.3e}"
+    np.testing.assert_allclose(gpu.weight, ref["weight"], rtol=1e-13)
+    np.testing.assert_allclose(gpu.time, ref["time"], rtol=1e-15, atol=0)
+    np.testing.assert_allclose(gpu.field, ref["field"], rtol=1e-12, atol=1e-16)
+    return t_err, m_err
+
+
+EXPLICIT = [Solver.EulerMaruyama, Solver.Heun_Strong, Solver.Millstein]
+PROBLEMS = [Problem.Neel, Problem.NeelSpherical, Problem.BrownAndNeelEulerSpherical, Problem.BrownAndNeel]
+CASES = [(p, s, a) for p in PROBLEMS for s in EXPLICIT for a in (Anisotropy.Uniaxial, Anisotropy.Cubic)]
+CASES += [(Problem.Neel, Solver.Implicit_Midpoint, Anisotropy.Uniaxial),
+          (Problem.Neel, Solver.Implicit_Midpoint, Anisotropy.Cubic),
+          (Problem.NeelSpherical, Solver.Implicit_Midpoint, Anisotropy.Uniaxial),
+          (Problem.BrownAndNeel, Solver.Implicit_Midpoint, Anisotropy.Uniaxial)]
+
+
+@pytest.mark.parametrize("problem,solver,aniso", CASES,
+                         ids=[f"{p.name}-{s.name}-{a.name}" for p, s, a in CASES])
+def test_injection_parity_fp64(ctx, problem, solver, aniso):
+    spec = provider.with_injected_noise(small_spec(problem, solver, aniso), seed=3)
+    if solver == Solver.Implicit_Midpoint:
+        spec = dataclasses.replace(spec, timestep=1e-11, max_iteration=20, accuracy_goal=1e-10)
+    gpu = ctx.simulate(spec, trajectories=True, final_state=True)
+    ref = oracle.simulate(spec, trajectories=True, final_state=True)
+    compare(gpu, ref)
+    assert gpu.stats["nonfinite_particles"] == 0
+    if solver == Solver.Implicit_Midpoint:
+        assert gpu.stats["newton_iterations"] > 0
+        # converged roots agree; iteration counts may differ by a few per run
+        assert abs(gpu.stats["newton_iterations"] - ref["newton_iterations"]) <= 0.01 * ref["newton_iterations"] + 5
+
+
+def test_philox_normals_bit_layout(ctx):
+    for m in (3, 6):
+        dev = ctx.philox_normals(seed=0x5EED0001, pid0=17, n=300, step0=123456, nsteps=40, noise_dim=m, precision=0)
+        cpu = oracle.philox_normals(0x5EED0001, 17, 300, 123456, 40, m)
+        np.testing.assert_allclose(dev, cpu, rtol=1e-13, atol=1e-14)
+        f32 = ctx.philox_normals(seed=0x5EED0001, pid0=17, n=300, step0=123456, nsteps=40, noise_dim=m, precision=1)
+        # FP32 draws use the same Philox words; SFU log/sincos keep them within ~1e-5 of the FP64 draws
+        assert np.max(np.abs(f32 - cpu)) < 2e-5
+
+
+@pytest.mark.parametrize("problem,solver", [(Problem.Neel, Solver.Heun_Strong),
+                                            (Problem.BrownAndNeelEulerSpherical, Solver.Millstein)])
+def test_philox_mode_parity_fp64(ctx, problem, solver):
+    spec = small_spec(problem, solver, n=129, steps=2000, W=100)
+    gpu = ctx.simulate(spec, trajectories=True)
+    ref = oracle.simulate(spec, trajectories=True)
+    compare(gpu, ref)
+
+
+def test_config_shaped_parity(ctx):
+    """The three single-ensemble workloads at reduced size, injection mode."""
+    for spec in (provider.neel_relaxation(n=256, steps=3000, oversampling=100),
+                 provider.brown_neel_relaxation(n=96, steps=3000, oversampling=100),
+                 provider.cubic_implicit(n=96, steps=600, oversampling=100)):
+        spec = provider.with_injected_noise(spec, seed=5)
+        gpu = ctx.simulate(spec, trajectories=True)
+        ref = oracle.simulate(spec, trajectories=True)
+        compare(gpu, ref)
+
+
+@pytest.mark.parametrize("n,steps,W", [(1, 500, 50), (33, 1050, 100), (300, 100, 100), (40, 999, 333)])
+def test_edge_sizes(ctx, n, steps, W):
+    """one particle, ragged warps, a single sample (no integrated steps), steps % W != 0"""
+    spec = provider.with_injected_noise(small_spec(Problem.Neel, Solver.Heun_Strong, n=n, steps=steps, W=W), seed=9)
+    gpu = ctx.simulate(spec, trajectories=True)
+    ref = oracle.simulate(spec, trajectories=True)
+    assert gpu.mean.shape == (steps // W, 3)
+    compare(gpu, ref)
+
+
+def test_chunked_advance_equals_one_shot(ctx):
+    """advancing in odd-sized pieces (windows straddle the pieces) gives identical results"""
+    spec = small_spec(Problem.BrownAndNeelEulerSpherical, Solver.Heun_Strong, n=100, steps=2000, W=100,
+                      record_trajectories=True)
+    one = ctx.simulate(spec, trajectories=True)
+    with ctx.ensemble(spec) as e:
+        done, total = e.steps()
+        assert (done, total) == (0, 1900)
+        while done < total:
+            e.advance(37)
+            done, _ = e.steps()
+        r = e.read(trajectories=True)
+    np.testing.assert_array_equal(r.mean, one.mean)
+    np.testing.assert_array_equal(r.trajectories, one.trajectories)
+
+
+def test_fp32_form_close_to_fp64(ctx):
+    """FP32 stepping with FP64 time/phase/sums vs the FP64 kernel on the same Philox noise."""
+    for problem, solver in ((Problem.Neel, Solver.Heun_Strong), (Problem.BrownAndNeelEulerSpherical, Solver.Millstein),
+                            (Problem.BrownAndNeelEulerSpherical, Solver.Heun_Strong)):
+        spec = small_spec(problem, solver, n=4096, steps=20000, W=1000)
+        r64 = ctx.simulate(spec)
+        r32 = ctx.simulate(dataclasses.replace(spec, precision=Precision.FP32))
+        m = r64.mean[:, -3:]
+        err = np.max(np.abs(r32.mean[:, -3:] - m))
+        assert err <= 1e-3, f"{problem.name}/{solver.name}: FP32 mean error {err:.2e}"
+
+
+def test_langevin_equilibrium(ctx):
+    """Zero anisotropy, constant field: <m.B/|B|> -> coth(xi) - 1/xi, xi = Ms V |B| / (kB T)."""
+    n, B = 16384, 0.01
+    rng = np.random.default_rng(21)
+    v = rng.standard_normal((n, 3))
+    m0 = v / np.linalg.norm(v, axis=1, keepdims=True)
+    spec = dataclasses.replace(provider.neel_relaxation(n=n, steps=60000, oversampling=1000),
+                               anisotropy_constant=np.zeros(n), magnetisation=m0,
+                               field=sp.FieldSpec.constant((0.0, 0.0, B)))
+    r = ctx.simulate(spec)
+    V = 4.0 / 3.0 * math.pi * (10e-9) ** 3
+    xi = 4.8e5 * V * B / (1.3806485279e-23 * 295.0)
+    langevin = 1.0 / math.tanh(xi) - 1.0 / xi
+    tail = r.mean[30:, 2]  # after ~5 relaxation times
+    se = 1.0 / math.sqrt(3.0 * n)  # per-window standard error bound (|m_z| <= 1, variance <= 1/3)
+    assert abs(tail.mean() - langevin) < 3 * se + 2e-3, (tail.mean(), langevin)
+
+
+def test_nonfinite_particle_is_flagged(ctx):
+    spec = small_spec(Problem.Neel, Solver.EulerMaruyama, n=64, steps=500, W=50)
+    mag = np.array(spec.magnetisation, copy=True)
+    mag[5] = 0.0  # normalising a zero vector gives NaN (NeelRelaxation.h:283)
+    r = ctx.simulate(dataclasses.replace(spec, magnetisation=mag))
+    assert r.stats["nonfinite_particles"] == 1
+
+
+def test_server_alone_equals_in_mix(ctx):
+    """Continuous batching: a request's result is identical alone and sharing launches."""
+    a = small_spec(Problem.Neel, Solver.Heun_Strong, n=3000, steps=30000, W=1000, seed=1)
+    b = small_spec(Problem.Neel, Solver.Heun_Strong, n=5000, steps=50000, W=1000, seed=2)
+    c = small_spec(Problem.BrownAndNeelEulerSpherical, Solver.Millstein, n=2000, steps=20000, W=1000, seed=3)
+    alone = ctx.simulate(a)
+    with ctx.server(chunk_steps=5000) as srv:
+        ib = srv.submit(b)
+        ia = srv.submit(a)
+        ic = srv.submit(c)
+        ra, lat_a = srv.wait(ia)
+        rb, _ = srv.wait(ib)
+        rc, _ = srv.wait(ic)
+    np.testing.assert_array_equal(ra.mean, alone.mean)
+    np.testing.assert_array_equal(rb.mean, ctx.simulate(b).mean)
+    np.testing.assert_array_equal(rc.mean, ctx.simulate(c).mean)
+    assert lat_a > 0
