@@ -55,6 +55,29 @@ def easy_axis(problem: Problem, euler: np.ndarray) -> np.ndarray:
                      np.sin(a) * np.sin(b)], axis=1)
 
 
+def body_axes(problem: Problem, euler: np.ndarray):
+    """Body x, y, z axes (world coordinates) as each problem derives them from the Euler angles."""
+    ph, th, ps = euler[:, 0], euler[:, 1], euler[:, 2]
+    cph, sph, cth, sth, cps, sps = np.cos(ph), np.sin(ph), np.cos(th), np.sin(th), np.cos(ps), np.sin(ps)
+    if problem == Problem.BrownAndNeelEulerSpherical:
+        # columns of the cached Euler rotation (BrownAndNeelRelaxationEulerSpherical.h:209-217)
+        x = np.stack([cph * cps - cth * sph * sps, cth * sph * cps + cph * sps, sth * sph], axis=1)
+        y = np.stack([-sph * cps - cth * cph * sps, cth * cph * cps - sph * sps, sth * cph], axis=1)
+        z = np.stack([sth * sps, -sth * cps, cth], axis=1)
+    else:
+        # calculateParticleAxes (Problems/NeelRelaxation.h:257-259)
+        x = np.stack([cph * cps - cth * sph * sps, -sph * cps - cth * cph * sps, sth * sps], axis=1)
+        y = np.stack([cth * sph * cps + cph * sps, cth * cph * cps - sph * sps, -sth * cps], axis=1)
+        z = np.stack([sth * sph, sth * cph, cth], axis=1)
+    return x, y, z
+
+
+def cubic_easy_direction(problem: Problem, euler: np.ndarray) -> np.ndarray:
+    """A <111> body diagonal: an easy direction of cubic anisotropy with K1 < 0."""
+    x, y, z = body_axes(problem, euler)
+    return (x + y + z) / math.sqrt(3.0)
+
+
 def along_axis_random_sign(rng: np.random.Generator, axis: np.ndarray) -> np.ndarray:
     sign = np.where(rng.uniform(size=axis.shape[0]) < 0.5, -1.0, 1.0)
     return axis * sign[:, None]
@@ -110,9 +133,9 @@ def cubic_implicit(n: int = 262144, steps: int = 2_000_000, oversampling: int = 
     rng = np.random.default_rng(seed)
     r = lognormal_radius(rng, n, 12e-9, 0.15)
     euler = isotropic_euler(rng, n)
-    # start along a random body axis (a cubic easy direction for K1 < 0 lies on <111>; any
-    # start relaxes within a few ns)
-    m0 = along_axis_random_sign(rng, easy_axis(Problem.Neel, euler))
+    # start on a <111> body diagonal, an easy direction for K1 < 0 (a <100> start would sit
+    # on an unstable equilibrium)
+    m0 = along_axis_random_sign(rng, cubic_easy_direction(Problem.Neel, euler))
     return EnsembleSpec(
         problem=Problem.Neel, n=n, magnetic_radius=r, saturation_magnetisation=np.full(n, MS_MAGNETITE),
         damping_constant=np.full(n, 0.05), gyromagnetic_ratio=np.full(n, GAMMA), anisotropy_constant=np.full(n, -1.1e4),
