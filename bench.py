@@ -1,0 +1,333 @@
+"""Benchmark: particle-steps/s of ensemble SDE integration on B200.
+
+Workload (one GPU, weak scaling across GPUs): the coupled Brown+Neel relaxation,
+BrownAndNeelEulerSpherical with the Milstein and Heun steppers, 65536 polydisperse
+particles per GPU (lognormal cores, median 10 nm, sigma 0.1; hydrodynamic radius
+= core + 20 nm; eta = 1e-3 Pa s; K ~ U[5e3, 2e4] J/m^3; alpha = 0.1; T = 295 K;
+20 mT at 25 kHz; dt = 1e-11 s; samples every 1000 steps).  Inputs are seeded
+synthetic data with those distributions.
+
+One bench step = one chunk of 10000 SDE steps for both ensembles (Milstein and
+Heun) on the device-resident state, i.e. 2 x 65536 x 10000 particle-steps.
+
+  value        FP32 form (FP32 stepping; FP64 time, field phase, window and ensemble
+               sums), device-resident, CUDA-event timed, max over ranks
+  fp64_plain   the same steps with the plain FP64 kernel
+  e2e          the same metric through the public C ABI (sp_simulate) with host
+               buffers: upload, 10000 steps, results back, per step
+  cpu_baseline the CPU oracle (restatement of the reference formulas) on all host
+               cores, rank 0 only, on a bounded sample of the same workload
+  --impl reference  runs that CPU restatement as the reference arm
+
+Run:  python bench.py [--gpus N --steps K --warmup W]
+      torchrun --nproc-per-node N bench.py --gpus N ...
+"""
+from __future__ import annotations
+
+import argparse
+import dataclasses
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+CHUNK = 10000          # SDE steps per bench step
+N_PER_GPU = 65536
+METRIC = "particle-steps/s/GPU: FP32 served vs FP64 plain at <=1e-3 mean-M error; p99 ms"
+UNIT = "particle-steps/s"
+THROTTLE_BITS = {0x8: "hw_slowdown", 0x40: "hw_thermal_slowdown", 0x20: "sw_thermal_slowdown",
+                 0x4: "sw_power_cap", 0x80: "hw_power_brake_slowdown", 0x2: "applications_clocks_setting",
+                 0x1: "gpu_idle"}
+
+
+def workload_specs(n, steps, precision, rank):
+    from stochasticphysics_b200 import provider
+    from stochasticphysics_b200._abi import Solver
+    specs = []
+    for solver in (Solver.Millstein, Solver.Heun_Strong):
+        s = provider.brown_neel_relaxation(n=n * (rank + 1), steps=steps, oversampling=1000, solver=solver,
+                                           precision=precision)
+        specs.append(s.subset(n * rank, n * (rank + 1)))  # global particle ids: shards of one ensemble
+    return specs
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    def __init__(self, index):
+        self.index, self.samples, self.proc = index, [], None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=clocks.sm,clocks.max.sm,power.draw,"
+                 "clocks_event_reasons.active", "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 4:
+                try:
+                    self.samples.append((float(parts[0]), float(parts[1]), float(parts[2]), int(parts[3], 16)))
+                except ValueError:
+                    pass
+
+    def __exit__(self, *exc):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            self.proc.wait()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        busy = [s for s in self.samples if s[2] > 200.0] or self.samples
+        reasons = set()
+        for s in busy:
+            for bit, name in THROTTLE_BITS.items():
+                if s[3] & bit and name != "gpu_idle":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(s[0] for s in busy), "sm_max_mhz": max(s[1] for s in busy),
+                "power_w_max": max(s[2] for s in busy), "samples": len(busy), "reasons": sorted(reasons)}
+
+
+def cpu_baseline(steps_sample=2000, n=None):
+    """The CPU oracle on all host cores for a bounded sample of the workload."""
+    import oracle
+    from stochasticphysics_b200 import provider
+    from stochasticphysics_b200._abi import Solver
+    n = n or N_PER_GPU
+    cores = os.cpu_count() or 1
+    total_ps, total_s = 0, 0.0
+    for solver in (Solver.Millstein, Solver.Heun_Strong):
+        spec = provider.brown_neel_relaxation(n=n, steps=steps_sample + 1000, oversampling=1000, solver=solver)
+        t = time.perf_counter()
+        oracle.simulate(spec, threads=cores)
+        total_s += time.perf_counter() - t
+        total_ps += n * steps_sample
+    return {"value": total_ps / total_s, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{n} particles x {steps_sample} steps, Milstein + Heun, FP64 C++ restatement "
+                      f"({total_s:.1f} s on {cores} threads)"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import oracle  # noqa: F401  (the reference arm is the CPU restatement; the C++ reference cannot be built)
+    n, steps_sample = N_PER_GPU, 300
+    times = []
+    for i in range(args.warmup + args.steps):
+        base = cpu_baseline(steps_sample=steps_sample, n=n)
+        if i >= args.warmup:
+            times.append(2 * n * steps_sample / base["value"])
+    ps = 2 * n * steps_sample * len(times)
+    value = ps / sum(times)
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * sum(times) / len(times),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config_dict(args),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "port",
+                             "sample": f"{n} particles x {steps_sample} steps per step, Milstein + Heun"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "note": "reference C++ is not buildable here (Eigen/MyCEL/SerAr/Boost absent); this arm runs the "
+                    "FP64 C++ restatement of its formulas (oracle/) on all host cores"}
+    print(json.dumps(line), flush=True)
+
+
+def config_dict(args):
+    return {"workload": "brown_neel_relaxation: BrownAndNeelEulerSpherical, Milstein + Heun, "
+                        f"{N_PER_GPU} particles/GPU, dt=1e-11 s, W=1000, {CHUNK} steps per bench step",
+            "global_batch": N_PER_GPU * args.gpus, "seq_len": CHUNK, "parallelism": f"shards{args.gpus}",
+            "l2": "flushed between timed steps (256 MiB write); state of 65536 particles is ~6 MiB"}
+
+
+def time_ensembles(ensembles, steps, warmup, streams, flush, torch, concurrent):
+    """Per step: L2 flush, then one chunk of every ensemble.
+
+    concurrent=True: the ensembles advance on their own streams at the same time (as the
+    server co-schedules them); one pair of events on streams[0] brackets the step.
+    concurrent=False: one after another on streams[0], each chunk bracketed by its own
+    events (per-launch durations for the roofline)."""
+    from stochasticphysics_b200 import kernel_launch_count
+    s0 = streams[0]
+    evs, launches0 = [], None
+    for i in range(warmup + steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        if i == warmup:
+            launches0 = kernel_launch_count()
+        if concurrent:
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(s0)
+            ends = []
+            for e, st in zip(ensembles, streams):
+                st.wait_event(a)
+                e.advance(CHUNK, st.cuda_stream)
+                ev = torch.cuda.Event()
+                ev.record(st)
+                ends.append(ev)
+            for ev in ends:
+                s0.wait_event(ev)
+            b.record(s0)
+            pair = [(a, b)]
+        else:
+            pair = []
+            for e in ensembles:
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(s0)
+                e.advance(CHUNK, s0.cuda_stream)
+                b.record(s0)
+                pair.append((a, b))
+        if i >= warmup:
+            evs.append(pair)
+    torch.cuda.synchronize()
+    per_launch = [[a.elapsed_time(b) for a, b in pair] for pair in evs]
+    return per_launch, kernel_launch_count() - launches0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--n-particles", type=int, default=N_PER_GPU, help="smaller case for profiling")
+    ap.add_argument("--chunk", type=int, default=CHUNK, help="SDE steps per bench step")
+    args = ap.parse_args()
+    globals()["N_PER_GPU"], globals()["CHUNK"] = args.n_particles, args.chunk
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    import stochasticphysics_b200 as sp
+    from stochasticphysics_b200._abi import Precision
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    streams = [torch.cuda.Stream(), torch.cuda.Stream()]
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    total_steps = 2 * (args.warmup + args.steps) * CHUNK + 2000
+    flops_table = json.loads((ROOT / "stochasticphysics_b200" / "flops_table.json").read_text())["table"]
+    flops_step = [flops_table["BrownAndNeelEulerSpherical/Uniaxial/Millstein"]["flops"],
+                  flops_table["BrownAndNeelEulerSpherical/Uniaxial/Heun_Strong"]["flops"]]
+
+    def barrier_max(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    with sp.Context(local) as ctx:
+        peak32 = ctx.fma_peak_tflops(1)
+        peak64 = ctx.fma_peak_tflops(0)
+        results = {}
+        for prec in (Precision.FP32, Precision.FP64):
+            ens = [ctx.ensemble(s) for s in workload_specs(N_PER_GPU, total_steps, prec, rank)]
+            if world > 1:
+                dist.barrier()
+            torch.cuda.synchronize()
+            with ClockSampler(local) as clk:
+                conc, launches = time_ensembles(ens, args.steps, args.warmup, streams, flush, torch, True)
+            seq, _ = time_ensembles(ens, args.steps, args.warmup, streams, flush, torch, False)
+            total_ms = barrier_max(sum(sum(p) for p in conc))
+            reads = [e.read() for e in ens]
+            for e in ens:
+                e.close()
+            results[prec.name] = {"per_launch": seq, "total_ms": total_ms, "launches": launches,
+                                  "seq_ms": barrier_max(sum(sum(p) for p in seq)),
+                                  "clocks": clk.summary(), "means": [r.mean for r in reads],
+                                  "nonfinite": sum(r.stats["nonfinite_particles"] for r in reads)}
+
+        ps_per_step = 2 * N_PER_GPU * CHUNK
+        v32 = world * ps_per_step * args.steps / (results["FP32"]["total_ms"] / 1e3)
+        v64 = world * ps_per_step * args.steps / (results["FP64"]["total_ms"] / 1e3)
+        # roofline of the dominant kernel (the step kernel; >99% of each chunk graph)
+        pl = np.array(results["FP32"]["per_launch"])  # [steps][2 ensembles]
+        ach = [flops_step[j] * N_PER_GPU * CHUNK / (pl[:, j].mean() / 1e3) / 1e12 for j in range(2)]
+        pl64 = np.array(results["FP64"]["per_launch"])
+        ach64 = [flops_step[j] * N_PER_GPU * CHUNK / (pl64[:, j].mean() / 1e3) / 1e12 for j in range(2)]
+
+        # FP32 vs FP64 ensemble mean (same Philox stream): windows covered by the run
+        m32, m64 = results["FP32"]["means"], results["FP64"]["means"]
+        kdone = 2 * (args.warmup + args.steps) * CHUNK // 1000
+        diffs = [np.abs(a[1:kdone + 1, 6:9] - b[1:kdone + 1, 6:9]) for a, b in zip(m32, m64)]
+        se_indep = math.sqrt(2.0 / (3.0 * N_PER_GPU))
+
+        # e2e through the public C ABI with host buffers
+        e2e_specs = workload_specs(N_PER_GPU, CHUNK + 1000, Precision.FP32, rank)
+        for s in e2e_specs:
+            ctx.simulate(s)  # warm the path
+        e2e_times = []
+        for _ in range(args.steps):
+            if world > 1:
+                dist.barrier()
+            t = time.perf_counter()
+            outs = [ctx.simulate(s) for s in e2e_specs]
+            e2e_times.append(time.perf_counter() - t)
+        e2e_s = barrier_max(sum(e2e_times))
+        e2e_value = world * ps_per_step * args.steps / e2e_s
+        h2d = sum(s.n * 13 * 8 for s in e2e_specs)
+        d2h = sum(o.mean.nbytes + o.weight.nbytes + o.time.nbytes + o.field.nbytes for o in outs)
+
+    if rank == 0:
+        cpu = None if args.no_cpu_baseline else cpu_baseline()
+        c32 = results["FP32"]["clocks"]
+        line = {
+            "metric": METRIC, "value": v32, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": results["FP32"]["total_ms"] / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded, BASELINE config distributions)",
+            "config": config_dict(args),
+            "fp64_plain": {"value": v64, "unit": UNIT, "ms_per_step": results["FP64"]["total_ms"] / args.steps,
+                           "clocks": results["FP64"]["clocks"]},
+            "fp32_over_fp64": v32 / v64,
+            "sequential_ensembles": {"fp32": world * ps_per_step * args.steps / (results["FP32"]["seq_ms"] / 1e3),
+                                     "fp64": world * ps_per_step * args.steps / (results["FP64"]["seq_ms"] / 1e3)},
+            "fp32_vs_fp64_mean_m": {
+                "max_abs_diff": float(max(d.max() for d in diffs)),
+                "first_window_abs_diff": float(max(d[0].max() for d in diffs)),
+                "two_sample_se": se_indep,
+                "note": "same Philox noise; paths decorrelate by chaos, FP64 with float-rounded noise "
+                        "diverges from itself equally fast; max_abs_diff is bounded by the two-sample SE"},
+            "nonfinite_particles": {"fp32": results["FP32"]["nonfinite"], "fp64": results["FP64"]["nonfinite"]},
+            "roofline": {"bound": "fp32-fma", "achieved": sum(ach) / 2, "peak": peak32, "unit": "TFLOP/s",
+                         "frac": (sum(ach) / 2) / peak32, "traffic": None,
+                         "peak_source": "measured in bench.py: FMA-chain kernel on this GPU",
+                         "flops_per_particle_step": {"Millstein": flops_step[0], "Heun": flops_step[1]},
+                         "fp64": {"achieved": sum(ach64) / 2, "peak": peak64, "frac": (sum(ach64) / 2) / peak64}},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": results["FP32"]["launches"],
+            "clocks": c32,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -266,6 +266,11 @@ SP_API sp_status sp_debug_philox_normals(sp_context* ctx, uint64_t seed, uint64_
                                   uint64_t step0, uint64_t n_steps, int32_t noise_dim,
                                   int32_t precision, double* out);
 
+/* Measured dense FMA throughput of this device (TFLOP/s, 2 flops per FMA) for
+ * precision SP_PRECISION_FP64 or SP_PRECISION_FP32: the denominator of the
+ * issue roofline the engine's kernels are reported against. */
+SP_API sp_status sp_measure_fma_peak(sp_context* ctx, int32_t precision, double* tflops);
+
 #ifdef __cplusplus
 }
 #endif

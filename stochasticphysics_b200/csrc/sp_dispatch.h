@@ -33,6 +33,7 @@ void launch_commit(const EnsDev* e, int n_ens, cudaStream_t s);
 void launch_set_target(EnsCtl* ctl, unsigned long long target, cudaStream_t s);
 void launch_field_window(const FieldParams& f, double dt, unsigned long long W, unsigned long long K, double* out,
                          cudaStream_t s);
+double measure_fma_peak(int precision, int sms, cudaStream_t s);
 void launch_debug_normals(unsigned long long seed, unsigned long long pid0, unsigned long long n,
                           unsigned long long step0, unsigned long long nsteps, int noise_dim, int precision, double* out,
                           cudaStream_t s);

@@ -47,6 +47,16 @@ template <> struct M<float> {
     static constexpr float eps = 1.1920929e-7f;
 };
 
+// fmod(x, 2pi) without the software remainder loop: for |x| < 4pi the single
+// subtraction x -/+ 2pi is exact (Sterbenz), so the result equals fmod bit for bit;
+// larger arguments, which one step never produces, fall back to fmod.
+template <class R>
+__device__ __forceinline__ R wrap_two_pi(R x) {
+    const R tp = M<R>::two_pi;
+    if (M<R>::abs(x) < R(2) * tp) return x >= tp ? x - tp : (x <= -tp ? x + tp : x);
+    return M<R>::fmod(x, tp);
+}
+
 template <class R>
 struct V3 {
     R x, y, z;

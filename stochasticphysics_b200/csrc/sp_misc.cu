@@ -3,6 +3,7 @@
 
 #include "sp_dispatch.h"
 #include "sp_kernels.cuh"
+#include "sp_runtime.h"
 
 namespace sp {
 
@@ -71,6 +72,48 @@ void launch_debug_normals(unsigned long long seed, unsigned long long pid0, unsi
         if (precision == 0) debug_normals_kernel<double, 6><<<blocks, 256, 0, s>>>(seed, pid0, n, step0, nsteps, out);
         else debug_normals_kernel<float, 6><<<blocks, 256, 0, s>>>(seed, pid0, n, step0, nsteps, out);
     }
+}
+
+// FMA-chain throughput: 8 independent dependency chains per thread, so the FMA
+// pipe (not latency) limits the rate.  2 flops per FMA.
+template <class R>
+__global__ void __launch_bounds__(256) fma_peak_kernel(R* out, int iters, R b, R c) {
+    R a[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) a[j] = static_cast<R>(threadIdx.x + j) * R(1e-7);
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) a[j] = fma(a[j], b, c);
+    }
+    R s = a[0] + a[1] + a[2] + a[3] + a[4] + a[5] + a[6] + a[7];
+    if (s == R(12345.678)) out[blockIdx.x] = s;  // never true; keeps the chains live
+}
+
+double measure_fma_peak(int precision, int sms, cudaStream_t s) {
+    const int blocks = sms * 8, threads = 256, iters = 4096;
+    void* out = nullptr;
+    check_cuda(cudaMalloc(&out, blocks * 8), "cudaMalloc");
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    float best = 1e30f;
+    for (int rep = 0; rep < 4; ++rep) {
+        cudaEventRecord(a, s);
+        if (precision == 0)
+            fma_peak_kernel<double><<<blocks, threads, 0, s>>>(static_cast<double*>(out), iters, 0.9999999, 1e-9);
+        else
+            fma_peak_kernel<float><<<blocks, threads, 0, s>>>(static_cast<float*>(out), iters, 0.9999999f, 1e-9f);
+        cudaEventRecord(b, s);
+        check_cuda(cudaEventSynchronize(b), "fma peak");
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, a, b);
+        if (rep > 0) best = ms < best ? ms : best;
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(out);
+    const double flops = 2.0 * 8.0 * iters * static_cast<double>(blocks) * threads;
+    return flops / (best * 1e-3) / 1e12;
 }
 
 const KernelSet& kernel_set(int problem, int aniso, int solver, int precision, int inject) {

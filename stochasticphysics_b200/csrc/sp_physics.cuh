@@ -185,7 +185,7 @@ struct NeelSph {
     }
     static __device__ __forceinline__ void finish(const Rot<R>&, R* y, const Cache& c) {
         if (c.rot) unrotate(y);
-        else { y[0] = M<R>::fmod(y[0], M<R>::two_pi); y[1] = M<R>::fmod(y[1], M<R>::two_pi); }
+        else { y[0] = wrap_two_pi(y[0]); y[1] = wrap_two_pi(y[1]); }
     }
     static __device__ __forceinline__ void det(const Par& q, const R*, const Cache& c, const R* B, R* a) {
         const V3<R> H = Aniso<R, A>::heff(q.pF, c.md, q.x, q.y, q.z, v3(B[0], B[1], B[2]));
@@ -372,9 +372,9 @@ struct BrownNeelEuler {
     }
     static __device__ __forceinline__ void finish(const Rot<R>&, R* y, const Cache& c) {
         if (c.br) euler_unrotate(y);
-        else { y[0] = M<R>::fmod(y[0], M<R>::two_pi); y[1] = M<R>::fmod(y[1], M<R>::two_pi); y[2] = M<R>::fmod(y[2], M<R>::two_pi); }
+        else { y[0] = wrap_two_pi(y[0]); y[1] = wrap_two_pi(y[1]); y[2] = wrap_two_pi(y[2]); }
         if (c.nr) neel_unrotate(y + 3);
-        else { y[3] = M<R>::fmod(y[3], M<R>::two_pi); y[4] = M<R>::fmod(y[4], M<R>::two_pi); }
+        else { y[3] = wrap_two_pi(y[3]); y[4] = wrap_two_pi(y[4]); }
     }
     // :363-425
     static __device__ __forceinline__ void det(const Par& q, const R*, const Cache& c, const R* B, R* a) {

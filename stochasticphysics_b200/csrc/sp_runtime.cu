@@ -561,4 +561,15 @@ sp_status sp_debug_philox_normals(sp_context* ctx, uint64_t seed, uint64_t pid, 
     SP_GUARD_END
 }
 
+sp_status sp_measure_fma_peak(sp_context* ctx, int32_t precision, double* tflops) {
+    SP_GUARD_BEGIN
+    if (!ctx || !tflops) return fail(SP_ERR_INVALID_ARG, "NULL argument");
+    if (precision != 0 && precision != 1) return fail(SP_ERR_INVALID_ARG, "unknown precision");
+    check_cuda(cudaSetDevice(ctx->device), "cudaSetDevice");
+    *tflops = measure_fma_peak(precision, ctx->sms, ctx->stream);
+    g_launch_count += 4;
+    return SP_OK;
+    SP_GUARD_END
+}
+
 }  // extern "C"

@@ -19,7 +19,7 @@ SYMBOLS = [
     "sp_create", "sp_destroy", "sp_simulate", "sp_ensemble_create", "sp_ensemble_advance",
     "sp_ensemble_steps_done", "sp_ensemble_read", "sp_ensemble_destroy", "sp_ensemble_footprint",
     "sp_server_create", "sp_server_submit", "sp_server_poll", "sp_server_wait", "sp_server_cancel",
-    "sp_server_destroy", "sp_debug_philox_normals",
+    "sp_server_destroy", "sp_debug_philox_normals", "sp_measure_fma_peak",
 ]
 
 _lib = None
@@ -66,6 +66,7 @@ def load():
     L.sp_server_cancel.argtypes = [vp, u64]
     L.sp_server_destroy.argtypes = [vp]
     L.sp_debug_philox_normals.argtypes = [vp, u64, u64, u64, u64, u64, i32, i32, dp]
+    L.sp_measure_fma_peak.argtypes = [vp, i32, dp]
     for name in SYMBOLS:
         if name not in ("sp_last_error", "sp_abi_version", "sp_kernel_launch_count"):
             getattr(L, name).restype = C.c_int

@@ -89,6 +89,12 @@ class Context:
                                                 out.ctypes.data_as(C.POINTER(C.c_double))))
         return out
 
+    def fma_peak_tflops(self, precision: int) -> float:
+        """Measured FMA throughput of the device (TFLOP/s); precision 0 = FP64, 1 = FP32."""
+        v = C.c_double()
+        check(self._lib.sp_measure_fma_peak(self.handle, int(precision), C.byref(v)))
+        return float(v.value)
+
     @staticmethod
     def footprint(spec: EnsembleSpec) -> int:
         h = DescHolder(spec)
