@@ -329,7 +329,9 @@ __global__ void __launch_bounds__(kReduceThreads) reduce_kernel(const EnsDev* __
         if (slot > 1) return;
         dst = (slot == 0) ? e.msum + c : e.wsum + c;
     }
-    const unsigned long long nwarps = e.Np >> 5;
+    // warps holding at least one particle; the step kernel's tiles cover exactly these
+    // (the 256-padding beyond them is never written after init)
+    const unsigned long long nwarps = (e.n + 31) >> 5;
     double acc = 0.0;
     for (unsigned long long w = threadIdx.x; w < nwarps; w += blockDim.x) acc += e.partial[(w * e.slots + slot) * OUT + c];
     __shared__ double red[kReduceThreads];
