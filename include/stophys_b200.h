@@ -271,6 +271,24 @@ SP_API sp_status sp_debug_philox_normals(sp_context* ctx, uint64_t seed, uint64_
  * issue roofline the engine's kernels are reported against. */
 SP_API sp_status sp_measure_fma_peak(sp_context* ctx, int32_t precision, double* tflops);
 
+/* ---- allocation-free run ----------------------------------------------------
+ * No counterpart in the reference: an addition for hosts whose plug-ins may not
+ * allocate device memory while they run (real-time or embedded control loops,
+ * hosts that pre-reserve and account all GPU memory, sandboxes that forbid
+ * cudaMalloc after start-up).  Runs the whole ensemble like sp_simulate, on
+ * cuda_stream (NULL = the legacy default stream), asynchronously, and allocates
+ * nothing: the caller passes the per-particle inputs as DEVICE pointers
+ * (device_particles, same layout as sp_particles; desc->particles is ignored)
+ * and receives mean [n_samples][out_dim] and weight [out_dim] in DEVICE memory,
+ * valid once the stream has completed.  Every internal buffer lives in one
+ * static device array of 32 MiB that each GPU loading the library holds until
+ * exit; ensembles needing more are refused with SP_ERR_INVALID_ARG.  Philox noise
+ * only, no trajectories.  The first call on a device resolves the array's
+ * address (make it before any stream capture); calls overlapping on the GPU
+ * share the array and race. */
+SP_API sp_status sp_simulate_noalloc(const sp_ensemble_desc* desc, const sp_particles* device_particles,
+                                     double* device_mean, double* device_weight, void* cuda_stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -31,6 +31,7 @@ extern thread_local std::string g_last_error;
 extern std::atomic<unsigned long long> g_launch_count;
 
 void check_cuda(cudaError_t e, const char* what);
+inline void launches_add(unsigned long long n) { g_launch_count += n; }
 sp_status fail(sp_status s, const std::string& msg);
 sp_status validate_desc(const sp_ensemble_desc* d, std::string& why);
 int state_dim(int p);

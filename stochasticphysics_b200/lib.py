@@ -9,7 +9,7 @@ from __future__ import annotations
 import ctypes as C
 from pathlib import Path
 
-from ._abi import (sp_ensemble_desc, sp_result, sp_server_config, sp_stats, Status)
+from ._abi import (sp_ensemble_desc, sp_particles, sp_result, sp_server_config, sp_stats, Status)
 
 PKG = Path(__file__).resolve().parent
 LIB_PATH = PKG / "libstophys_b200.so"
@@ -19,7 +19,7 @@ SYMBOLS = [
     "sp_create", "sp_destroy", "sp_simulate", "sp_ensemble_create", "sp_ensemble_advance",
     "sp_ensemble_steps_done", "sp_ensemble_read", "sp_ensemble_destroy", "sp_ensemble_footprint",
     "sp_server_create", "sp_server_submit", "sp_server_poll", "sp_server_wait", "sp_server_cancel",
-    "sp_server_destroy", "sp_debug_philox_normals", "sp_measure_fma_peak",
+    "sp_server_destroy", "sp_debug_philox_normals", "sp_measure_fma_peak", "sp_simulate_noalloc",
 ]
 
 _lib = None
@@ -67,6 +67,7 @@ def load():
     L.sp_server_destroy.argtypes = [vp]
     L.sp_debug_philox_normals.argtypes = [vp, u64, u64, u64, u64, u64, i32, i32, dp]
     L.sp_measure_fma_peak.argtypes = [vp, i32, dp]
+    L.sp_simulate_noalloc.argtypes = [C.POINTER(sp_ensemble_desc), C.POINTER(sp_particles), dp, dp, vp]
     for name in SYMBOLS:
         if name not in ("sp_last_error", "sp_abi_version", "sp_kernel_launch_count"):
             getattr(L, name).restype = C.c_int
