@@ -1,0 +1,52 @@
+""".ini runs on the GPU: the command-line driver against the Python API and the oracle.
+
+`stophys_b200 -parfile:<ini>` (the reference's application entry point,
+Simulator/SimulationApplication.cpp:29-158) must give the same Mean_Results as
+Context.simulate on the EnsembleSpec the same .ini and seed describe — the same
+library call on the same inputs, so equal bit for bit — and the CPU oracle's
+ensemble mean within the FP64 Philox-mode parity bar (1e-10 absolute).
+"""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import oracle
+import stochasticphysics_b200 as sp
+from stochasticphysics_b200 import settings
+
+pytestmark = pytest.mark.gpu
+
+INI = Path(__file__).resolve().parent / "data" / "ini"
+ABS_MEAN = 1e-10
+
+
+def _copy(tmp_path, main, n, particles):
+    for name in particles:
+        (tmp_path / name).write_text((INI / name).read_text())
+    text = (INI / main).read_text()
+    lines = [f"Number_of_simulations = {n}" if ln.startswith("Number_of_simulations") else ln
+             for ln in text.splitlines()]
+    out = tmp_path / main
+    out.write_text("\n".join(lines) + "\n")
+    return out
+
+
+@pytest.mark.parametrize("main, n, particles", [
+    ("legacy_neel_spherical.ini", 10, ("legacy_particle_small.ini", "legacy_particle_large.ini")),
+    ("current_brown_neel.ini", 256, ("current_particle.ini", "current_particle_b.ini")),
+])
+def test_ini_run_matches_api_and_oracle(tmp_path, main, n, particles):
+    path = _copy(tmp_path, main, n, particles)
+    rec = settings.run_ini(path, seed=21)["Mean_Results"]
+    spec = settings.load_ini(path, seed=21)
+    with sp.Context(0) as ctx:
+        api = ctx.simulate(spec)
+    mean = np.array(rec["Results"], dtype=float)
+    np.testing.assert_array_equal(mean, api.mean)
+    np.testing.assert_array_equal(np.array(rec["Weight"], dtype=float), api.weight)
+    np.testing.assert_array_equal(np.array(rec["Time"], dtype=float), api.time)
+    np.testing.assert_array_equal(np.array(rec["Field"], dtype=float), api.field)
+    ref = oracle.simulate(spec)
+    assert np.all(np.isfinite(ref["mean"]))
+    assert np.max(np.abs(mean - ref["mean"])) <= ABS_MEAN
