@@ -271,6 +271,35 @@ SP_API sp_status sp_debug_philox_normals(sp_context* ctx, uint64_t seed, uint64_
  * issue roofline the engine's kernels are reported against. */
 SP_API sp_status sp_measure_fma_peak(sp_context* ctx, int32_t precision, double* tflops);
 
+/* ---- autotuner ----------------------------------------------------------
+ * No counterpart in the reference (its thread pool has no launch shape).
+ * Launch shape of one kernel key (problem, anisotropy, solver, precision,
+ * noise): threads per CTA (one particle per thread), persistent grid (CTAs =
+ * resident CTAs x SMs striding over the tiles) or one CTA per tile, and SDE
+ * steps per captured chunk. */
+typedef struct sp_launch_config {
+    int32_t block;
+    int32_t persistent;
+    uint64_t chunk_steps;
+    double particle_steps_per_s; /* measured rate of this shape on the probe */
+} sp_launch_config;
+/* Times every candidate shape on a probe of desc (its first
+ * min(n_particles, probe_particles) particles; 0 = 65536) with CUDA events and
+ * caches the fastest for desc's kernel key in this process; every later
+ * ensemble, sp_simulate and server group of that key uses it.  best and
+ * candidates[max_candidates] (optional) receive the winner and the timings;
+ * *n_candidates the number timed.  SP_NOISE_INJECTED descriptions are refused. */
+SP_API sp_status sp_autotune(sp_context* ctx, const sp_ensemble_desc* desc, uint64_t probe_particles,
+                             sp_launch_config* best, sp_launch_config* candidates, int32_t max_candidates,
+                             int32_t* n_candidates);
+/* Launch shape the library uses for desc now (tuned or default). */
+SP_API sp_status sp_launch_config_for(sp_context* ctx, const sp_ensemble_desc* desc, sp_launch_config* out);
+/* Write / read (merge) the tuned shapes of this process as text, one key per
+ * line; reset forgets them all (defaults apply again). */
+SP_API sp_status sp_tuning_save(const char* path);
+SP_API sp_status sp_tuning_load(const char* path);
+SP_API sp_status sp_tuning_reset(void);
+
 /* ---- allocation-free run ----------------------------------------------------
  * No counterpart in the reference: an addition for hosts whose plug-ins may not
  * allocate device memory while they run (real-time or embedded control loops,

@@ -171,6 +171,19 @@ class sp_stats(C.Structure):
     ]
 
 
+class sp_launch_config(C.Structure):
+    _fields_ = [
+        ("block", C.c_int32),
+        ("persistent", C.c_int32),
+        ("chunk_steps", C.c_uint64),
+        ("particle_steps_per_s", C.c_double),
+    ]
+
+    def to_dict(self) -> dict:
+        return {"block": int(self.block), "persistent": int(self.persistent), "chunk_steps": int(self.chunk_steps),
+                "particle_steps_per_s": float(self.particle_steps_per_s)}
+
+
 class sp_server_config(C.Structure):
     _fields_ = [
         ("memory_budget_bytes", C.c_uint64),

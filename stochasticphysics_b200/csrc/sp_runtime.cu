@@ -404,12 +404,6 @@ Ensemble::~Ensemble() {
 using namespace sp;
 
 // ====================================================================== C ABI
-#define SP_GUARD_BEGIN try {
-#define SP_GUARD_END                                                   \
-    }                                                                  \
-    catch (const Error& e) { return fail(e.status, e.what()); }        \
-    catch (const std::bad_alloc&) { return fail(SP_ERR_OUT_OF_MEMORY, "host allocation failed"); } \
-    catch (const std::exception& e) { return fail(SP_ERR_CUDA, e.what()); }
 
 extern "C" {
 

@@ -100,3 +100,11 @@ struct Ensemble {
 };
 
 }  // namespace sp
+
+// every C entry point: no exception crosses the ABI
+#define SP_GUARD_BEGIN try {
+#define SP_GUARD_END                                                                                   \
+    }                                                                                                  \
+    catch (const sp::Error& e) { return sp::fail(e.status, e.what()); }                                \
+    catch (const std::bad_alloc&) { return sp::fail(SP_ERR_OUT_OF_MEMORY, "host allocation failed"); } \
+    catch (const std::exception& e) { return sp::fail(SP_ERR_CUDA, e.what()); }

@@ -291,12 +291,6 @@ void copy_desc_arrays(const sp_ensemble_desc& in, Request& r) {
 }
 }  // namespace sp
 
-#define SP_GUARD_BEGIN try {
-#define SP_GUARD_END                                                   \
-    }                                                                  \
-    catch (const Error& e) { return fail(e.status, e.what()); }        \
-    catch (const std::bad_alloc&) { return fail(SP_ERR_OUT_OF_MEMORY, "host allocation failed"); } \
-    catch (const std::exception& e) { return fail(SP_ERR_CUDA, e.what()); }
 
 extern "C" {
 

@@ -9,7 +9,7 @@ from __future__ import annotations
 import ctypes as C
 from pathlib import Path
 
-from ._abi import (sp_ensemble_desc, sp_particles, sp_result, sp_server_config, sp_stats, Status)
+from ._abi import (sp_ensemble_desc, sp_launch_config, sp_particles, sp_result, sp_server_config, sp_stats, Status)
 
 PKG = Path(__file__).resolve().parent
 LIB_PATH = PKG / "libstophys_b200.so"
@@ -20,6 +20,7 @@ SYMBOLS = [
     "sp_ensemble_steps_done", "sp_ensemble_read", "sp_ensemble_destroy", "sp_ensemble_footprint",
     "sp_server_create", "sp_server_submit", "sp_server_poll", "sp_server_wait", "sp_server_cancel",
     "sp_server_destroy", "sp_debug_philox_normals", "sp_measure_fma_peak", "sp_simulate_noalloc",
+    "sp_autotune", "sp_launch_config_for", "sp_tuning_save", "sp_tuning_load", "sp_tuning_reset",
 ]
 
 _lib = None
@@ -68,6 +69,12 @@ def load():
     L.sp_debug_philox_normals.argtypes = [vp, u64, u64, u64, u64, u64, i32, i32, dp]
     L.sp_measure_fma_peak.argtypes = [vp, i32, dp]
     L.sp_simulate_noalloc.argtypes = [C.POINTER(sp_ensemble_desc), C.POINTER(sp_particles), dp, dp, vp]
+    L.sp_autotune.argtypes = [vp, C.POINTER(sp_ensemble_desc), u64, C.POINTER(sp_launch_config),
+                              C.POINTER(sp_launch_config), i32, C.POINTER(i32)]
+    L.sp_launch_config_for.argtypes = [vp, C.POINTER(sp_ensemble_desc), C.POINTER(sp_launch_config)]
+    L.sp_tuning_save.argtypes = [C.c_char_p]
+    L.sp_tuning_load.argtypes = [C.c_char_p]
+    L.sp_tuning_reset.argtypes = []
     for name in SYMBOLS:
         if name not in ("sp_last_error", "sp_abi_version", "sp_kernel_launch_count"):
             getattr(L, name).restype = C.c_int

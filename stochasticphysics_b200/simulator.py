@@ -15,7 +15,8 @@ from typing import Optional
 
 import numpy as np
 
-from ._abi import DescHolder, EnsembleSpec, ResultBuffers, sp_result, sp_server_config, sp_stats, RequestState
+from ._abi import (DescHolder, EnsembleSpec, ResultBuffers, sp_launch_config, sp_result, sp_server_config, sp_stats,
+                   RequestState)
 from .lib import check, load
 
 
@@ -94,6 +95,34 @@ class Context:
         v = C.c_double()
         check(self._lib.sp_measure_fma_peak(self.handle, int(precision), C.byref(v)))
         return float(v.value)
+
+    def autotune(self, spec: EnsembleSpec, probe_particles: int = 65536) -> dict:
+        """Times the candidate launch shapes for spec's kernel key on a probe of its
+        particles and caches the fastest in this process (sp_autotune)."""
+        best = sp_launch_config()
+        cands = (sp_launch_config * 16)()
+        n = C.c_int32()
+        check(self._lib.sp_autotune(self.handle, DescHolder(spec).byref(), int(probe_particles), C.byref(best),
+                                    cands, 16, C.byref(n)))
+        return {"best": best.to_dict(), "candidates": [cands[i].to_dict() for i in range(min(n.value, 16))]}
+
+    def launch_config(self, spec: EnsembleSpec) -> dict:
+        """Launch shape the library uses for spec now (tuned or default)."""
+        out = sp_launch_config()
+        check(self._lib.sp_launch_config_for(self.handle, DescHolder(spec).byref(), C.byref(out)))
+        return out.to_dict()
+
+    @staticmethod
+    def tuning_save(path) -> None:
+        check(load().sp_tuning_save(str(path).encode()))
+
+    @staticmethod
+    def tuning_load(path) -> None:
+        check(load().sp_tuning_load(str(path).encode()))
+
+    @staticmethod
+    def tuning_reset() -> None:
+        check(load().sp_tuning_reset())
 
     @staticmethod
     def footprint(spec: EnsembleSpec) -> int:

@@ -1,0 +1,68 @@
+"""Autotuner on the GPU: timings, cache, and launch-shape independence of results.
+
+The ensemble mean is reduced per warp in a fixed order, so no launch shape
+(CTA size, persistent grid, chunk length) may change a single bit of the result.
+"""
+import dataclasses
+
+import numpy as np
+import pytest
+
+import stochasticphysics_b200 as sp
+from stochasticphysics_b200 import provider
+from stochasticphysics_b200._abi import Precision, Solver
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture
+def ctx():
+    sp.Context.tuning_reset()
+    c = sp.Context(0)
+    yield c
+    c.close()
+    sp.Context.tuning_reset()
+
+
+def test_autotune_picks_the_fastest_candidate(ctx):
+    spec = provider.brown_neel_relaxation(n=65536, steps=200000, oversampling=1000, solver=Solver.Millstein,
+                                          precision=Precision.FP32)
+    out = ctx.autotune(spec, probe_particles=32768)
+    best, cands = out["best"], out["candidates"]
+    assert len(cands) >= 4
+    assert all(c["particle_steps_per_s"] > 0 for c in cands)
+    assert best["particle_steps_per_s"] == max(c["particle_steps_per_s"] for c in cands)
+    used = ctx.launch_config(spec)
+    assert (used["block"], used["persistent"], used["chunk_steps"]) == (best["block"], best["persistent"],
+                                                                         best["chunk_steps"])
+
+
+@pytest.mark.parametrize("shape", ["0/0/0/0/0 64 1 3000", "0/0/0/0/0 256 0 1000", "0/0/0/0/0 32 1 500"])
+def test_results_do_not_depend_on_the_launch_shape(ctx, tmp_path, shape):
+    spec = provider.neel_relaxation(n=5000, steps=6000, oversampling=100, solver=Solver.EulerMaruyama)
+    key = f"{int(spec.problem)}/{int(spec.anisotropy)}/{int(spec.solver)}/{int(spec.precision)}/{int(spec.noise)}"
+    assert key == "0/0/0/0/0"
+    ref = ctx.simulate(spec)
+    f = tmp_path / "shape.txt"
+    f.write_text(shape + " 0\n")
+    sp.Context.tuning_load(f)
+    got = ctx.simulate(spec)
+    block, persistent, chunk = (int(v) for v in shape.split()[1:4])
+    used = ctx.launch_config(spec)
+    assert (used["persistent"], used["chunk_steps"]) == (persistent, chunk)
+    np.testing.assert_array_equal(got.mean, ref.mean)
+    np.testing.assert_array_equal(got.weight, ref.weight)
+
+
+def test_tuned_shapes_reach_the_server(ctx, tmp_path):
+    spec = provider.neel_relaxation(n=3000, steps=4000, oversampling=100, solver=Solver.Heun_Strong)
+    ref = ctx.simulate(spec)
+    f = tmp_path / "shape.txt"
+    f.write_text("0/0/1/0/0 64 1 2000 0\n")
+    sp.Context.tuning_load(f)
+    other = dataclasses.replace(spec, seed=spec.seed + 1)
+    with sp.Server(ctx) as srv:
+        ids = [srv.submit(spec), srv.submit(other)]
+        res = [srv.wait(i)[0] for i in ids]
+    np.testing.assert_array_equal(res[0].mean, ref.mean)
+    assert not np.array_equal(res[1].mean, ref.mean)

@@ -1,0 +1,76 @@
+"""Autotuner cache on the CPU: load / save / reset and the shape lookup.
+
+sp_autotune itself times kernels (GPU test in test_gpu_tuning.py); the cache it
+fills is plain host state keyed by problem/anisotropy/solver/precision/noise.
+"""
+import ctypes as C
+
+import pytest
+
+from stochasticphysics_b200 import provider
+from stochasticphysics_b200._abi import DescHolder, Precision, Solver, sp_launch_config
+from stochasticphysics_b200.lib import load
+
+
+def _shape(spec):
+    out = sp_launch_config()
+    assert load().sp_launch_config_for(None, DescHolder(spec).byref(), C.byref(out)) == 0, load().sp_last_error()
+    return out.to_dict()
+
+
+@pytest.fixture(autouse=True)
+def clean_cache():
+    load().sp_tuning_reset()
+    yield
+    load().sp_tuning_reset()
+
+
+def test_defaults_without_tuning():
+    spec = provider.brown_neel_relaxation(n=65536, steps=20000, oversampling=1000, precision=Precision.FP32)
+    s = _shape(spec)
+    # CTA size halved from 256 until there are >= 2 CTAs per SM (148 SMs), down to 32
+    assert s == {"block": 128, "persistent": 0, "chunk_steps": 10000, "particle_steps_per_s": 0.0}
+    small = provider.brown_neel_relaxation(n=4000, steps=20000, oversampling=1000)
+    assert _shape(small)["block"] == 32
+
+
+def test_loaded_shape_applies_to_its_key_only(tmp_path):
+    bn = provider.brown_neel_relaxation(n=65536, steps=20000, oversampling=1000, solver=Solver.Millstein,
+                                        precision=Precision.FP32)
+    key = f"{int(bn.problem)}/{int(bn.anisotropy)}/{int(bn.solver)}/{int(bn.precision)}/{int(bn.noise)}"
+    f = tmp_path / "tune.txt"
+    f.write_text(f"{key} 128 1 30000 1.5e10\n")
+    assert load().sp_tuning_load(str(f).encode()) == 0
+    assert _shape(bn) == {"block": 128, "persistent": 1, "chunk_steps": 30000, "particle_steps_per_s": 1.5e10}
+    heun = provider.brown_neel_relaxation(n=65536, steps=20000, oversampling=1000, solver=Solver.Heun_Strong,
+                                          precision=Precision.FP32)
+    assert _shape(heun)["persistent"] == 0 and _shape(heun)["block"] == 128
+    # chunks stay whole windows; small ensembles still cover the SMs
+    odd = provider.brown_neel_relaxation(n=65536, steps=70000, oversampling=7000, solver=Solver.Millstein,
+                                         precision=Precision.FP32)
+    assert _shape(odd)["chunk_steps"] == 28000
+    tiny = provider.brown_neel_relaxation(n=5000, steps=20000, oversampling=1000, solver=Solver.Millstein,
+                                          precision=Precision.FP32)
+    assert _shape(tiny)["block"] == 32
+
+
+def test_save_load_roundtrip_and_reset(tmp_path):
+    a = tmp_path / "a.txt"
+    a.write_text("0/0/1/1/0 64 0 20000 2e10\n2/0/2/0/0 256 1 10000 4e9\n")
+    assert load().sp_tuning_load(str(a).encode()) == 0
+    b = tmp_path / "b.txt"
+    assert load().sp_tuning_save(str(b).encode()) == 0
+    assert sorted(b.read_text().split("\n")) == sorted(["0/0/1/1/0 64 0 20000 2e+10", "2/0/2/0/0 256 1 10000 4e+09", ""])
+    load().sp_tuning_reset()
+    c = tmp_path / "c.txt"
+    assert load().sp_tuning_save(str(c).encode()) == 0
+    assert c.read_text() == ""
+
+
+@pytest.mark.parametrize("text", ["0/0/1/1 64 0 100 1\n", "0/0/1/1/0 48 0 100 1\n", "0/0/1/1/0 64 0\n",
+                                  "0/0/1/1/0 64 0 0 1\n"])
+def test_malformed_tuning_files_are_refused(tmp_path, text):
+    f = tmp_path / "bad.txt"
+    f.write_text(text)
+    assert load().sp_tuning_load(str(f).encode()) == 1
+    assert load().sp_tuning_load(str(tmp_path / "missing.txt").encode()) == 1
