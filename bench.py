@@ -17,7 +17,14 @@ Heun) on the device-resident state, i.e. 2 x 65536 x 10000 particle-steps.
                buffers: upload, 10000 steps, results back, per step
   cpu_baseline the CPU oracle (restatement of the reference formulas) on all host
                cores, rank 0 only, on a bounded sample of the same workload
+  serving      continuous-batching leg (N=1): Poisson arrivals of mixed Neel /
+               BrownAndNeelEulerSpherical requests (batched-set distributions, 2D
+               Lissajous field) through sp_server_*, FP32; p50/p99 latency,
+               aggregate particle-steps/s, and the same requests one at a time in
+               FP64 as the serial baseline
   --impl reference  runs that CPU restatement as the reference arm
+
+Launch shapes come from the autotuner (sp_autotune) unless --no-autotune.
 
 Run:  python bench.py [--gpus N --steps K --warmup W]
       torchrun --nproc-per-node N bench.py --gpus N ...
@@ -102,6 +109,94 @@ class ClockSampler:
                     reasons.add(name)
         return {"sm_mhz": statistics.median(s[0] for s in busy), "sm_max_mhz": max(s[1] for s in busy),
                 "power_w_max": max(s[2] for s in busy), "samples": len(busy), "reasons": sorted(reasons)}
+
+
+def profiled_traffic_per_particle():
+    """DRAM bytes per particle per step-kernel launch from the committed ncu summary
+    (dram__bytes_read.sum + dram__bytes_write.sum of one capture, divided by the
+    captured launch's particles); the traffic of a launch scales with particles, not
+    steps (state, Kahan sums and prefactors are read once and written once)."""
+    import re
+    path = ROOT / "profiles" / "step_kernel_brown_neel_euler_fp32_16384.md"
+    try:
+        m = re.search(r"traffic_bytes_per_particle_per_launch:\s*([0-9.eE+-]+)", path.read_text())
+    except OSError:
+        return None, None
+    return (float(m.group(1)), path.name) if m else (None, None)
+
+
+def serving_leg(ctx, seconds, rate, step_scale, seed=0x5EED0005, serial_sample=48):
+    """Poisson arrivals of mixed Neel / BrownAndNeelEulerSpherical requests with the
+    batched-set distributions and the 2D Lissajous field, served by the continuous-
+    batching server in FP32; latency = submit -> result ready (server clock).  The
+    same requests, one at a time through the plain FP64 path (every k-th request, at
+    most serial_sample), give the serial baseline and the FP32-vs-FP64 mean error."""
+    import numpy as np
+
+    import stochasticphysics_b200 as sp
+    from stochasticphysics_b200 import provider
+    from stochasticphysics_b200._abi import Precision, Problem
+
+    rng = np.random.default_rng(seed)
+    arrivals = []
+    t = 0.0
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t > seconds:
+            break
+        arrivals.append(t)
+    specs = provider.batched_sets(count=len(arrivals), seed=seed, precision=Precision.FP32, step_scale=step_scale,
+                                  lissajous=True, problems=(Problem.Neel, Problem.BrownAndNeelEulerSpherical))
+    free, _ = __import__("torch").cuda.mem_get_info()
+    budget = int(min(150e9, 0.8 * free))
+    ids = [None] * len(specs)
+    with sp.Server(ctx, memory_budget_bytes=budget) as srv:
+        def submitter():
+            t0 = time.perf_counter()
+            for i, (ta, spec) in enumerate(zip(arrivals, specs)):
+                d = t0 + ta - time.perf_counter()
+                if d > 0:
+                    time.sleep(d)
+                ids[i] = srv.submit(spec)
+        th = threading.Thread(target=submitter)
+        t_start = time.perf_counter()
+        th.start()
+        lat, served = [], []
+        for i in range(len(specs)):
+            while ids[i] is None:
+                time.sleep(0.0005)
+            res, ms = srv.wait(ids[i])
+            lat.append(ms)
+            served.append(res.mean)
+        t_end = time.perf_counter()
+        th.join()
+    ps = [s.n * s.integrated_steps for s in specs]
+    k = max(1, len(specs) // serial_sample)
+    sample = list(range(0, len(specs), k))[:serial_sample]
+    serial_s, errs = 0.0, []
+    for i in sample:
+        s64 = dataclasses.replace(specs[i], precision=Precision.FP64)
+        t = time.perf_counter()
+        r64 = ctx.simulate(s64)
+        serial_s += time.perf_counter() - t
+        cols = slice(6, 9) if specs[i].problem == Problem.BrownAndNeelEulerSpherical else slice(0, 3)
+        d = float(np.max(np.abs(served[i][:, cols] - r64.mean[:, cols])))
+        errs.append((d, d / math.sqrt(2.0 / (3.0 * specs[i].n))))
+    lat_s = sorted(lat)
+    return {
+        "requests": len(specs), "arrival_rate_per_s": rate, "arrival_window_s": seconds,
+        "p50_ms": float(np.percentile(lat_s, 50)), "p99_ms": float(np.percentile(lat_s, 99)),
+        "max_ms": float(lat_s[-1]), "value": sum(ps) / (t_end - t_start), "unit": UNIT,
+        "offered_particle_steps_per_s": sum(ps) / seconds, "memory_budget_bytes": budget,
+        "serial_fp64": {"value": sum(ps[i] for i in sample) / serial_s, "unit": UNIT, "requests": len(sample),
+                        "note": "same requests one at a time through sp_simulate in FP64 (every k-th request)"},
+        "fp32_vs_fp64_mean_m": {"max_abs_diff": max(e[0] for e in errs),
+                                "max_diff_over_two_sample_se": max(e[1] for e in errs)},
+        "workload": f"Poisson {rate}/s for {seconds} s; N ~ logU[1e3, 6.4e4], S ~ logU[1e5, 1e7] x {step_scale} "
+                    "(whole windows of 1000 steps, >= 2 windows); Neel or BrownAndNeelEulerSpherical (p = 1/2), "
+                    "Heun / Millstein alternating, FP32; Lissajous 12 mT at 25.25 kHz (x) and 26.04 kHz (y); "
+                    "dt = 1e-11 s",
+    }
 
 
 def cpu_baseline(steps_sample=2000, n=None):
@@ -208,6 +303,11 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--n-particles", type=int, default=N_PER_GPU, help="smaller case for profiling")
     ap.add_argument("--chunk", type=int, default=CHUNK, help="SDE steps per bench step")
+    ap.add_argument("--no-autotune", action="store_true", help="use the default launch shapes")
+    ap.add_argument("--serving-seconds", type=float, default=8.0, help="arrival window of the serving leg (0: skip)")
+    ap.add_argument("--serving-rate", type=float, default=50.0, help="mean Poisson arrival rate (requests/s)")
+    ap.add_argument("--serving-step-scale", type=float, default=0.006,
+                    help="scale of the request step counts (S ~ logU[1e5, 1e7] x scale)")
     args = ap.parse_args()
     globals()["N_PER_GPU"], globals()["CHUNK"] = args.n_particles, args.chunk
     args.warmup = max(args.warmup, 3)
@@ -244,7 +344,12 @@ def main():
     with sp.Context(local) as ctx:
         peak32 = ctx.fma_peak_tflops(1)
         peak64 = ctx.fma_peak_tflops(0)
-        results = {}
+        results, shapes = {}, {}
+        for prec in (Precision.FP32, Precision.FP64):
+            for s in workload_specs(N_PER_GPU, total_steps, prec, rank):
+                if not args.no_autotune:
+                    ctx.autotune(s, probe_particles=N_PER_GPU)
+                shapes[f"{prec.name}/{s.solver.name}"] = ctx.launch_config(s)
         for prec in (Precision.FP32, Precision.FP64):
             ens = [ctx.ensemble(s) for s in workload_specs(N_PER_GPU, total_steps, prec, rank)]
             if world > 1:
@@ -292,8 +397,12 @@ def main():
         e2e_value = world * ps_per_step * args.steps / e2e_s
         h2d = sum(s.n * 13 * 8 for s in e2e_specs)
         d2h = sum(o.mean.nbytes + o.weight.nbytes + o.time.nbytes + o.field.nbytes for o in outs)
+        serving = None
+        if world == 1 and args.serving_seconds > 0:
+            serving = serving_leg(ctx, args.serving_seconds, args.serving_rate, args.serving_step_scale)
 
     if rank == 0:
+        tpp, tsrc = profiled_traffic_per_particle()
         cpu = None if args.no_cpu_baseline else cpu_baseline()
         c32 = results["FP32"]["clocks"]
         line = {
@@ -314,7 +423,10 @@ def main():
                         "diverges from itself equally fast; max_abs_diff is bounded by the two-sample SE"},
             "nonfinite_particles": {"fp32": results["FP32"]["nonfinite"], "fp64": results["FP64"]["nonfinite"]},
             "roofline": {"bound": "fp32-fma", "achieved": sum(ach) / 2, "peak": peak32, "unit": "TFLOP/s",
-                         "frac": (sum(ach) / 2) / peak32, "traffic": None,
+                         "frac": (sum(ach) / 2) / peak32,
+                         "traffic": None if tpp is None else tpp * N_PER_GPU,
+                         "traffic_source": None if tpp is None else
+                         f"profiles/{tsrc}: DRAM bytes per particle per launch x {N_PER_GPU} particles",
                          "peak_source": "measured in bench.py: FMA-chain kernel on this GPU",
                          "flops_per_particle_step": {"Millstein": flops_step[0], "Heun": flops_step[1]},
                          "fp64": {"achieved": sum(ach64) / 2, "peak": peak64, "frac": (sum(ach64) / 2) / peak64}},
@@ -322,6 +434,8 @@ def main():
             "gpu_launches": results["FP32"]["launches"],
             "clocks": c32,
             "cpu_baseline": cpu,
+            "launch_shapes": shapes,
+            "serving": serving,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
