@@ -34,7 +34,7 @@
 extern "C" {
 #endif
 
-#define SP_ABI_VERSION 1u
+#define SP_ABI_VERSION 2u
 
 #if defined(_WIN32)
 #define SP_API __declspec(dllexport)
@@ -93,6 +93,19 @@ typedef enum sp_precision {
     SP_PRECISION_FP32 = 1  /* FP32 stepping; FP64 time, field phase, ensemble sums,
                               Newton acceptance test                                 */
 } sp_precision;
+
+/* Newton matrix of ImplicitMidpoint, S = -I + dt/2 J_a + 1/2 J_b at the midpoint
+ * (Implicit_Midpoint.inl:83-98).  REFERENCE uses the problems' own Jacobians as
+ * the reference defines them (NeelRelaxation.h:134-190 with its -2 alpha/dt [m]x
+ * term and the b Jacobian's cross-product part only; CubicAnisotropy.h:228-236
+ * J_H = I; BrownAndNeelRelaxation.h:178-187 J = 0), so the iteration matches the
+ * reference step for step.  EXACT uses the analytic Jacobians of a(y) and
+ * b(y)·dW (Neel Cartesian, uniaxial and cubic): the same fixed point, reached in
+ * fewer iterations (quadratic convergence); other problems refuse it. */
+typedef enum sp_jacobian {
+    SP_JACOBIAN_REFERENCE = 0,
+    SP_JACOBIAN_EXACT = 1
+} sp_jacobian;
 
 typedef enum sp_noise {
     SP_NOISE_PHILOX = 0,   /* counter-based Philox4x32-10 + Box-Muller, in-kernel    */
@@ -155,6 +168,8 @@ typedef struct sp_ensemble_desc {
     int32_t max_iteration;       /* Solver_Settings Max_Iterations (ImplicitMidpoint) */
     int32_t record_trajectories; /* keep per-particle window means on the device (parity
                                     runs; the reference's per-particle result vectors) */
+    int32_t jacobian;            /* sp_jacobian (ImplicitMidpoint only)               */
+    int32_t reserved0;
     double accuracy_goal;        /* Solver_Settings Accuracy_Goal (ImplicitMidpoint)  */
     uint64_t number_of_steps;    /* Simulation_Settings Number_of_steps               */
     uint64_t oversampling;       /* Simulation_Settings OverSampling (window W)       */

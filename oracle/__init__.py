@@ -51,6 +51,8 @@ def lib():
         L.oracle_eval_problem.restype = C.c_int
         L.oracle_eval_problem.argtypes = [C.c_int, C.c_int, _dp, _dp, _dp, _dp, _dp, C.c_double, _dp,
                                           _dp, _dp, _dp, _dp, _dp, _dp, _dp, C.POINTER(C.c_int), C.c_int]
+        L.oracle_neel_exact_jacobians.restype = None
+        L.oracle_neel_exact_jacobians.argtypes = [C.c_int] + [_dp] * 7
         L.oracle_count_ops.restype = C.c_int
         L.oracle_count_ops.argtypes = [C.c_void_p, _dp]
         _lib = L
@@ -148,6 +150,15 @@ def eval_problem(problem: int, aniso: int, props, euler, settings, state, field=
         raise RuntimeError(f"oracle_eval_problem failed ({rc})")
     out["rotated"] = (bool(rot[0]), bool(rot[1]))
     return out
+
+
+def neel_exact_jacobians(aniso: int, props, euler, m, field, dW):
+    """Analytic d a/d m and d (b(m) dW)/d m of the Neel (Cartesian) problem.
+    props: radius, Ms, alpha, gamma, K, temperature."""
+    arr = [np.ascontiguousarray(v, dtype=float) for v in (props, euler, m, field, dW)]
+    jd, js = np.zeros((3, 3)), np.zeros((3, 3))
+    lib().oracle_neel_exact_jacobians(int(aniso), *[_p(a) for a in arr], _p(jd), _p(js))
+    return jd, js
 
 
 def count_ops(spec: EnsembleSpec) -> dict:

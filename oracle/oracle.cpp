@@ -200,7 +200,7 @@ struct Stepper {
     // with S = -I + dt/2 J_a + 1/2 J_b (:83-98), initial guess y_n (:56),
     // accept when |dy| <= AccuracyGoal (legacy loop :175), at most MaxIteration.
     static Dep implicit_midpoint(P& pr, const Dep& yi, const V3<T>& xj, const Vec<T, M>& dW, const T& dt,
-                                 int maxIter, double tol, NewtonStats& st) {
+                                 int maxIter, double tol, bool exact, NewtonStats& st) {
         Dep yj = yi;
         bool converged = false;
         for (int it = 0; it < maxIter; ++it) {
@@ -209,8 +209,14 @@ struct Stepper {
             pr.prepareJacobiCalculations(res);
             const Dep a = pr.getDeterministicVector(res, xj);
             const auto b = pr.getStochasticMatrix(res);
-            const auto Ja = pr.getJacobiDeterministic(res, xj, dt);
-            const auto Jb = pr.getJacobiStochastic(dW);
+            auto Ja = pr.getJacobiDeterministic(res, xj, dt);
+            auto Jb = pr.getJacobiStochastic(dW);
+            if constexpr (P::HasExactJacobian) {
+                if (exact) {  // analytic Newton matrix (not in the reference)
+                    Ja = pr.getJacobiDeterministicExact(res, xj);
+                    Jb = pr.getJacobiStochasticExact(res, dW);
+                }
+            }
             auto S = (Mat<T, D, D>::identity() * T(-1.0) + (T(0.5) * dt) * Ja) + T(0.5) * Jb;
             res = res + (a * dt + b * dW);
             pr.finishCalculations(res);
@@ -235,6 +241,7 @@ struct SimSpec {
     int problem, aniso, solver;
     ProblemCfg cfg;
     int maxIter; double tol;
+    bool exactJacobian;
     uint64_t steps, W; double dt;
     FieldEval field;
     uint64_t seed, pid_offset;
@@ -279,7 +286,8 @@ void simulate_particle(const SimSpec& sp, const ParticleIn& pin, uint64_t p, dou
             if (sp.solver == SP_SOLVER_IMPLICIT_MIDPOINT) {
                 sp.field.eval(time + 0.5 * sp.dt, B);  // Implicit_Midpoint.inl:59
                 for (int i = 0; i < 3; ++i) xi[i] = T(B[i]);
-                if constexpr (P::HasJacobian) yi = Stepper<P, T>::implicit_midpoint(pr, yi, xi, dW, dt, sp.maxIter, sp.tol, nst);
+                if constexpr (P::HasJacobian)
+                    yi = Stepper<P, T>::implicit_midpoint(pr, yi, xi, dW, dt, sp.maxIter, sp.tol, sp.exactJacobian, nst);
             } else {
                 sp.field.eval(time, B);  // field at t_{n+1} (SingleParticleSimulator.h:145-146)
                 for (int i = 0; i < 3; ++i) xi[i] = T(B[i]);
@@ -382,6 +390,7 @@ SimSpec spec_of(const sp_ensemble_desc& d) {
     s.cfg.neelMinAngle = d.problem_settings.neel_min_angle_before_transformation;
     s.cfg.simpleModel = d.problem_settings.use_simple_model != 0;
     s.maxIter = d.max_iteration; s.tol = d.accuracy_goal;
+    s.exactJacobian = d.jacobian == SP_JACOBIAN_EXACT;
     s.steps = d.number_of_steps; s.W = d.oversampling; s.dt = d.timestep;
     s.field.init(d.field);
     s.seed = d.seed; s.pid_offset = d.particle_id_offset;
@@ -420,7 +429,7 @@ using namespace orc;
 
 extern "C" {
 
-int oracle_abi_version(void) { return 1; }
+int oracle_abi_version(void) { return 2; }
 
 // Runs the ensemble described by desc.  mean[K][OUT], weight[OUT], time[K],
 // field[K][3], traj[N][K][OUT] and final_state[N][D] are optional (NULL).
@@ -429,6 +438,8 @@ int oracle_simulate(const sp_ensemble_desc* d, double* mean, double* weight, dou
                     double* traj, double* final_state, uint64_t* newton_stats, int nthreads, int precision_mode) {
     if (!d || d->oversampling == 0 || d->number_of_steps < d->oversampling) return 1;
     if (d->solver == SP_SOLVER_IMPLICIT_MIDPOINT && d->problem == SP_PROBLEM_BROWN_AND_NEEL_EULER_SPHERICAL) return 2;
+    if (d->solver == SP_SOLVER_IMPLICIT_MIDPOINT && d->jacobian == SP_JACOBIAN_EXACT && d->problem != SP_PROBLEM_NEEL)
+        return 3;
     const SimSpec s = spec_of(*d);
     const int OUT = out_dim(d->problem), SD = state_dim(d->problem);
     const uint64_t K = s.steps / s.W, N = d->n_particles;
@@ -540,6 +551,28 @@ void oracle_cubic(double K1, double Ms, double radius, const double* m, const do
     const V3<double> h = cb.getAnisotropyField(mm, xx, yy, zz);
     const V3<double> t = cb.getEffTorque(mm, xx, yy, zz, statesin, statecos);
     for (int i = 0; i < 3; ++i) { field[i] = h[i]; torque[i] = t[i]; }
+}
+
+// Exact Neel (Cartesian) Jacobians at state m (the analytic Newton matrix of
+// SP_JACOBIAN_EXACT): jdet[9] = d a / d m, jsto[9] = d (b(m) dW) / d m, row-major.
+// props: radius, Ms, alpha, gamma, K, temperature
+void oracle_neel_exact_jacobians(int aniso, const double* props, const double* euler, const double* m,
+                                 const double* field, const double* dW, double* jdet, double* jsto) {
+    ParticleIn pin{};
+    pin.radius = props[0]; pin.Ms = props[1]; pin.alpha = props[2]; pin.gamma = props[3]; pin.K = props[4];
+    pin.temperature = props[5];
+    for (int i = 0; i < 3; ++i) { pin.euler[i] = euler[i]; pin.mag[i] = 0.0; }
+    ProblemCfg cfg;
+    auto run = [&](auto& pr) {
+        pr.init(pin, cfg);
+        V3<double> y, B, w;
+        for (int i = 0; i < 3; ++i) { y[i] = m[i]; B[i] = field[i]; w[i] = dW[i]; }
+        const auto Ja = pr.getJacobiDeterministicExact(y, B);
+        const auto Jb = pr.getJacobiStochasticExact(y, w);
+        for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) { jdet[3 * i + j] = Ja(i, j); jsto[3 * i + j] = Jb(i, j); }
+    };
+    if (aniso == SP_ANISOTROPY_CUBIC) { NeelProblem<double, Cubic<double>> p; run(p); }
+    else { NeelProblem<double, Uniaxial<double>> p; run(p); }
 }
 
 // Evaluates one problem at one state the way the reference's unit tests do:

@@ -195,6 +195,10 @@ struct Uniaxial {
     M3<T> getJacobiAnisotropyField(const V3<T>&, const V3<T>&, const V3<T>&, const V3<T>& zi) const {
         return outer(prefactorField * zi, zi);  // :130-137
     }
+    // the reference's uniaxial Jacobian is already the exact derivative
+    M3<T> getJacobiAnisotropyFieldExact(const V3<T>& ei, const V3<T>& xi, const V3<T>& yi, const V3<T>& zi) const {
+        return getJacobiAnisotropyField(ei, xi, yi, zi);
+    }
 };
 
 // Problems/Anisotropy/CubicAnisotropy.h:92-236
@@ -227,6 +231,20 @@ struct Cubic {
     }
     M3<T> getJacobiAnisotropyField(const V3<T>&, const V3<T>&, const V3<T>&, const V3<T>&) const {
         return M3<T>::identity();  // placeholder Jacobian in the reference (:228-236)
+    }
+    // exact derivative of getAnisotropyField (:133-146): with c_i = m.a_i,
+    // dH/dm = K1_MS * sum_i a_i [ (c_j^2 + c_k^2) a_i + 2 c_i c_j a_j + 2 c_i c_k a_k ]^T
+    M3<T> getJacobiAnisotropyFieldExact(const V3<T>& ei, const V3<T>& xi, const V3<T>& yi, const V3<T>& zi) const {
+        const V3<T> ax[3] = {xi, yi, zi};
+        const T c[3] = {dot(ei, xi), dot(ei, yi), dot(ei, zi)};
+        M3<T> J = M3<T>::zero();
+        for (int i = 0; i < 3; ++i) {
+            const int j = (i + 1) % 3, k = (i + 2) % 3;
+            const V3<T> row = (c[j] * c[j] + c[k] * c[k]) * ax[i] + (T(2.0) * c[i] * c[j]) * ax[j] +
+                              (T(2.0) * c[i] * c[k]) * ax[k];
+            J = J + outer(ax[i], row);
+        }
+        return K1_MS * J;
     }
 };
 

@@ -94,6 +94,27 @@ struct NeelProblem {
     }
     // :210-214
     Vec<T, OUT> calculateOutputResult(const Dep& yi) const { return yi; }
+
+    // Exact Jacobians (not in the reference; its versions above keep the
+    // -2 alpha/dt [m]x stand-in and drop the damping and projection derivatives).
+    //   a = NF1 u - NF2 m x u, u = m x Heff(m):  J_u = [m]x J_H - [Heff]x,
+    //   J_a = NF1 J_u - NF2 ([m]x J_u - [u]x)
+    static constexpr bool HasExactJacobian = true;
+    Mat<T, 3, 3> getJacobiDeterministicExact(const Dep& yi, const V3<T>& xi) const {
+        mAnisotropy.prepareField(yi, xAxis, yAxis, zAxis);
+        const V3<T> Heff = mAnisotropy.getAnisotropyField(yi, xAxis, yAxis, zAxis) + xi;
+        const M3<T> JH = mAnisotropy.getJacobiAnisotropyFieldExact(yi, xAxis, yAxis, zAxis);
+        const M3<T> mx = crossmat(yi);
+        const M3<T> Ju = mx * JH - crossmat(Heff);
+        const M3<T> Jv = mx * Ju - crossmat(cross(yi, Heff));
+        return NeelFactor1 * Ju - NeelFactor2 * Jv;
+    }
+    //   b(m) dW = pre2 (dW - m (m.dW)) + pre1 m x dW:  J = -pre2 ((m.dW) I + m dW^T) - pre1 [dW]x
+    Mat<T, 3, 3> getJacobiStochasticExact(const Dep& yi, const Vec<T, 3>& dW) const {
+        const T pre2 = NeelFactor2 * NoisePrefactor;
+        const T pre1 = NeelFactor1 * NoisePrefactor;
+        return (T(-1.0) * pre2) * (dot(yi, dW) * M3<T>::identity() + outer(yi, dW)) - pre1 * crossmat(dW);
+    }
 };
 
 // ====================================================================== Neel (spherical)
@@ -102,6 +123,7 @@ template <class T, class Aniso>
 struct NeelSphericalProblem {
     static constexpr int D = 2, M = 3, OUT = 3;
     static constexpr bool HasJacobian = true;
+    static constexpr bool HasExactJacobian = false;
     using Dep = Vec<T, 2>;
     T NeelFactor1, NeelFactor2, DriftPrefactor, NoisePrefactor, Damping;
     V3<T> xAxis, yAxis, zAxis;
@@ -299,6 +321,7 @@ template <class T, class Aniso>
 struct BrownNeelEulerProblem {
     static constexpr int D = 5, M = 6, OUT = 9;
     static constexpr bool HasJacobian = false;  // assert(false) in the reference (:605-626)
+    static constexpr bool HasExactJacobian = false;
     using Dep = Vec<T, 5>;
     T a_, b_, DN, c_, DB, cF, MagneticMoment;  // NeelFactor1/2, NoisePrefactor, BrownPrefactor/Diffusion, Brown_F_Noise
     Aniso mAnisotropy;
@@ -529,6 +552,7 @@ template <class T, class Aniso, bool IsCubic>
 struct BrownNeelProblem {
     static constexpr int D = 6, M = 6, OUT = 6;
     static constexpr bool HasJacobian = true;
+    static constexpr bool HasExactJacobian = false;
     using Dep = Vec<T, 6>;
     T a_, b_, DN, c_, cF, MagneticMoment;
     Aniso mAnisotropy;

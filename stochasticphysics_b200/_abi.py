@@ -13,7 +13,7 @@ from typing import Optional
 
 import numpy as np
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 
 
 class Status(IntEnum):
@@ -66,6 +66,11 @@ class Precision(IntEnum):
 class Noise(IntEnum):
     Philox = 0
     Injected = 1
+
+
+class Jacobian(IntEnum):
+    Reference = 0
+    Exact = 1
 
 
 class RequestState(IntEnum):
@@ -135,6 +140,8 @@ class sp_ensemble_desc(C.Structure):
         ("problem_settings", sp_problem_settings),
         ("max_iteration", C.c_int32),
         ("record_trajectories", C.c_int32),
+        ("jacobian", C.c_int32),
+        ("reserved0", C.c_int32),
         ("accuracy_goal", C.c_double),
         ("number_of_steps", C.c_uint64),
         ("oversampling", C.c_uint64),
@@ -281,6 +288,7 @@ class EnsembleSpec:
     use_simple_model: bool = False
     injected_dw: Optional[np.ndarray] = None
     record_trajectories: bool = False
+    jacobian: Jacobian = Jacobian.Reference
 
     @property
     def dims(self):
@@ -344,6 +352,7 @@ class DescHolder:
         ps.neel_min_angle_before_transformation = float(spec.neel_min_angle_before_transformation)
         d.max_iteration = int(spec.max_iteration)
         d.record_trajectories = int(bool(spec.record_trajectories))
+        d.jacobian = int(spec.jacobian)
         d.accuracy_goal = float(spec.accuracy_goal)
         d.number_of_steps = int(spec.number_of_steps)
         d.oversampling = int(spec.oversampling)

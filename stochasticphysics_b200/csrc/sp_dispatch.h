@@ -17,12 +17,18 @@ struct KernelSet {
     const void* step_fn = nullptr;  // for cudaFuncGetAttributes / occupancy queries
 };
 
-// index: problem, anisotropy, solver, precision (0 FP64, 1 FP32), injected noise
+// index: problem, anisotropy, solver slot (sp_solver, or kImplicitMidpointExact),
+// precision (0 FP64, 1 FP32), injected noise
 const KernelSet& kernel_set(int problem, int aniso, int solver, int precision, int inject);
+constexpr int kSolverSlots = 5;
 inline int kernel_index(int aniso, int solver, int precision, int inject) {
-    return ((aniso * 4 + solver) * 2 + precision) * 2 + inject;
+    return ((aniso * kSolverSlots + solver) * 2 + precision) * 2 + inject;
 }
-constexpr int kKernelsPerProblem = 32;
+constexpr int kKernelsPerProblem = 2 * kSolverSlots * 2 * 2;
+// solver slot of a description: ImplicitMidpoint with SP_JACOBIAN_EXACT has its own kernels
+inline int solver_slot(int solver, int jacobian) {
+    return (solver == kImplicitMidpoint && jacobian == 1) ? kImplicitMidpointExact : solver;
+}
 
 void fill_neel(KernelSet* tab);
 void fill_neel_spherical(KernelSet* tab);

@@ -29,6 +29,8 @@ KernelSet make_set() {
     KernelSet k;
     if constexpr (SOLVER == kImplicitMidpoint && !Prob::kHasJacobian) {
         return k;  // not supported by the reference either
+    } else if constexpr (SOLVER == kImplicitMidpointExact && !Prob::kHasExactJacobian) {
+        return k;  // no analytic Newton matrix for this problem
     } else {
         k.valid = true;
         k.D = Prob::D; k.Mn = Prob::Mn; k.OUT = Prob::OUT; k.P = ProblemOf<PROB, R, A>::P;
@@ -55,6 +57,7 @@ void fill_aniso(KernelSet* tab) {
     fill_solver<PROB, A, kHeun>(tab);
     fill_solver<PROB, A, kMillstein>(tab);
     fill_solver<PROB, A, kImplicitMidpoint>(tab);
+    fill_solver<PROB, A, kImplicitMidpointExact>(tab);
 }
 template <int PROB>
 void fill_problem(KernelSet* tab) {

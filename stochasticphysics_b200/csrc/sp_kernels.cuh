@@ -298,7 +298,7 @@ __global__ void __launch_bounds__(kMaxBlock) step_kernel(const EnsDev* __restric
             for (int c = 0; c < OUT; ++c) { ks[c * Np + p] = sum[c]; kc[c * Np + p] = comp[c]; }
             if (!finite) e.status[p] = 1;
         }
-        if constexpr (SOLVER == kImplicitMidpoint) {
+        if constexpr (SOLVER == kImplicitMidpoint || SOLVER == kImplicitMidpointExact) {
             unsigned int it = nc.iterations, un = nc.unconverged;
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) { it += __shfl_xor_sync(0xffffffffu, it, o); un += __shfl_xor_sync(0xffffffffu, un, o); }

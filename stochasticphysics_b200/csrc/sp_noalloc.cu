@@ -94,7 +94,8 @@ extern "C" SP_API sp_status sp_simulate_noalloc(const sp_ensemble_desc* desc, co
         check_cuda(cudaDeviceGetAttribute(&c.sms, cudaDevAttrMultiProcessorCount, device), "cudaDeviceGetAttribute");
         const LaunchConfig lc = default_launch(&c, *desc);
         const EnsembleLayout L = layout_of(*desc, lc);
-        const KernelSet& ks = kernel_set(desc->problem, desc->anisotropy, desc->solver, desc->precision, 0);
+        const KernelSet& ks = kernel_set(desc->problem, desc->anisotropy, solver_slot(desc->solver, desc->jacobian),
+                                         desc->precision, 0);
         if (!ks.valid) return fail(SP_ERR_UNSUPPORTED_COMBO, "no kernel for this problem/solver combination");
 
         // carve the scratch

@@ -41,6 +41,40 @@ struct Aniso {
             return pF * (((c2s + c3s) * c1) * x + ((c1s + c3s) * c2) * y + ((c1s + c2s) * c3) * z) + B;
         }
     }
+    // analytic dH/dm.  Uniaxial: pF z z^T (UniaxialAnisotropy.h:130-137, exact already).
+    // Cubic: H = pF sum_i c_i (c_j^2 + c_k^2) a_i with c_i = m.a_i, so
+    // dH/dm = pF sum_il G_il a_i a_l^T, G_ii = c_j^2 + c_k^2, G_il = 2 c_i c_l (the
+    // reference returns the identity here, CubicAnisotropy.h:228-236).
+    static __device__ __forceinline__ void jacobian(R pF, V3<R> m, V3<R> x, V3<R> y, V3<R> z, R J[3][3]) {
+        if constexpr (A == kUniaxial) {
+            const R zz[3] = {z.x, z.y, z.z};
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) J[i][j] = (pF * zz[i]) * zz[j];
+        } else {
+            const R c[3] = {dot(m, x), dot(m, y), dot(m, z)};
+            const R a[3][3] = {{x.x, x.y, x.z}, {y.x, y.y, y.z}, {z.x, z.y, z.z}};  // a[i] = axis i
+            R G[3][3];
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int l = 0; l < 3; ++l)
+                    G[i][l] = (i == l) ? (c[(i + 1) % 3] * c[(i + 1) % 3] + c[(i + 2) % 3] * c[(i + 2) % 3])
+                                       : R(2) * c[i] * c[l];
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+#pragma unroll
+                for (int col = 0; col < 3; ++col) {
+                    R acc = R(0);
+#pragma unroll
+                    for (int i = 0; i < 3; ++i)
+#pragma unroll
+                        for (int l = 0; l < 3; ++l) acc = acc + (G[i][l] * a[i][r]) * a[l][col];
+                    J[r][col] = pF * acc;
+                }
+        }
+    }
 };
 
 // ======================================================================= Neel (Cartesian)
@@ -108,6 +142,35 @@ struct NeelCart {
                 S[i][j] = (i == j ? R(-1) : R(0)) + (R(0.5) * dt) * jdet + R(0.5) * jsto;
             }
     }
+    static constexpr bool kHasExactJacobian = true;
+    // S = -I + dt/2 J_a + 1/2 J_b with the analytic Jacobians at the midpoint m:
+    //   a = NF1 u - NF2 (m x u), u = m x H(m):  J_u = [m]x J_H - [H]x,
+    //   J_a = NF1 J_u - NF2 ([m]x J_u - [u]x);
+    //   b.w = pre2 (w - m (m.w)) + pre1 (m x w):  J_b = -pre2 ((m.w) I + m w^T) - pre1 [w]x.
+    // Column j of [v]x is v x e_j.
+    static __device__ __forceinline__ void newton_matrix_exact(const Par& q, const R* y, const Cache&, const R* B,
+                                                               const R* w, R dt, R S[D][D]) {
+        const V3<R> m = v3(y[0], y[1], y[2]);
+        const V3<R> H = Aniso<R, A>::heff(q.pF, m, q.x, q.y, q.z, v3(B[0], B[1], B[2]));
+        R JH[3][3];
+        Aniso<R, A>::jacobian(q.pF, m, q.x, q.y, q.z, JH);
+        const V3<R> u = cross(m, H);
+        const V3<R> W = v3(w[0], w[1], w[2]);
+        const R mw = dot(m, W);
+        const R wv[3] = {w[0], w[1], w[2]};
+        const R hdt = R(0.5) * dt;
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            const V3<R> ej = v3(R(j == 0), R(j == 1), R(j == 2));
+            const V3<R> Ju = cross(m, v3(JH[0][j], JH[1][j], JH[2][j])) - cross(H, ej);
+            const V3<R> Jv = cross(m, Ju) - cross(u, ej);
+            const V3<R> Ja = q.NF1 * Ju - q.NF2 * Jv;
+            const V3<R> Jb = (-q.pre2) * (mw * ej + wv[j] * m) - q.pre1 * cross(W, ej);
+            S[0][j] = (j == 0 ? R(-1) : R(0)) + hdt * Ja.x + R(0.5) * Jb.x;
+            S[1][j] = (j == 1 ? R(-1) : R(0)) + hdt * Ja.y + R(0.5) * Jb.y;
+            S[2][j] = (j == 2 ? R(-1) : R(0)) + hdt * Ja.z + R(0.5) * Jb.z;
+        }
+    }
 };
 
 // ======================================================================= Neel (spherical)
@@ -115,6 +178,7 @@ template <class R, int A>
 struct NeelSph {
     static constexpr int D = 2, Mn = 3, OUT = 3;
     static constexpr bool kHasJacobian = true;
+    static constexpr bool kHasExactJacobian = false;
     struct Par {
         R NF1, NF2, Dp, DN, pF, twoalpha;
         V3<R> z, x, y;
@@ -264,6 +328,7 @@ template <class R, int A>
 struct BrownNeelEuler {
     static constexpr int D = 5, Mn = 6, OUT = 9;
     static constexpr bool kHasJacobian = false;  // assert(false) in the reference (:605-626)
+    static constexpr bool kHasExactJacobian = false;
     struct Par {
         R a, bpd, d, cT, pF, cF, dDN, bpdDN, aDN, adDN2, d2fDN2, cF2h, nd;
     };
@@ -467,6 +532,7 @@ template <class R, int A>
 struct BrownNeelCart {
     static constexpr int D = 6, Mn = 6, OUT = 6;
     static constexpr bool kHasJacobian = true;  // both Jacobians are zero in the reference (.h:119-128)
+    static constexpr bool kHasExactJacobian = false;
     struct Par {
         R a, bpd, d, cT, pF, cF, dDN, bpdDN, aDN, cF2, adDN2, hd2DN2, ndrift, cFe;
     };
@@ -628,7 +694,8 @@ struct Stepper {
                     R a[D], bw[D], S[D][D];
                     P::det(q, r, c, B, a);
                     P::bdw(q, r, c, w, bw);
-                    P::newton_matrix(q, r, c, B, w, dt, S);
+                    if constexpr (SOLVER == kImplicitMidpointExact) P::newton_matrix_exact(q, r, c, B, w, dt, S);
+                    else P::newton_matrix(q, r, c, B, w, dt, S);
 #pragma unroll
                     for (int i = 0; i < D; ++i) r[i] = r[i] + (a[i] * dt + bw[i]);
                     P::finish(rot, r, c);

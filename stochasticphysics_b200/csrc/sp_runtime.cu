@@ -75,7 +75,12 @@ sp_status validate_desc(const sp_ensemble_desc* d, std::string& why) {
         }
         if (d->max_iteration < 1 || d->max_iteration > 1000) return bad("ImplicitMidpoint needs 1 <= max_iteration <= 1000");
         if (!(d->accuracy_goal > 0.0)) return bad("ImplicitMidpoint needs accuracy_goal > 0");
+        if (d->jacobian == SP_JACOBIAN_EXACT && d->problem != SP_PROBLEM_NEEL) {
+            why = "the exact Newton Jacobian is implemented for the Neel (Cartesian) problem only";
+            return SP_ERR_UNSUPPORTED_COMBO;
+        }
     }
+    if (d->jacobian != SP_JACOBIAN_REFERENCE && d->jacobian != SP_JACOBIAN_EXACT) return bad("unknown jacobian mode");
     const unsigned long long K = d->number_of_steps / d->oversampling;
     if (K > (1ull << 31)) return bad("too many samples");
     return SP_OK;
@@ -130,7 +135,8 @@ void* Ensemble::dalloc(size_t bytes) {
 }
 
 Ensemble::Ensemble(sp_context* c, const sp_ensemble_desc& d, const LaunchConfig& lc) : ctx(c), desc(d), launch(lc) {
-    ks = &kernel_set(d.problem, d.anisotropy, d.solver, d.precision, d.noise == SP_NOISE_INJECTED ? 1 : 0);
+    ks = &kernel_set(d.problem, d.anisotropy, solver_slot(d.solver, d.jacobian), d.precision,
+                     d.noise == SP_NOISE_INJECTED ? 1 : 0);
     if (!ks->valid) throw Error(SP_ERR_UNSUPPORTED_COMBO, "no kernel for this problem/solver combination");
     L = layout_of(d, lc);
     check_cuda(cudaSetDevice(ctx->device), "cudaSetDevice");

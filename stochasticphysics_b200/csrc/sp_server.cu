@@ -89,7 +89,8 @@ struct sp_server {
     std::map<int, Group> groups;  // key -> group
 
     static int key_of(const sp_ensemble_desc& d) {
-        return (((d.problem * 2 + d.anisotropy) * 4 + d.solver) * 2 + d.precision) * 2 + (d.noise == SP_NOISE_INJECTED);
+        return (((d.problem * 2 + d.anisotropy) * kSolverSlots + solver_slot(d.solver, d.jacobian)) * 2 + d.precision) * 2 +
+               (d.noise == SP_NOISE_INJECTED);
     }
 
     LaunchConfig launch_for(const sp_ensemble_desc& d) const {

@@ -28,8 +28,9 @@ std::unordered_map<std::string, LaunchConfig> g_tuned;
 std::unordered_map<std::string, double> g_tuned_rate;
 
 std::string key_of(const sp_ensemble_desc& d) {
-    return std::to_string(d.problem) + "/" + std::to_string(d.anisotropy) + "/" + std::to_string(d.solver) + "/" +
-           std::to_string(d.precision) + "/" + std::to_string(d.noise);
+    return std::to_string(d.problem) + "/" + std::to_string(d.anisotropy) + "/" +
+           std::to_string(solver_slot(d.solver, d.jacobian)) + "/" + std::to_string(d.precision) + "/" +
+           std::to_string(d.noise);
 }
 
 unsigned long long round_chunk(unsigned long long chunk, unsigned long long W) {

@@ -20,7 +20,7 @@ import pytest
 import oracle
 import stochasticphysics_b200 as sp
 from stochasticphysics_b200 import provider
-from stochasticphysics_b200._abi import Anisotropy, Noise, Precision, Problem, Solver
+from stochasticphysics_b200._abi import Anisotropy, Jacobian, Noise, Precision, Problem, Solver
 
 pytestmark = pytest.mark.gpu
 
@@ -137,6 +137,34 @@ def test_injection_parity_fp64(ctx, problem, solver, aniso):
         assert gpu.stats["newton_iterations"] > 0
         # converged roots agree; iteration counts may differ by a few per run
         assert abs(gpu.stats["newton_iterations"] - ref["newton_iterations"]) <= 0.01 * ref["newton_iterations"] + 5
+
+
+@pytest.mark.parametrize("aniso", [Anisotropy.Uniaxial, Anisotropy.Cubic])
+def test_exact_jacobian_parity_fp64(ctx, aniso):
+    """ImplicitMidpoint with the analytic Newton matrix: same bars as the reference
+    mode, every step converged, iteration counts as in the oracle."""
+    spec = provider.with_injected_noise(small_spec(Problem.Neel, Solver.Implicit_Midpoint, aniso), seed=3)
+    spec = dataclasses.replace(spec, max_iteration=20, accuracy_goal=1e-10, jacobian=Jacobian.Exact)
+    gpu = ctx.simulate(spec, trajectories=True, final_state=True)
+    ref = oracle.simulate(spec, trajectories=True, final_state=True)
+    rel, mabs = conditioned_bars(spec, ref)
+    compare(gpu, ref, rel=rel, mean_abs=mabs)
+    assert gpu.stats["newton_unconverged"] == 0 and ref["newton_unconverged"] == 0
+    assert abs(gpu.stats["newton_iterations"] - ref["newton_iterations"]) <= 0.01 * ref["newton_iterations"] + 5
+    assert gpu.stats["newton_iterations"] <= 4.1 * spec.n * spec.integrated_steps
+
+
+def test_exact_jacobian_fp32_state_with_fp64_acceptance(ctx):
+    """The stiff cubic ImplicitMidpoint workload in the FP32 form (FP32 state, FP64
+    residual acceptance) against the all-FP64 kernel, both with the exact Newton matrix."""
+    base = dataclasses.replace(provider.cubic_implicit(n=4096, steps=3000, oversampling=100),
+                               jacobian=Jacobian.Exact)
+    r64 = ctx.simulate(base)
+    r32 = ctx.simulate(dataclasses.replace(base, precision=Precision.FP32))
+    steps = base.n * base.integrated_steps
+    assert r64.stats["newton_unconverged"] == 0
+    assert r32.stats["newton_unconverged"] <= 1e-3 * steps
+    assert np.max(np.abs(r32.mean - r64.mean)) < 1e-3
 
 
 def test_runaway_particles_match(ctx):
