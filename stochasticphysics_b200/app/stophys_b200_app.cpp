@@ -13,11 +13,18 @@
 // excitation, Frequency_1, Phase_1) and the older per-file anisotropy keys
 // (Anisotropy_1, Anisotropy_constants_distribution_*).
 //
-// Usage: stophys_b200 -parfile:<ini> [-out:<json>] [-device:N] [-seed:S]
-//                     [-precision:fp64|fp32] [-print]
+// Usage: stophys_b200 -parfile:<ini> [-sysmatrix:<ini>] [-out:<json>] [-device:N]
+//                     [-seed:S] [-precision:fp64|fp32] [-print]
 //   -print parses the files, runs the provider and validates the description
-//   without touching a GPU; it writes the description and every particle.
+//   without touching a GPU; it writes the description and every particle (with
+//   -sysmatrix: the voxels and their offset fields).
+//   -sysmatrix runs the system-matrix sweep of the reference
+//   (Settings/SystemMatrixSettings.h, Settings/SystemMatrix_SimulationManagerSettings_Factory.h,
+//   Simulator/SimulationApplication.cpp:80-128): one ensemble per voxel with the
+//   offset field shifted to the voxel's field, all voxels submitted to the
+//   continuous-batching server so they share batched launches.
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -453,6 +460,86 @@ Run build(const std::string& path, unsigned long long seed, int precision) {
     return run;
 }
 
+// ------------------------------------------------------------------ system matrix
+// [System_Matrix_Settings] Startfield, Stopfield, Slices, Use_start_stop_Voxel,
+// Start_Voxel, Stop_Voxel (SystemMatrixSettings.h:276-303)
+struct SysMat {
+    double start[3] = {0, 0, 0}, stop[3] = {1, 1, 1};
+    unsigned long long slices[3] = {0, 0, 0}, vstart[3] = {0, 0, 0}, vstop[3] = {1, 1, 1};
+    bool use_start_stop = false;
+
+    static SysMat load(const std::string& path) {
+        const Ini ini = Ini::load(path);
+        SysMat m;
+        auto vec3 = [&](const char* k, double* dst, bool required) {
+            const std::string* v = ini.within("System_Matrix_Settings", k);
+            if (!v) {
+                if (required) throw std::runtime_error(std::string("missing key ") + k + " in [System_Matrix_Settings]");
+                return;
+            }
+            const auto a = Ini::vec(*v);
+            if (a.size() != 3) throw std::runtime_error(std::string(k) + " needs three values");
+            std::copy(a.begin(), a.end(), dst);
+        };
+        auto idx3 = [&](const char* k, unsigned long long* dst, bool required) {
+            double t[3] = {0, 0, 0};
+            vec3(k, t, required);
+            for (int i = 0; i < 3; ++i) {
+                if (t[i] < 0 || t[i] != std::floor(t[i])) throw std::runtime_error(std::string(k) + " must hold non-negative integers");
+                dst[i] = static_cast<unsigned long long>(t[i]);
+            }
+        };
+        vec3("Startfield", m.start, true);
+        vec3("Stopfield", m.stop, true);
+        idx3("Slices", m.slices, true);
+        if (auto v = ini.within("System_Matrix_Settings", "Use_start_stop_Voxel")) m.use_start_stop = Ini::boolean(*v);
+        for (int i = 0; i < 3; ++i) {
+            if (m.slices[i] < 1) throw std::runtime_error("SystemMatrixSettings: Number of Voxels must be at least one for every dimension!");
+            // a single slice needs Startfield == Stopfield in that direction (:52-76)
+            if (m.slices[i] == 1 && std::abs(m.stop[i] - m.start[i]) > 1e-15 * std::max(1.0, std::abs(m.stop[i])))
+                throw std::runtime_error("SystemMatrixSettings: Invalid Parameters. Unable to calculate VoxelSize.");
+        }
+        if (m.use_start_stop) {
+            idx3("Start_Voxel", m.vstart, true);
+            idx3("Stop_Voxel", m.vstop, true);
+            for (int i = 0; i < 3; ++i)
+                if (m.vstart[i] > m.slices[i] || m.vstop[i] > m.slices[i])
+                    throw std::runtime_error("SystemMatrixSettings: Start/Stop voxel beyond the defined slices");
+        } else {
+            for (int i = 0; i < 3; ++i) { m.vstart[i] = 0; m.vstop[i] = m.slices[i] - 1; }
+        }
+        return m;
+    }
+    // Size_FOV / max(slices - 1, 1) per direction (:247-268)
+    void voxel_size(double* out) const {
+        for (int i = 0; i < 3; ++i)
+            out[i] = (stop[i] - start[i]) / static_cast<double>(slices[i] > 1 ? slices[i] - 1 : 1);
+    }
+    // getNumberVoxelsToSimulate (:159-182), including its signed-difference rule
+    unsigned long long count() const {
+        if (!use_start_stop) return slices[0] * slices[1] * slices[2];
+        auto absdiff = [](unsigned long long a, unsigned long long b) { return a > b ? a - b : b - a; };
+        const unsigned long long zp = absdiff(vstart[2], vstop[2]) * slices[0] * slices[1];
+        const unsigned long long yp = absdiff(vstart[1], vstop[1]) * slices[0];
+        const unsigned long long xp = absdiff(vstart[0], vstop[0]);
+        return vstart[0] > vstop[0] ? yp + zp - xp : xp + yp + zp;
+    }
+    // generateSimulationVoxels (:184-215): z-major from the start voxel, x fastest
+    std::vector<std::array<unsigned long long, 3>> voxels() const {
+        std::vector<std::array<unsigned long long, 3>> out;
+        const unsigned long long n = count();
+        unsigned long long sv[3] = {vstart[0], vstart[1], vstart[2]};
+        for (unsigned long long z = sv[2]; z < slices[2] && out.size() < n; ++z) {
+            for (unsigned long long y = sv[1]; y < slices[1] && out.size() < n; ++y) {
+                for (unsigned long long x = sv[0]; x < slices[0] && out.size() < n; ++x) out.push_back({x, y, z});
+                sv[0] = 0;
+            }
+            sv[1] = 0;
+        }
+        return out;
+    }
+};
+
 // ------------------------------------------------------------------ JSON
 std::string jnum(double v) {
     if (!std::isfinite(v)) return "null";
@@ -533,10 +620,120 @@ void write_description(std::ostream& o, const Run& run) {
     o << "},\"savefile\":" << jstr(run.savefile) << "}\n";
 }
 
+void write_mean_results(std::ostream& os, const std::vector<double>& time, const std::vector<double>& field,
+                        const std::vector<double>& mean, const std::vector<double>& weight, size_t K, size_t od,
+                        const Run& run) {
+    const sp_ensemble_desc& d = run.d;
+    os << "{\"Time\":";
+    jarr(os, time.data(), K);
+    os << ",\"Field\":";
+    jrows(os, field.data(), K, 3);
+    os << ",\"Results\":";
+    jrows(os, mean.data(), K, od);
+    os << ",\"Weight\":";
+    jarr(os, weight.data(), od);
+    os << ",\"Mean_Properties\":{\"Temperature\":" << jnum(d.temperature)
+       << ",\"Magnetic_radius\":" << jnum(mean_of(run.r)) << ",\"Saturation_magnetisation\":" << jnum(mean_of(run.Ms))
+       << ",\"Damping_constant\":" << jnum(mean_of(run.alpha)) << ",\"Gyromagnetic_ratio\":" << jnum(mean_of(run.gamma))
+       << ",\"Anisotropy_constant\":" << jnum(mean_of(run.K)) << ",\"Hydrodynamic_Radius\":" << jnum(mean_of(run.rh))
+       << ",\"Viscosity\":" << jnum(mean_of(run.eta)) << "}}";
+}
+
+// File name of one voxel's result: Savefile stem + "_Vox_x_y_z" + extension
+// (SystemMatrix_SimulationManagerSettings_Factory.h:44-63)
+std::string voxel_file(const std::string& savefile, const std::array<unsigned long long, 3>& v) {
+    const std::string base = savefile.empty() ? "Result.json" : savefile;
+    const auto slash = base.find_last_of('/');
+    const auto dot = base.find_last_of('.');
+    const bool has_ext = dot != std::string::npos && (slash == std::string::npos || dot > slash);
+    const std::string stem = has_ext ? base.substr(0, dot) : base, ext = has_ext ? base.substr(dot) : "";
+    return stem + "_Vox_" + std::to_string(v[0]) + "_" + std::to_string(v[1]) + "_" + std::to_string(v[2]) + ext;
+}
+
+// One ensemble per voxel: the base description with the offset field moved to
+// Startfield + VoxelSize * voxel (added to the configured offset, :36-42) and its
+// own Philox key (seed + voxel number), all submitted to one server.
+int run_sysmatrix(const Run& run, const SysMat& sm, std::ostream& os, int device, bool print_only) {
+    const auto vox = sm.voxels();
+    double size[3];
+    sm.voxel_size(size);
+    std::vector<sp_ensemble_desc> descs;
+    for (size_t i = 0; i < vox.size(); ++i) {
+        sp_ensemble_desc d = run.d;
+        for (int c = 0; c < 3; ++c)
+            d.field.offset[c] = run.d.field.offset[c] + sm.start[c] + size[c] * static_cast<double>(vox[i][c]);
+        d.seed = run.d.seed + i;
+        descs.push_back(d);
+    }
+    auto write_header = [&]() {
+        os << "{\"System_Matrix_Settings\":{\"Startfield\":";
+        jarr(os, sm.start, 3);
+        os << ",\"Stopfield\":";
+        jarr(os, sm.stop, 3);
+        os << ",\"Slices\":[" << sm.slices[0] << "," << sm.slices[1] << "," << sm.slices[2]
+           << "],\"Use_start_stop_Voxel\":" << (sm.use_start_stop ? "true" : "false") << ",\"Start_Voxel\":["
+           << sm.vstart[0] << "," << sm.vstart[1] << "," << sm.vstart[2] << "],\"Stop_Voxel\":[" << sm.vstop[0] << ","
+           << sm.vstop[1] << "," << sm.vstop[2] << "],\"Voxel_Size\":";
+        jarr(os, size, 3);
+        os << "},\"Number_of_voxels\":" << vox.size() << ",\"Voxels\":[";
+    };
+    write_header();
+    if (print_only) {
+        for (size_t i = 0; i < vox.size(); ++i) {
+            os << (i ? "," : "") << "{\"Voxel\":[" << vox[i][0] << "," << vox[i][1] << "," << vox[i][2]
+               << "],\"Offset_Field\":";
+            jarr(os, descs[i].field.offset, 3);
+            os << ",\"Seed\":" << descs[i].seed << ",\"File\":" << jstr(voxel_file(run.savefile, vox[i])) << "}";
+        }
+        os << "]}\n";
+        return 0;
+    }
+    sp_context* ctx = nullptr;
+    if (sp_create(&ctx, device) != SP_OK) throw std::runtime_error(sp_last_error());
+    sp_server* srv = nullptr;
+    sp_server_config cfg{};
+    if (sp_server_create(ctx, &cfg, &srv) != SP_OK) {
+        sp_destroy(ctx);
+        throw std::runtime_error(sp_last_error());
+    }
+    std::vector<uint64_t> ids(descs.size());
+    std::string err;
+    for (size_t i = 0; i < descs.size() && err.empty(); ++i)
+        if (sp_server_submit(srv, &descs[i], &ids[i]) != SP_OK) err = sp_last_error();
+    int32_t sd = 0, nd = 0, od = 0;
+    sp_query_dims(run.d.problem, &sd, &nd, &od);
+    const size_t K = run.d.number_of_steps / run.d.oversampling;
+    uint64_t total_steps = 0;
+    double max_latency = 0.0;
+    for (size_t i = 0; i < descs.size() && err.empty(); ++i) {
+        std::vector<double> mean(K * od), weight(od), time(K), field(3 * K);
+        sp_result res{mean.data(), weight.data(), time.data(), field.data(), nullptr, nullptr};
+        sp_stats st{};
+        double lat = 0.0;
+        if (sp_server_wait(srv, ids[i], -1.0, &res, &st, &lat) != SP_OK) {
+            err = sp_last_error();
+            break;
+        }
+        total_steps += st.particle_steps;
+        max_latency = std::max(max_latency, lat);
+        os << (i ? "," : "") << "{\"Voxel\":[" << vox[i][0] << "," << vox[i][1] << "," << vox[i][2]
+           << "],\"Offset_Field\":";
+        jarr(os, descs[i].field.offset, 3);
+        os << ",\"File\":" << jstr(voxel_file(run.savefile, vox[i])) << ",\"Mean_Results\":";
+        write_mean_results(os, time, field, mean, weight, K, static_cast<size_t>(od), run);
+        os << "}";
+    }
+    sp_server_destroy(srv);
+    sp_destroy(ctx);
+    if (!err.empty()) throw std::runtime_error(err);
+    os << "],\"Stats\":{\"particle_steps\":" << total_steps << ",\"max_latency_ms\":" << jnum(max_latency) << "}}\n";
+    return 0;
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
-    std::string par, out;
+    std::string par, out, sysmatrix;
     int device = 0, precision = SP_PRECISION_FP64;
     unsigned long long seed = 0x5EED;
     bool print_only = false;
@@ -545,6 +742,7 @@ int main(int argc, char** argv) {
         auto val = [&](const char* p) { return a.substr(std::string(p).size()); };
         if (a.rfind("-parfile:", 0) == 0) par = val("-parfile:");
         else if (a.rfind("-out:", 0) == 0) out = val("-out:");
+        else if (a.rfind("-sysmatrix:", 0) == 0) sysmatrix = val("-sysmatrix:");
         else if (a.rfind("-device:", 0) == 0) device = std::atoi(val("-device:").c_str());
         else if (a.rfind("-seed:", 0) == 0) seed = std::strtoull(val("-seed:").c_str(), nullptr, 0);
         else if (a == "-precision:fp32") precision = SP_PRECISION_FP32;
@@ -556,8 +754,8 @@ int main(int argc, char** argv) {
         }
     }
     if (par.empty()) {
-        std::fprintf(stderr, "usage: stophys_b200 -parfile:<ini> [-out:<json>] [-device:N] [-seed:S] "
-                             "[-precision:fp64|fp32] [-print]\n");
+        std::fprintf(stderr, "usage: stophys_b200 -parfile:<ini> [-sysmatrix:<ini>] [-out:<json>] [-device:N] "
+                             "[-seed:S] [-precision:fp64|fp32] [-print]\n");
         return 2;
     }
     try {
@@ -570,6 +768,7 @@ int main(int argc, char** argv) {
             if (!fo) throw std::runtime_error("cannot write " + out);
         }
         std::ostream& os = out.empty() ? std::cout : fo;
+        if (!sysmatrix.empty()) return run_sysmatrix(run, SysMat::load(sysmatrix), os, device, print_only);
         if (print_only) {
             write_description(os, run);
             return 0;
@@ -585,19 +784,9 @@ int main(int argc, char** argv) {
         const sp_status s = sp_simulate(ctx, &d, &res, &st);
         sp_destroy(ctx);
         if (s != SP_OK) throw std::runtime_error(sp_last_error());
-        os << "{\"Mean_Results\":{\"Time\":";
-        jarr(os, time.data(), K);
-        os << ",\"Field\":";
-        jrows(os, field.data(), K, 3);
-        os << ",\"Results\":";
-        jrows(os, mean.data(), K, static_cast<size_t>(od));
-        os << ",\"Weight\":";
-        jarr(os, weight.data(), static_cast<size_t>(od));
-        os << ",\"Mean_Properties\":{\"Temperature\":" << jnum(d.temperature)
-           << ",\"Magnetic_radius\":" << jnum(mean_of(run.r)) << ",\"Saturation_magnetisation\":" << jnum(mean_of(run.Ms))
-           << ",\"Damping_constant\":" << jnum(mean_of(run.alpha)) << ",\"Gyromagnetic_ratio\":" << jnum(mean_of(run.gamma))
-           << ",\"Anisotropy_constant\":" << jnum(mean_of(run.K)) << ",\"Hydrodynamic_Radius\":" << jnum(mean_of(run.rh))
-           << ",\"Viscosity\":" << jnum(mean_of(run.eta)) << "}},\"Stats\":{\"particle_steps\":" << st.particle_steps
+        os << "{\"Mean_Results\":";
+        write_mean_results(os, time, field, mean, weight, K, static_cast<size_t>(od), run);
+        os << ",\"Stats\":{\"particle_steps\":" << st.particle_steps
            << ",\"nonfinite_particles\":" << st.nonfinite_particles << ",\"device_ms\":" << jnum(st.device_ms)
            << "},\"Savefile\":" << jstr(run.savefile) << "}\n";
         return 0;

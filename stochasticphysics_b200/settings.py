@@ -92,6 +92,15 @@ def load_ini(path, seed: int = 0x5EED, precision: Precision = Precision.FP64) ->
 
 
 def run_ini(path, seed: int = 0x5EED, precision: Precision = Precision.FP64, device: int = 0,
-            timeout: float = 3600.0) -> dict:
-    """Runs the .ini on `device` through the driver; returns its JSON record."""
-    return json.loads(_call(_flags(path, seed, precision) + [f"-device:{int(device)}"], timeout))
+            timeout: float = 3600.0, sysmatrix=None) -> dict:
+    """Runs the .ini on `device` through the driver; returns its JSON record.  With
+    `sysmatrix` (a System_Matrix_Settings .ini) it runs the voxel sweep: one
+    ensemble per voxel, offset field moved to the voxel's field, Philox key
+    seed + voxel number, all batched through the server."""
+    extra = [f"-sysmatrix:{sysmatrix}"] if sysmatrix else []
+    return json.loads(_call(_flags(path, seed, precision) + extra + [f"-device:{int(device)}"], timeout))
+
+
+def describe_sysmatrix(path, sysmatrix, seed: int = 0x5EED, timeout: float = 120.0) -> dict:
+    """Voxels, their offset fields, keys and file names of a system-matrix sweep (no GPU)."""
+    return json.loads(_call(_flags(path, seed, Precision.FP64) + [f"-sysmatrix:{sysmatrix}", "-print"], timeout))

@@ -6,6 +6,7 @@ Context.simulate on the EnsembleSpec the same .ini and seed describe — the sam
 library call on the same inputs, so equal bit for bit — and the CPU oracle's
 ensemble mean within the FP64 Philox-mode parity bar (1e-10 absolute).
 """
+import dataclasses
 from pathlib import Path
 
 import numpy as np
@@ -50,3 +51,21 @@ def test_ini_run_matches_api_and_oracle(tmp_path, main, n, particles):
     ref = oracle.simulate(spec)
     assert np.all(np.isfinite(ref["mean"]))
     assert np.max(np.abs(mean - ref["mean"])) <= ABS_MEAN
+
+
+def test_system_matrix_sweep_equals_per_voxel_runs(tmp_path):
+    """Every voxel of the batched sweep equals a separate run of the same voxel
+    description (same offset field, same Philox key) bit for bit."""
+    path = _copy(tmp_path, "legacy_neel_spherical.ini", 40, ("legacy_particle_small.ini", "legacy_particle_large.ini"))
+    sm = INI / "sysmatrix_2x3.ini"
+    rec = settings.run_ini(path, seed=9, sysmatrix=sm)
+    assert rec["Number_of_voxels"] == 6
+    base = settings.load_ini(path, seed=9)
+    with sp.Context(0) as ctx:
+        for i, v in enumerate(rec["Voxels"]):
+            f = base.field
+            spec = dataclasses.replace(base, seed=9 + i, field=sp.FieldSpec(f.type, tuple(v["Offset_Field"]), f.amplitude,
+                                                                            f.frequency, f.phase))
+            alone = ctx.simulate(spec)
+            np.testing.assert_array_equal(np.array(v["Mean_Results"]["Results"], dtype=float), alone.mean)
+            np.testing.assert_array_equal(np.array(v["Mean_Results"]["Field"], dtype=float), alone.field)

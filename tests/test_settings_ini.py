@@ -175,3 +175,42 @@ def test_invalid_settings_are_reported(tmp_path, edit, message):
     bad.write_text(text.replace(edit[0], edit[1]))
     with pytest.raises(settings.SettingsError, match=message):
         settings.describe_ini(bad)
+
+
+def test_system_matrix_voxels_and_fields():
+    """SystemMatrixSettings.h: voxel size (stop - start) / (slices - 1), x fastest,
+    offset = configured offset + Startfield + size * voxel; files *_Vox_x_y_z.*"""
+    d = settings.describe_sysmatrix(INI / "legacy_neel_spherical.ini", INI / "sysmatrix_2x3.ini", seed=100)
+    assert d["Number_of_voxels"] == 6
+    assert d["System_Matrix_Settings"]["Voxel_Size"] == [4e-3, 1e-3, 0.0]
+    vox = [v["Voxel"] for v in d["Voxels"]]
+    assert vox == [[0, 0, 0], [1, 0, 0], [0, 1, 0], [1, 1, 0], [0, 2, 0], [1, 2, 0]]
+    base = np.array([1e-5, -3e-5, 2e-5])  # Amplitude_1 of the particle run
+    for i, v in enumerate(d["Voxels"]):
+        x, y, z = v["Voxel"]
+        np.testing.assert_allclose(v["Offset_Field"], base + [-2e-3 + 4e-3 * x, -1e-3 + 1e-3 * y, 0.0], rtol=0, atol=1e-18)
+        assert v["Seed"] == 100 + i
+        assert v["File"] == f"legacy_result_Vox_{x}_{y}_{z}.mat"
+
+
+def test_system_matrix_start_stop_voxels_follow_the_reference_count():
+    """Use_start_stop_Voxel: walk from Start_Voxel in x-fastest order for
+    getNumberVoxelsToSimulate voxels (SystemMatrixSettings.h:159-215); with
+    Start.x > Stop.x the count is |dz| nx ny + |dy| nx - |dx|."""
+    d = settings.describe_sysmatrix(INI / "legacy_neel_spherical.ini", INI / "sysmatrix_start_stop.ini")
+    vox = [tuple(v["Voxel"]) for v in d["Voxels"]]
+    assert d["Number_of_voxels"] == len(vox) == 1 * 16 + 2 * 4 - 1
+    lin = [x + 4 * y + 16 * z for x, y, z in vox]
+    assert lin == list(range(2 + 4 * 1, 2 + 4 * 1 + 23))
+
+
+@pytest.mark.parametrize("text, message", [
+    ("Startfield = {0,0,0}\nStopfield = {1,0,0}\nSlices = {1,1,1}\n", "Unable to calculate VoxelSize"),
+    ("Startfield = {0,0,0}\nStopfield = {0,0,0}\nSlices = {0,1,1}\n", "at least one"),
+    ("Startfield = {0,0,0}\nSlices = {1,1,1}\n", "missing key Stopfield"),
+])
+def test_invalid_system_matrix_settings(tmp_path, text, message):
+    f = tmp_path / "sm.ini"
+    f.write_text("[System_Matrix_Settings]\n" + text)
+    with pytest.raises(settings.SettingsError, match=message):
+        settings.describe_sysmatrix(INI / "legacy_neel_spherical.ini", f)
