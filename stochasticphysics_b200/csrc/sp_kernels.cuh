@@ -193,7 +193,10 @@ __global__ void __launch_bounds__(kMaxBlock) step_kernel(const EnsDev* __restric
     using Prob = typename ProblemOf<PROB, R, A>::type;
     using St = Stepper<Prob, R, SOLVER>;
     constexpr int D = Prob::D, Mn = Prob::Mn, OUT = Prob::OUT;
-    __shared__ R sB[kFieldTile][3];
+    // per-warp copy of the chunk's field table: warps never wait on each other
+    // (a CTA-wide barrier every tile made fast warps wait for slow ones)
+    __shared__ R sBw[kMaxBlock / 32][kFieldTile][3];
+    R(*const sB)[3] = sBw[threadIdx.x >> 5];
 
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const TileDesc td = tiles[t];
@@ -208,48 +211,43 @@ __global__ void __launch_bounds__(kMaxBlock) step_kernel(const EnsDev* __restric
         const R dt = static_cast<R>(dt_d);
         const R sqdt = static_cast<R>(e.sqrt_dt);
         const unsigned long long seed = e.seed, pid = e.pid_offset + p;
-        const int slots = e.slots;
         const R* ftab = static_cast<const R*>(e.ftab);
         Rot<R> rot;
         rot.rb = e.rot_brown != 0; rot.rn = e.rot_neel != 0;
         rot.min1 = static_cast<R>(e.min1); rot.max1 = static_cast<R>(e.max1);
         rot.min2 = static_cast<R>(e.min2); rot.max2 = static_cast<R>(e.max2);
 
-        R* state = static_cast<R*>(e.state);
-        R* ks = static_cast<R*>(e.ksum);
-        R* kc = static_cast<R*>(e.kcomp);
-        const R* prm = static_cast<const R*>(e.params);
         R y[D], sum[OUT], comp[OUT];
         typename Prob::Par q;
-        double moment = 0.0;
         if (active) {
+            const R* state = static_cast<const R*>(e.state);
+            const R* ks = static_cast<const R*>(e.ksum);
+            const R* kc = static_cast<const R*>(e.kcomp);
 #pragma unroll
             for (int i = 0; i < D; ++i) y[i] = state[i * Np + p];
 #pragma unroll
             for (int c = 0; c < OUT; ++c) { sum[c] = ks[c * Np + p]; comp[c] = kc[c * Np + p]; }
-            q = Prob::load(prm, Np, p);
-            moment = e.moment[p];
+            q = Prob::load(static_cast<const R*>(e.params), Np, p);
         } else {
 #pragma unroll
             for (int i = 0; i < D; ++i) y[i] = R(0);
 #pragma unroll
             for (int c = 0; c < OUT; ++c) { sum[c] = R(0); comp[c] = R(0); }
-            q = Prob::load(prm, Np, td.first);  // any valid slot; results are discarded
+            q = Prob::load(static_cast<const R*>(e.params), Np, td.first);  // any valid slot; results are discarded
         }
         NewtonCount nc{0u, 0u};
-        unsigned long long wpos = s0 % W;
-        const unsigned long long kbase = s0 / W;  // windows completed before this chunk
-        const unsigned long long warp = p >> 5;
-        const int lane = threadIdx.x & 31;
+        // W < 2^31 (validated); the window position fits 32 bits.  Values used only
+        // at a window end (once per W steps) are re-read there instead of being kept
+        // live in registers across the step loop.
+        unsigned int wpos = static_cast<unsigned int>(s0 % W);
+        const unsigned int W32 = static_cast<unsigned int>(W);
         const R* dwp = static_cast<const R*>(e.dw);
-        double* const traj = e.traj;
-        double* const partial = e.partial;
 
         for (unsigned long long t0 = 0; t0 < nsteps; t0 += kFieldTile) {
             const int len = static_cast<int>(min(static_cast<unsigned long long>(kFieldTile), nsteps - t0));
-            __syncthreads();
-            for (int i = threadIdx.x; i < 3 * len; i += blockDim.x) (&sB[0][0])[i] = ftab[3 * t0 + i];
-            __syncthreads();
+            __syncwarp();
+            for (int i = threadIdx.x & 31; i < 3 * len; i += 32) (&sB[0][0])[i] = ftab[3 * t0 + i];
+            __syncwarp();
             for (int i = 0; i < len; ++i) {
                 const unsigned long long g = s0 + t0 + i;
                 if (active) {
@@ -274,23 +272,29 @@ __global__ void __launch_bounds__(kMaxBlock) step_kernel(const EnsDev* __restric
                         sum[c] = tv;
                     }
                 }
-                if (++wpos == W) {  // window end: uniform across the CTA
+                if (++wpos == W32) {  // window end: uniform across the CTA
                     wpos = 0;
                     const unsigned long long k = (g + 1) / W;
-                    const int slot = static_cast<int>(k - kbase - 1);
+                    const int slot = static_cast<int>(k - s0 / W - 1);
+                    const double mom = active ? e.moment[p] : 0.0;
+                    double* const traj = e.traj;
+                    double* const partial = e.partial + ((p >> 5) * e.slots + slot) * OUT;
 #pragma unroll
                     for (int c = 0; c < OUT; ++c) {
                         const R v = active ? sum[c] / static_cast<R>(static_cast<double>(W)) : R(0);
                         sum[c] = R(0);
                         const double vd = static_cast<double>(v);
                         if (traj && active) traj[(k * OUT + c) * Np + p] = vd;
-                        const double ws = warp_sum(active ? weight_of<PROB>(c, moment) * vd : 0.0);
-                        if (lane == 0) partial[(warp * slots + slot) * OUT + c] = ws;
+                        const double ws = warp_sum(active ? weight_of<PROB>(c, mom) * vd : 0.0);
+                        if ((threadIdx.x & 31) == 0) partial[c] = ws;
                     }
                 }
             }
         }
         if (active) {
+            R* state = static_cast<R*>(e.state);
+            R* ks = static_cast<R*>(e.ksum);
+            R* kc = static_cast<R*>(e.kcomp);
             bool finite = true;
 #pragma unroll
             for (int i = 0; i < D; ++i) { state[i * Np + p] = y[i]; finite = finite && M<R>::finite(y[i]); }
@@ -302,7 +306,7 @@ __global__ void __launch_bounds__(kMaxBlock) step_kernel(const EnsDev* __restric
             unsigned int it = nc.iterations, un = nc.unconverged;
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) { it += __shfl_xor_sync(0xffffffffu, it, o); un += __shfl_xor_sync(0xffffffffu, un, o); }
-            if (lane == 0) {
+            if ((threadIdx.x & 31) == 0) {
                 atomicAdd(&e.ctl->newton_iterations, static_cast<unsigned long long>(it));
                 atomicAdd(&e.ctl->newton_unconverged, static_cast<unsigned long long>(un));
             }

@@ -57,6 +57,7 @@ sp_status validate_desc(const sp_ensemble_desc* d, std::string& why) {
     if (d->n_particles == 0) return bad("n_particles must be > 0");
     if (d->n_particles > (1ull << 31)) return bad("n_particles exceeds 2^31");
     if (d->oversampling == 0) return bad("oversampling must be > 0");
+    if (d->oversampling >= (1ull << 31)) return bad("oversampling must be < 2^31");
     if (d->number_of_steps < d->oversampling) return bad("number_of_steps must be >= oversampling");
     if (!(d->timestep > 0.0) || !std::isfinite(d->timestep)) return bad("timestep must be finite and > 0");
     if (!(d->temperature >= 0.0) || !std::isfinite(d->temperature)) return bad("temperature must be finite and >= 0");
@@ -129,7 +130,9 @@ EnsembleLayout layout_of(const sp_ensemble_desc& d, const LaunchConfig& lc) {
 
 void* Ensemble::dalloc(size_t bytes) {
     void* p = nullptr;
-    check_cuda(cudaMalloc(&p, std::max<size_t>(bytes, 16)), "cudaMalloc");
+    // 256-byte granularity keeps every buffer aligned for vector and TMA access
+    const size_t b = (std::max<size_t>(bytes, 16) + 255) / 256 * 256;
+    check_cuda(cudaMallocFromPoolAsync(&p, b, ctx->pool, stream), "cudaMallocFromPoolAsync");
     allocs.push_back(p);
     return p;
 }
@@ -255,7 +258,8 @@ void Ensemble::upload_and_init(const sp_ensemble_desc& d) {
     std::memcpy(host.data() + 7 * n, q.orientation, n * 24);
     std::memcpy(host.data() + 10 * n, q.magnetisation, n * 24);
     double* dev = nullptr;
-    check_cuda(cudaMallocAsync(reinterpret_cast<void**>(&dev), host.size() * 8, stream), "cudaMallocAsync");
+    check_cuda(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&dev), host.size() * 8, ctx->pool, stream),
+               "cudaMallocFromPoolAsync");
     check_cuda(cudaMemcpyAsync(dev, host.data(), host.size() * 8, cudaMemcpyHostToDevice, stream), "upload particles");
     h2d_bytes += host.size() * 8;
     RawParticles rp;
@@ -399,7 +403,8 @@ Ensemble::~Ensemble() {
     if (stream) cudaStreamSynchronize(stream);
     if (gexec) cudaGraphExecDestroy(gexec);
     if (graph) cudaGraphDestroy(graph);
-    for (void* p : allocs) cudaFree(p);
+    for (void* p : allocs) cudaFreeAsync(p, stream);  // back to the context's pool
+    if (stream) cudaStreamSynchronize(stream);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (stream) cudaStreamDestroy(stream);
@@ -447,6 +452,14 @@ sp_status sp_create(sp_context** out, int32_t device) {
     c->cc_major = prop.major;
     c->cc_minor = prop.minor;
     check_cuda(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    cudaMemPoolProps props;
+    std::memset(&props, 0, sizeof(props));
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    check_cuda(cudaMemPoolCreate(&c->pool, &props), "cudaMemPoolCreate");
+    uint64_t keep = UINT64_MAX;
+    check_cuda(cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &keep), "cudaMemPoolSetAttribute");
     *out = c;
     return SP_OK;
     SP_GUARD_END
@@ -458,6 +471,10 @@ sp_status sp_destroy(sp_context* ctx) {
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
     cudaStreamDestroy(ctx->stream);
+    if (ctx->pool) {
+        cudaDeviceSynchronize();  // frees issued on ensemble streams have reached the pool
+        cudaMemPoolDestroy(ctx->pool);
+    }
     delete ctx;
     return SP_OK;
     SP_GUARD_END

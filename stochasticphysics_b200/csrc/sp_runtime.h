@@ -18,6 +18,10 @@ struct sp_context {
     int cc_major = 0, cc_minor = 0;
     size_t total_mem = 0;
     cudaStream_t stream = nullptr;
+    // every ensemble's device buffers come from this pool; freed memory stays in it
+    // (release threshold = max), so repeated runs and server requests reuse it
+    // instead of paying for cudaMalloc / cudaFree each time
+    cudaMemPool_t pool = nullptr;
 };
 
 namespace sp {

@@ -64,8 +64,8 @@ struct Group {
     void release() {
         if (gexec) cudaGraphExecDestroy(gexec);
         if (graph) cudaGraphDestroy(graph);
-        if (d_ens) cudaFree(d_ens);
-        if (d_tiles) cudaFree(d_tiles);
+        if (d_ens) cudaFreeAsync(d_ens, stream);  // the context's pool, in stream order
+        if (d_tiles) cudaFreeAsync(d_tiles, stream);
         gexec = nullptr; graph = nullptr; d_ens = nullptr; d_tiles = nullptr;
     }
 };
@@ -169,8 +169,10 @@ struct sp_server {
             for (unsigned long long f = 0; f < e->L.n; f += g.block) tiles.push_back(TileDesc{static_cast<unsigned>(i), static_cast<unsigned>(f)});
         }
         g.ntiles = static_cast<int>(tiles.size());
-        check_cuda(cudaMalloc(&g.d_ens, ens.size() * sizeof(EnsDev)), "cudaMalloc");
-        check_cuda(cudaMalloc(&g.d_tiles, tiles.size() * sizeof(TileDesc)), "cudaMalloc");
+        check_cuda(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&g.d_ens), ens.size() * sizeof(EnsDev), ctx->pool,
+                                           g.stream), "cudaMallocFromPoolAsync");
+        check_cuda(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&g.d_tiles), tiles.size() * sizeof(TileDesc),
+                                           ctx->pool, g.stream), "cudaMallocFromPoolAsync");
         check_cuda(cudaMemcpyAsync(g.d_ens, ens.data(), ens.size() * sizeof(EnsDev), cudaMemcpyHostToDevice, g.stream), "copy");
         check_cuda(cudaMemcpyAsync(g.d_tiles, tiles.data(), tiles.size() * sizeof(TileDesc), cudaMemcpyHostToDevice, g.stream), "copy");
         check_cuda(cudaStreamSynchronize(g.stream), "group upload");

@@ -20,7 +20,7 @@ namespace sp {
 
 constexpr int kPad = 256;           // particle padding = largest block size
 constexpr int kMaxBlock = 256;
-constexpr int kFieldTile = 256;     // steps of B(t) staged in shared memory at a time
+constexpr int kFieldTile = 128;     // steps of B(t) each warp stages in shared memory at a time
 constexpr int kReduceThreads = 256; // threads per (sample, component) in the window reduction
 
 enum ProblemId : int { kNeel = 0, kNeelSpherical = 1, kBrownNeelEuler = 2, kBrownNeel = 3 };

@@ -156,7 +156,10 @@ def test_exact_jacobian_parity_fp64(ctx, aniso):
 
 def test_exact_jacobian_fp32_state_with_fp64_acceptance(ctx):
     """The stiff cubic ImplicitMidpoint workload in the FP32 form (FP32 state, FP64
-    residual acceptance) against the all-FP64 kernel, both with the exact Newton matrix."""
+    residual acceptance) against the all-FP64 kernel, both with the exact Newton matrix.
+    Particles hop between cubic easy axes (~1 kT barriers), so FP32 and FP64 paths on
+    the same noise decorrelate by chaos as they do for the explicit steppers: the first
+    window must agree closely, every window within 4 two-sample standard errors."""
     base = dataclasses.replace(provider.cubic_implicit(n=4096, steps=3000, oversampling=100),
                                jacobian=Jacobian.Exact)
     r64 = ctx.simulate(base)
@@ -164,7 +167,9 @@ def test_exact_jacobian_fp32_state_with_fp64_acceptance(ctx):
     steps = base.n * base.integrated_steps
     assert r64.stats["newton_unconverged"] == 0
     assert r32.stats["newton_unconverged"] <= 1e-3 * steps
-    assert np.max(np.abs(r32.mean - r64.mean)) < 1e-3
+    d = np.abs(r32.mean - r64.mean)
+    assert d[1].max() < 1e-4
+    assert d.max() < 4 * math.sqrt(2.0 / (3.0 * base.n))
 
 
 def test_runaway_particles_match(ctx):
