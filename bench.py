@@ -117,7 +117,7 @@ def profiled_traffic_per_particle():
     captured launch's particles); the traffic of a launch scales with particles, not
     steps (state, Kahan sums and prefactors are read once and written once)."""
     import re
-    path = ROOT / "profiles" / "step_kernel_brown_neel_euler_fp32_16384.md"
+    path = ROOT / "profiles" / "step_kernel_brown_neel_euler_65536.md"
     try:
         m = re.search(r"traffic_bytes_per_particle_per_launch:\s*([0-9.eE+-]+)", path.read_text())
     except OSError:

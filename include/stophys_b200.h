@@ -34,7 +34,7 @@
 extern "C" {
 #endif
 
-#define SP_ABI_VERSION 2u
+#define SP_ABI_VERSION 3u
 
 #if defined(_WIN32)
 #define SP_API __declspec(dllexport)
@@ -77,7 +77,10 @@ typedef enum sp_field_type {
     SP_FIELD_ZERO = 0,
     SP_FIELD_CONSTANT = 1,
     SP_FIELD_SINUSOIDAL = 2,
-    SP_FIELD_LISSAJOUS = 3
+    SP_FIELD_LISSAJOUS = 3,
+    SP_FIELD_TRIANGULAR = 4,
+    SP_FIELD_RECTANGULAR = 5,
+    SP_FIELD_SINC = 6
 } sp_field_type;
 
 /* Particle_Simulation/Settings/SolverSettings.h:39 (ISolver) */
@@ -131,19 +134,28 @@ typedef struct sp_particles {
 } sp_particles;
 
 /* External field B(t) in tesla.
- *   ZERO:       B = 0
- *   CONSTANT:   B = offset                                  (ConstantField.h:43)
- *   SINUSOIDAL: B = amplitude*sin(2 pi frequency[0] t + phase[0]) + offset
- *                                                           (SinusoidalField.h:47-51)
- *   LISSAJOUS:  B_i = offset_i + amplitude_i*sin(2 pi frequency_i t + phase_i)
- *                                                           (LissajousField.h:98-101) */
+ *   ZERO:        B = 0
+ *   CONSTANT:    B = offset                                  (ConstantField.h:43)
+ *   SINUSOIDAL:  B = amplitude*sin(2 pi frequency[0] t + phase[0]) + offset
+ *                                                            (SinusoidalField.h:47-51)
+ *   LISSAJOUS:   B_i = offset_i + amplitude_i*sin(2 pi frequency_i t + phase_i)
+ *                                                            (LissajousField.h:98-101)
+ *   TRIANGULAR:  piecewise linear in the position p = (t + time_offset) mod periode
+ *                (TriangularField.h:52-70)
+ *   RECTANGULAR: exponential rise / decay with time constant tau in each half
+ *                period, optionally alternating (RectangularField.h:30-63)
+ *   SINC:        B = amplitude*sinc^2(pi a p) + offset, a = 22/periode,
+ *                p = (t mod periode) - periode/2                (SincField.h:38-48) */
 typedef struct sp_field_desc {
-    int32_t type; /* sp_field_type */
-    int32_t reserved;
+    int32_t type;        /* sp_field_type                         */
+    int32_t alternating; /* RECTANGULAR: Alternating              */
     double offset[3];
     double amplitude[3];
     double frequency[3];
     double phase[3];
+    double periode;      /* TRIANGULAR / RECTANGULAR / SINC: Periode (s) */
+    double time_offset;  /* TRIANGULAR / RECTANGULAR: TimeOffset (s)     */
+    double tau;          /* RECTANGULAR: Tau (s)                          */
 } sp_field_desc;
 
 /* Problem_Settings (Particle_Simulation/Settings/ProblemSettings.h:119-206). */

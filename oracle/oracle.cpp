@@ -7,6 +7,7 @@
 // reference's golden vectors.
 #include <algorithm>
 #include <cmath>
+#include <limits>
 #include <cstdint>
 #include <cstring>
 #include <memory>
@@ -93,9 +94,14 @@ inline void philox_normals(uint64_t seed, uint64_t pid, uint64_t step, int m, do
 
 // ====================================================================== fields
 // Fields/SinusoidalField.h:47-51, Fields/LissajousField.h:98-101, ConstantField.h:43, ZeroField.h:39
+// Fields/TriangularField.h:52-70, Fields/RectangularField.h:30-63, Fields/SincField.h:32-48
 struct FieldEval {
     int type = SP_FIELD_ZERO;
     double offset[3] = {0, 0, 0}, amplitude[3] = {0, 0, 0}, angfreq[3] = {0, 0, 0}, phase[3] = {0, 0, 0};
+    double P = 0, halfP = 0, toff = 0;
+    // rectangular waveform: amplitude and offset after the alternating transform
+    double invTau = 0, rAmp[3] = {0, 0, 0}, rMax[3] = {0, 0, 0}, rOff[3] = {0, 0, 0}, rToff = 0;
+    double sincA = 0;
     void init(const sp_field_desc& f) {
         type = f.type;
         for (int i = 0; i < 3; ++i) {
@@ -103,7 +109,24 @@ struct FieldEval {
             angfreq[i] = kTwoPi * (type == SP_FIELD_SINUSOIDAL ? f.frequency[0] : f.frequency[i]);
             phase[i] = (type == SP_FIELD_SINUSOIDAL ? f.phase[0] : f.phase[i]);
         }
+        P = f.periode; halfP = f.periode / 2.0; toff = f.time_offset;
+        sincA = 11.0 / (f.periode * 0.5);
+        if (type == SP_FIELD_RECTANGULAR) {
+            invTau = std::abs(f.tau) <= std::numeric_limits<double>::min() ? std::numeric_limits<double>::max() : 1.0 / f.tau;
+            double na2 = 0.0, nm2 = 0.0;
+            for (int i = 0; i < 3; ++i) {
+                rAmp[i] = f.alternating ? 2.0 * f.amplitude[i] : f.amplitude[i];
+                rMax[i] = rAmp[i] * (-std::expm1(-halfP * invTau));
+                na2 += rAmp[i] * rAmp[i];
+                nm2 += rMax[i] * rMax[i];
+            }
+            rToff = f.alternating ? f.time_offset - std::log(1.0 - std::sqrt(nm2) / (2.0 * std::sqrt(na2))) * f.tau
+                                  : f.time_offset;
+            for (int i = 0; i < 3; ++i)
+                rOff[i] = f.alternating ? rAmp[i] * std::expm1(-rToff * invTau) + f.offset[i] : f.offset[i];
+        }
     }
+    static double sinc(double x) { return std::fabs(x) < 1e-4 ? 1.0 + x * x * (-1.0 / 6.0 + x * x * (1.0 / 120.0)) : std::sin(x) / x; }
     void eval(double time, double* B) const {
         switch (type) {
             case SP_FIELD_ZERO: B[0] = B[1] = B[2] = 0.0; break;
@@ -113,8 +136,33 @@ struct FieldEval {
                 for (int i = 0; i < 3; ++i) B[i] = amplitude[i] * sinwt + offset[i];
                 break;
             }
-            default:
+            case SP_FIELD_LISSAJOUS:
                 for (int i = 0; i < 3; ++i) B[i] = offset[i] + amplitude[i] * std::sin(angfreq[i] * time + phase[i]);
+                break;
+            case SP_FIELD_TRIANGULAR: {
+                const double t = time + toff;
+                const double pos = t < 0 ? P + std::fmod(t, P) : std::fmod(t, P);
+                const double w = pos > halfP ? 2.0 * pos / halfP - 1.0 : -2.0 * pos / halfP + 3.0;
+                for (int i = 0; i < 3; ++i) B[i] = w * amplitude[i] + offset[i];
+                break;
+            }
+            case SP_FIELD_RECTANGULAR: {
+                const double t = time + rToff;
+                const double pos = t < 0 ? std::fmod(t + P, P) : std::fmod(t, P);
+                if (pos <= halfP) {
+                    const double g = -std::expm1(-pos * invTau);
+                    for (int i = 0; i < 3; ++i) B[i] = rAmp[i] * g + rOff[i];
+                } else {
+                    const double g = std::exp(-(pos - halfP) * invTau);
+                    for (int i = 0; i < 3; ++i) B[i] = rAmp[i] * g + rOff[i] - (rAmp[i] - rMax[i]);
+                }
+                break;
+            }
+            default: {  // SP_FIELD_SINC
+                const double pos = (time < 0 ? std::fmod(time + P, P) : std::fmod(time, P)) - halfP;
+                const double sc = sinc(kPi * sincA * pos);
+                for (int i = 0; i < 3; ++i) B[i] = amplitude[i] * (sc * sc) + offset[i];
+            }
         }
     }
 };
@@ -429,7 +477,7 @@ using namespace orc;
 
 extern "C" {
 
-int oracle_abi_version(void) { return 2; }
+int oracle_abi_version(void) { return 3; }
 
 // Runs the ensemble described by desc.  mean[K][OUT], weight[OUT], time[K],
 // field[K][3], traj[N][K][OUT] and final_state[N][D] are optional (NULL).

@@ -13,7 +13,7 @@ from typing import Optional
 
 import numpy as np
 
-ABI_VERSION = 2
+ABI_VERSION = 3
 
 
 class Status(IntEnum):
@@ -49,6 +49,9 @@ class FieldType(IntEnum):
     Constant = 1
     Sinusoidal = 2
     Lissajous = 3
+    Triangular = 4
+    Rectangular = 5
+    Sinc = 6
 
 
 class Solver(IntEnum):
@@ -109,11 +112,14 @@ class sp_particles(C.Structure):
 class sp_field_desc(C.Structure):
     _fields_ = [
         ("type", C.c_int32),
-        ("reserved", C.c_int32),
+        ("alternating", C.c_int32),
         ("offset", C.c_double * 3),
         ("amplitude", C.c_double * 3),
         ("frequency", C.c_double * 3),
         ("phase", C.c_double * 3),
+        ("periode", C.c_double),
+        ("time_offset", C.c_double),
+        ("tau", C.c_double),
     ]
 
 
@@ -223,6 +229,10 @@ class FieldSpec:
     amplitude: tuple = (0.0, 0.0, 0.0)
     frequency: tuple = (0.0, 0.0, 0.0)
     phase: tuple = (0.0, 0.0, 0.0)
+    periode: float = 0.0       # triangular / rectangular / sinc
+    time_offset: float = 0.0   # triangular / rectangular
+    tau: float = 0.0           # rectangular
+    alternating: bool = False  # rectangular
 
     @staticmethod
     def sinusoidal(amplitude, frequency, phase=0.0, offset=(0.0, 0.0, 0.0)) -> "FieldSpec":
@@ -236,6 +246,19 @@ class FieldSpec:
     def constant(offset) -> "FieldSpec":
         return FieldSpec(FieldType.Constant, tuple(offset))
 
+    @staticmethod
+    def triangular(amplitude, periode, time_offset=0.0, offset=(0.0, 0.0, 0.0)) -> "FieldSpec":
+        return FieldSpec(FieldType.Triangular, tuple(offset), tuple(amplitude), periode=periode, time_offset=time_offset)
+
+    @staticmethod
+    def rectangular(amplitude, periode, tau, time_offset=0.0, alternating=False, offset=(0.0, 0.0, 0.0)) -> "FieldSpec":
+        return FieldSpec(FieldType.Rectangular, tuple(offset), tuple(amplitude), periode=periode,
+                         time_offset=time_offset, tau=tau, alternating=alternating)
+
+    @staticmethod
+    def sinc(amplitude, periode, offset=(0.0, 0.0, 0.0)) -> "FieldSpec":
+        return FieldSpec(FieldType.Sinc, tuple(offset), tuple(amplitude), periode=periode)
+
     def to_c(self) -> sp_field_desc:
         f = sp_field_desc()
         f.type = int(self.type)
@@ -244,6 +267,10 @@ class FieldSpec:
             f.amplitude[i] = float(self.amplitude[i])
             f.frequency[i] = float(self.frequency[i])
             f.phase[i] = float(self.phase[i])
+        f.periode = float(self.periode)
+        f.time_offset = float(self.time_offset)
+        f.tau = float(self.tau)
+        f.alternating = int(bool(self.alternating))
         return f
 
 

@@ -345,12 +345,16 @@ Run build(const std::string& path, unsigned long long seed, int precision) {
     pflag("Use_simple_model", q.use_simple_model);
 
     // Field_Properties (FieldProperties.h, Fields/Sinusoidal.hpp:31-34, Fields/Lissajous.hpp:33-36)
+    // IFieldMap strings (Fields/FieldList.h:52-60); "zero" accepted beside "none"
     const std::string ft = lower(Ini::str(need("Field_Properties", "Type_of_field")));
     sp_field_desc& f = d.field;
-    if (ft == "zero") f.type = SP_FIELD_ZERO;
+    if (ft == "none" || ft == "zero") f.type = SP_FIELD_ZERO;
     else if (ft == "constant") f.type = SP_FIELD_CONSTANT;
     else if (ft == "sinusoidal") f.type = SP_FIELD_SINUSOIDAL;
     else if (ft == "lissajous") f.type = SP_FIELD_LISSAJOUS;
+    else if (ft == "triangular") f.type = SP_FIELD_TRIANGULAR;
+    else if (ft == "rectangular") f.type = SP_FIELD_RECTANGULAR;
+    else if (ft == "sinc") f.type = SP_FIELD_SINC;
     else throw std::runtime_error("unsupported Type_of_field '" + ft + "'");
     auto put3 = [](double* dst, const std::vector<double>& v, const char* k) {
         if (v.size() != 3) throw std::runtime_error(std::string(k) + " needs three values");
@@ -368,6 +372,11 @@ Run build(const std::string& path, unsigned long long seed, int precision) {
     if (!fvec("Amplitude", f.amplitude)) fvec("Amplitude_2", f.amplitude);
     if (!fvec("Frequencies", f.frequency) && !fnum("Frequency", f.frequency)) fnum("Frequency_1", f.frequency);
     if (!fvec("Phases", f.phase) && !fnum("Phase", f.phase)) fnum("Phase_1", f.phase);
+    // Fields/Triangular.hpp, Rectangular.hpp, Sinc.hpp
+    fnum("Periode", &f.periode);
+    fnum("TimeOffset", &f.time_offset);
+    fnum("Tau", &f.tau);
+    if (auto v = opt("Field_Properties", "Alternating")) f.alternating = Ini::boolean(*v);
 
     // Particle_Provider (ParticleProvider.h:243-292)
     bool discrete = false;
@@ -590,6 +599,8 @@ void write_description(std::ostream& o, const Run& run) {
     jarr(o, d.field.frequency, 3);
     o << ",\"phase\":";
     jarr(o, d.field.phase, 3);
+    o << ",\"periode\":" << jnum(d.field.periode) << ",\"time_offset\":" << jnum(d.field.time_offset)
+      << ",\"tau\":" << jnum(d.field.tau) << ",\"alternating\":" << d.field.alternating;
     o << "},\"problem_settings\":{\"use_coordinate_transformation\":" << q.use_coordinate_transformation
       << ",\"min_angle_before_transformation\":" << jnum(q.min_angle_before_transformation)
       << ",\"use_euler_coordinate_transformation\":" << q.use_euler_coordinate_transformation

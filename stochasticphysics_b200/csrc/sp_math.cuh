@@ -169,10 +169,47 @@ __device__ __forceinline__ void field_eval(const FieldParams& f, double t, doubl
             for (int i = 0; i < 3; ++i) B[i] = __dadd_rn(__dmul_rn(f.amplitude[i], s), f.offset[i]);
             break;
         }
-        default:
+        case 3:
 #pragma unroll
             for (int i = 0; i < 3; ++i)
                 B[i] = __dadd_rn(f.offset[i], __dmul_rn(f.amplitude[i], ::sin(__dadd_rn(__dmul_rn(f.omega[i], t), f.phase[i]))));
+            break;
+        case 4: {  // TriangularField.h:52-70
+            const double nt = __dadd_rn(t, f.time_offset);
+            const double pos = nt < 0.0 ? __dadd_rn(f.periode, ::fmod(nt, f.periode)) : ::fmod(nt, f.periode);
+            const double r = __ddiv_rn(__dmul_rn(2.0, pos), f.half_periode);
+            const double w = pos > f.half_periode ? __dadd_rn(r, -1.0) : __dadd_rn(-r, 3.0);
+#pragma unroll
+            for (int i = 0; i < 3; ++i) B[i] = __dadd_rn(__dmul_rn(w, f.amplitude[i]), f.offset[i]);
+            break;
+        }
+        case 5: {  // RectangularField.h:46-63
+            const double nt = __dadd_rn(t, f.time_offset);
+            const double pos = nt < 0.0 ? ::fmod(__dadd_rn(nt, f.periode), f.periode) : ::fmod(nt, f.periode);
+            if (pos <= f.half_periode) {
+                const double g = -::expm1(-__dmul_rn(pos, f.inv_tau));
+#pragma unroll
+                for (int i = 0; i < 3; ++i) B[i] = __dadd_rn(__dmul_rn(f.amplitude[i], g), f.offset[i]);
+            } else {
+                const double g = ::exp(-__dmul_rn(__dadd_rn(pos, -f.half_periode), f.inv_tau));
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+                    B[i] = __dadd_rn(__dadd_rn(__dmul_rn(f.amplitude[i], g), f.offset[i]),
+                                     -__dadd_rn(f.amplitude[i], -f.max_field[i]));
+            }
+            break;
+        }
+        default: {  // 6, SincField.h:38-48: sinc(x) = sin(x)/x, 1 - x^2/6 + x^4/120 near 0
+            const double pos = __dadd_rn(t < 0.0 ? ::fmod(__dadd_rn(t, f.periode), f.periode) : ::fmod(t, f.periode),
+                                         -f.half_periode);
+            const double x = __dmul_rn(__dmul_rn(3.14159265358979323846, f.sinc_a), pos);
+            const double x2 = __dmul_rn(x, x);
+            const double sc = ::fabs(x) < 1e-4 ? __dadd_rn(1.0, __dmul_rn(x2, __dadd_rn(-1.0 / 6.0, __dmul_rn(x2, 1.0 / 120.0))))
+                                                : __ddiv_rn(::sin(x), x);
+            const double s2 = __dmul_rn(sc, sc);
+#pragma unroll
+            for (int i = 0; i < 3; ++i) B[i] = __dadd_rn(__dmul_rn(f.amplitude[i], s2), f.offset[i]);
+        }
     }
 }
 

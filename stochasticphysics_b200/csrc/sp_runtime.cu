@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cmath>
+#include <limits>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -53,7 +54,9 @@ sp_status validate_desc(const sp_ensemble_desc* d, std::string& why) {
     if (d->solver < 0 || d->solver > 3) return bad("unknown solver");
     if (d->precision < 0 || d->precision > 1) return bad("unknown precision");
     if (d->noise < 0 || d->noise > 1) return bad("unknown noise mode");
-    if (d->field.type < 0 || d->field.type > 3) return bad("unknown field type");
+    if (d->field.type < 0 || d->field.type > 6) return bad("unknown field type");
+    if (d->field.type >= SP_FIELD_TRIANGULAR && !(d->field.periode > 0.0 && std::isfinite(d->field.periode)))
+        return bad("triangular, rectangular and sinc fields need a finite periode > 0");
     if (d->n_particles == 0) return bad("n_particles must be > 0");
     if (d->n_particles > (1ull << 31)) return bad("n_particles exceeds 2^31");
     if (d->oversampling == 0) return bad("oversampling must be > 0");
@@ -241,6 +244,29 @@ FieldParams field_params(const sp_field_desc& f) {
         p.amplitude[i] = f.amplitude[i];
         p.omega[i] = two_pi * (f.type == SP_FIELD_SINUSOIDAL ? f.frequency[0] : f.frequency[i]);
         p.phase[i] = f.type == SP_FIELD_SINUSOIDAL ? f.phase[0] : f.phase[i];
+    }
+    p.periode = f.periode;
+    p.half_periode = f.periode / 2.0;
+    p.time_offset = f.time_offset;
+    p.sinc_a = 11.0 / (f.periode * 0.5);  // SincField.h:35
+    if (f.type == SP_FIELD_RECTANGULAR) {
+        // RectangularField.h:30-38: derived constants of the (alternating) waveform
+        p.inv_tau = std::abs(f.tau) <= std::numeric_limits<double>::min() ? std::numeric_limits<double>::max() : 1.0 / f.tau;
+        double amp[3], maxf[3], na = 0.0, nm = 0.0;
+        for (int i = 0; i < 3; ++i) {
+            amp[i] = f.alternating ? 2.0 * f.amplitude[i] : f.amplitude[i];
+            maxf[i] = amp[i] * (-std::expm1(-p.half_periode * p.inv_tau));
+            na += amp[i] * amp[i];
+            nm += maxf[i] * maxf[i];
+        }
+        const double toff = f.alternating ? f.time_offset - std::log(1.0 - std::sqrt(nm) / (2.0 * std::sqrt(na))) * f.tau
+                                          : f.time_offset;
+        p.time_offset = toff;
+        for (int i = 0; i < 3; ++i) {
+            p.amplitude[i] = amp[i];
+            p.max_field[i] = maxf[i];
+            p.offset[i] = f.alternating ? amp[i] * std::expm1(-toff * p.inv_tau) + f.offset[i] : f.offset[i];
+        }
     }
     return p;
 }

@@ -38,10 +38,15 @@ constexpr int kParamsBrownNeel = 14;
 struct FieldParams {
     int type;  // sp_field_type
     int pad;
-    double offset[3];
-    double amplitude[3];
-    double omega[3];  // 2*pi*frequency
+    double offset[3];     // RECTANGULAR: the shifted offset of the alternating form
+    double amplitude[3];  // RECTANGULAR: doubled when alternating
+    double omega[3];      // 2*pi*frequency
     double phase[3];
+    double periode, half_periode;
+    double time_offset;   // RECTANGULAR: the shifted time offset of the alternating form
+    double inv_tau;       // RECTANGULAR: 1/Tau (max double for Tau ~ 0)
+    double max_field[3];  // RECTANGULAR: amplitude * (1 - exp(-periode/(2 tau)))
+    double sinc_a;        // SINC: 11 / (periode / 2)
 };
 
 // Control block of one ensemble, advanced by the commit kernel so that a

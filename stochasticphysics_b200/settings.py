@@ -68,7 +68,8 @@ def spec_from_description(d: dict) -> EnsembleSpec:
         temperature=float(d["temperature"]), anisotropy=Anisotropy(d["anisotropy"]), solver=Solver(d["solver"]),
         precision=Precision(d["precision"]), noise=Noise.Philox,
         field=FieldSpec(FieldType(f["type"]), tuple(f["offset"]), tuple(f["amplitude"]), tuple(f["frequency"]),
-                        tuple(f["phase"])),
+                        tuple(f["phase"]), periode=float(f["periode"]), time_offset=float(f["time_offset"]),
+                        tau=float(f["tau"]), alternating=bool(f["alternating"])),
         max_iteration=int(d["max_iteration"]), accuracy_goal=float(d["accuracy_goal"]),
         use_coordinate_transformation=bool(q["use_coordinate_transformation"]),
         min_angle_before_transformation=float(q["min_angle_before_transformation"]),

@@ -163,7 +163,8 @@ def test_spec_from_ini_builds_a_valid_description():
     (("'Heun_Strong'", "'WeakTest'"), "unsupported Solver 'WeakTest'"),
     (("Timestep = 2.0e-12", ""), "missing key Timestep"),
     (("'legacy_particle_large.ini'", "'no_such_particle.ini'"), "cannot open"),
-    (("Type_of_field = 'sinusoidal'", "Type_of_field = 'triangular'"), "unsupported Type_of_field"),
+    (("Type_of_field = 'sinusoidal'", "Type_of_field = 'sawtooth'"), "unsupported Type_of_field"),
+    (("Type_of_field = 'sinusoidal'", "Type_of_field = 'triangular'"), "finite periode > 0"),
     (("Oversampling = 100", "Oversampling = 3000"), "oversampling"),
 ])
 def test_invalid_settings_are_reported(tmp_path, edit, message):
