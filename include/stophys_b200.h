@@ -88,7 +88,8 @@ typedef enum sp_solver {
     SP_SOLVER_EULER_MARUYAMA = 0,
     SP_SOLVER_HEUN_STRONG = 1,
     SP_SOLVER_MILLSTEIN = 2,
-    SP_SOLVER_IMPLICIT_MIDPOINT = 3
+    SP_SOLVER_IMPLICIT_MIDPOINT = 3,
+    SP_SOLVER_EULER_MARUYAMA_NORMALIZED = 4  /* EulerMaruyama_Normalized.inl:40-56 */
 } sp_solver;
 
 typedef enum sp_precision {

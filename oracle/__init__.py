@@ -51,6 +51,8 @@ def lib():
         L.oracle_eval_problem.restype = C.c_int
         L.oracle_eval_problem.argtypes = [C.c_int, C.c_int, _dp, _dp, _dp, _dp, _dp, C.c_double, _dp,
                                           _dp, _dp, _dp, _dp, _dp, _dp, _dp, C.POINTER(C.c_int), C.c_int]
+        L.oracle_field_eval.restype = None
+        L.oracle_field_eval.argtypes = [C.c_void_p, _dp, C.c_uint64, _dp]
         L.oracle_neel_exact_jacobians.restype = None
         L.oracle_neel_exact_jacobians.argtypes = [C.c_int] + [_dp] * 7
         L.oracle_count_ops.restype = C.c_int
@@ -149,6 +151,15 @@ def eval_problem(problem: int, aniso: int, props, euler, settings, state, field=
     if rc != 0:
         raise RuntimeError(f"oracle_eval_problem failed ({rc})")
     out["rotated"] = (bool(rot[0]), bool(rot[1]))
+    return out
+
+
+def field_eval(field, times) -> np.ndarray:
+    """B(t) [len(times)][3] of a FieldSpec."""
+    f = field.to_c()
+    t = np.ascontiguousarray(times, dtype=float)
+    out = np.zeros((t.size, 3))
+    lib().oracle_field_eval(C.addressof(f), _p(t), t.size, _p(out))
     return out
 
 

@@ -213,6 +213,12 @@ struct Stepper {
         pr.finishCalculations(res);
         return res;
     }
+    // SDEFramework/Solver/EulerMaruyama_Normalized.inl:40-56: EulerMaruyama, then normalize
+    static Dep euler_maruyama_normalized(P& pr, const Dep& yi, const V3<T>& xi, const Vec<T, M>& dW, const T& dt) {
+        Dep res = euler_maruyama(pr, yi, xi, dW, dt);
+        pr.normalize(res);
+        return res;
+    }
     // SDEFramework/Solver/Heun_Strong.inl:37-47.  The reference's Heun is not
     // wired into its simulator (SimulationManager.h:322-328) and never calls
     // prepare/finish; this restatement evaluates both stages in the chart that
@@ -342,6 +348,9 @@ void simulate_particle(const SimSpec& sp, const ParticleIn& pin, uint64_t p, dou
                 switch (sp.solver) {
                     case SP_SOLVER_EULER_MARUYAMA: yi = Stepper<P, T>::euler_maruyama(pr, yi, xi, dW, dt); break;
                     case SP_SOLVER_HEUN_STRONG: yi = Stepper<P, T>::heun(pr, yi, xi, dW, dt); break;
+                    case SP_SOLVER_EULER_MARUYAMA_NORMALIZED:
+                        yi = Stepper<P, T>::euler_maruyama_normalized(pr, yi, xi, dW, dt);
+                        break;
                     default: yi = Stepper<P, T>::millstein(pr, yi, xi, dW, dt); break;
                 }
             }
@@ -599,6 +608,13 @@ void oracle_cubic(double K1, double Ms, double radius, const double* m, const do
     const V3<double> h = cb.getAnisotropyField(mm, xx, yy, zz);
     const V3<double> t = cb.getEffTorque(mm, xx, yy, zz, statesin, statecos);
     for (int i = 0; i < 3; ++i) { field[i] = h[i]; torque[i] = t[i]; }
+}
+
+// B(t) of a field description at n times: out[n][3]
+void oracle_field_eval(const sp_field_desc* f, const double* times, uint64_t n, double* out) {
+    FieldEval fe;
+    fe.init(*f);
+    for (uint64_t i = 0; i < n; ++i) fe.eval(times[i], out + 3 * i);
 }
 
 // Exact Neel (Cartesian) Jacobians at state m (the analytic Newton matrix of

@@ -94,6 +94,11 @@ struct NeelProblem {
     }
     // :210-214
     Vec<T, OUT> calculateOutputResult(const Dep& yi) const { return yi; }
+    // NeelRelaxation.h:204-208 (Eigen normalize: unchanged at |m| = 0)
+    void normalize(Dep& yi) const {
+        const T n2 = yi[0] * yi[0] + yi[1] * yi[1] + yi[2] * yi[2];
+        if (n2 > T(0.0)) { const T n = sqrt(n2); for (int k = 0; k < 3; ++k) yi[k] = yi[k] / n; }
+    }
 
     // Exact Jacobians (not in the reference; its versions above keep the
     // -2 alpha/dt [m]x stand-in and drop the damping and projection derivatives).
@@ -313,6 +318,7 @@ struct NeelSphericalProblem {
         const T sin_t = sin(yi[0]), cos_t = cos(yi[0]), sin_p = sin(yi[1]), cos_p = cos(yi[1]);
         Vec<T, 3> o; o[0] = sin_t * cos_p; o[1] = sin_t * sin_p; o[2] = cos_t; return o;
     }
+    void normalize(Dep&) const {}  // spherical coordinates: no-op in the reference
 };
 
 // ====================================================================== Brown + Neel, Euler/spherical
@@ -544,6 +550,7 @@ struct BrownNeelEulerProblem {
         o[6] = s[3] * c[4]; o[7] = s[3] * s[4]; o[8] = c[3];
         return o;
     }
+    void normalize(Dep&) const {}  // spherical coordinates: no-op in the reference
 };
 
 // ====================================================================== Brown + Neel (Cartesian)
@@ -659,6 +666,13 @@ struct BrownNeelProblem {
     Mat<T, 6, 6> getJacobiDeterministic(const Dep&, const V3<T>&, const T&) const { return Mat<T, 6, 6>::zero(); }
     Mat<T, 6, 6> getJacobiStochastic(const Vec<T, 6>&) const { return Mat<T, 6, 6>::zero(); }
     Vec<T, OUT> calculateOutputResult(const Dep& yi) const { return yi; }
+    // BrownAndNeelRelaxation.h:168-172: n and m separately
+    void normalize(Dep& yi) const {
+        for (int h = 0; h < 6; h += 3) {
+            const T n2 = yi[h] * yi[h] + yi[h + 1] * yi[h + 1] + yi[h + 2] * yi[h + 2];
+            if (n2 > T(0.0)) { const T n = sqrt(n2); for (int k = 0; k < 3; ++k) yi[h + k] = yi[h + k] / n; }
+        }
+    }
 };
 
 }  // namespace orc

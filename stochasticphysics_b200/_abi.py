@@ -59,6 +59,7 @@ class Solver(IntEnum):
     Heun_Strong = 1
     Millstein = 2
     Implicit_Midpoint = 3
+    EulerMaruyama_Normalized = 4
 
 
 class Precision(IntEnum):

@@ -188,6 +188,7 @@ int solver_of(const std::string& s) {
     if (t == "heun_strong") return SP_SOLVER_HEUN_STRONG;
     if (t == "millstein") return SP_SOLVER_MILLSTEIN;
     if (t == "implicit_midpoint") return SP_SOLVER_IMPLICIT_MIDPOINT;
+    if (t == "eulermaruyama_normalized") return SP_SOLVER_EULER_MARUYAMA_NORMALIZED;
     throw std::runtime_error("unsupported Solver '" + s + "'");
 }
 

@@ -20,7 +20,7 @@ struct KernelSet {
 // index: problem, anisotropy, solver slot (sp_solver, or kImplicitMidpointExact),
 // precision (0 FP64, 1 FP32), injected noise
 const KernelSet& kernel_set(int problem, int aniso, int solver, int precision, int inject);
-constexpr int kSolverSlots = 5;
+constexpr int kSolverSlots = 6;
 inline int kernel_index(int aniso, int solver, int precision, int inject) {
     return ((aniso * kSolverSlots + solver) * 2 + precision) * 2 + inject;
 }

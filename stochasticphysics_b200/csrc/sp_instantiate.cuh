@@ -57,6 +57,7 @@ void fill_aniso(KernelSet* tab) {
     fill_solver<PROB, A, kHeun>(tab);
     fill_solver<PROB, A, kMillstein>(tab);
     fill_solver<PROB, A, kImplicitMidpoint>(tab);
+    fill_solver<PROB, A, kEulerMaruyamaNormalized>(tab);
     fill_solver<PROB, A, kImplicitMidpointExact>(tab);
 }
 template <int PROB>

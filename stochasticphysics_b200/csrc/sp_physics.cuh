@@ -120,6 +120,14 @@ struct NeelCart {
         r[0] = o.x; r[1] = o.y; r[2] = o.z;
     }
     static __device__ __forceinline__ void out(const R* y, R* o) { o[0] = y[0]; o[1] = y[1]; o[2] = y[2]; }
+    // NeelRelaxation.h:204-208: m / |m| (Eigen normalize: unchanged when |m| = 0)
+    static __device__ __forceinline__ void normalize(R* y) {
+        const R n2 = (y[0] * y[0] + y[1] * y[1]) + y[2] * y[2];
+        if (n2 > R(0)) {
+            const R n = M<R>::sqrt(n2);
+            y[0] = y[0] / n; y[1] = y[1] / n; y[2] = y[2] / n;
+        }
+    }
     // S = -I + dt/2 J_det + 1/2 J_sto with the reference Jacobians (NeelRelaxation.h:134-190):
     // J_det = NF1([m]x J_H - [H]x) - (2 alpha/dt)[m]x, J_sto = -pre1 [dW]x, J_H = pF z z^T (cubic: I)
     static __device__ __forceinline__ void newton_matrix(const Par& q, const R* y, const Cache&, const R* B, const R* w,
@@ -272,6 +280,7 @@ struct NeelSph {
         M<R>::sincos(y[1], &sp, &cp);
         o[0] = st * cp; o[1] = st * sp; o[2] = ct;
     }
+    static __device__ __forceinline__ void normalize(R*) {}  // NeelRelaxationSpherical.h:534-537
     // NeelRelaxationSpherical.h:312-432 and finishJacobiCalculations :473-497
     static __device__ __forceinline__ void newton_matrix(const Par& q, const R*, const Cache& c, const R* B, const R* w,
                                                          R dt, R S[D][D]) {
@@ -521,6 +530,7 @@ struct BrownNeelEuler {
         o[3] = -sphicpsi - c[1] * cphispsi; o[4] = c[1] * cphicpsi - sphispsi; o[5] = s[1] * c[0];
         o[6] = s[3] * c[4]; o[7] = s[3] * s[4]; o[8] = c[3];
     }
+    static __device__ __forceinline__ void normalize(R*) {}  // BrownAndNeelRelaxationEulerSpherical.h:738-741
     static __device__ __forceinline__ void newton_matrix(const Par&, const R*, const Cache&, const R*, const R*, R,
                                                          R S[D][D]) {
         for (int i = 0; i < D; ++i) for (int j = 0; j < D; ++j) S[i][j] = R(i == j ? -1 : 0);
@@ -581,6 +591,17 @@ struct BrownNeelCart {
     static __device__ __forceinline__ void out(const R* y, R* o) {
 #pragma unroll
         for (int i = 0; i < 6; ++i) o[i] = y[i];
+    }
+    // BrownAndNeelRelaxation.h:168-172: n and m normalised separately
+    static __device__ __forceinline__ void normalize(R* y) {
+#pragma unroll
+        for (int h = 0; h < 6; h += 3) {
+            const R n2 = (y[h] * y[h] + y[h + 1] * y[h + 1]) + y[h + 2] * y[h + 2];
+            if (n2 > R(0)) {
+                const R n = M<R>::sqrt(n2);
+                y[h] = y[h] / n; y[h + 1] = y[h + 1] / n; y[h + 2] = y[h + 2] / n;
+            }
+        }
     }
     static __device__ __forceinline__ void newton_matrix(const Par&, const R*, const Cache&, const R*, const R*, R,
                                                          R S[D][D]) {
@@ -663,6 +684,17 @@ struct Stepper {
 #pragma unroll
             for (int i = 0; i < D; ++i) y[i] = (y[i] + (R(0.5) * ((a2[i] + d[i]) + a1[i])) * dt) + bw[i];
             P::finish(rot, y, c);
+        } else if constexpr (SOLVER == kEulerMaruyamaNormalized) {
+            Cache c;
+            P::prepare(q, rot, y, c);
+            R a[D], d[D], bw[D];
+            P::det(q, y, c, B, a);
+            P::drift(q, y, c, d);
+            P::bdw(q, y, c, w, bw);
+#pragma unroll
+            for (int i = 0; i < D; ++i) y[i] = y[i] + ((a[i] + d[i]) * dt + bw[i]);
+            P::finish(rot, y, c);
+            P::normalize(y);
         } else if constexpr (SOLVER == kMillstein) {
             Cache c;
             P::prepare(q, rot, y, c);

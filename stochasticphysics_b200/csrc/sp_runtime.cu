@@ -51,7 +51,7 @@ sp_status validate_desc(const sp_ensemble_desc* d, std::string& why) {
     if (d->abi_version != SP_ABI_VERSION) return bad("abi_version mismatch");
     if (d->problem < 0 || d->problem > 3) return bad("unknown problem");
     if (d->anisotropy < 0 || d->anisotropy > 1) return bad("unknown anisotropy");
-    if (d->solver < 0 || d->solver > 3) return bad("unknown solver");
+    if (d->solver < 0 || d->solver > 4) return bad("unknown solver");
     if (d->precision < 0 || d->precision > 1) return bad("unknown precision");
     if (d->noise < 0 || d->noise > 1) return bad("unknown noise mode");
     if (d->field.type < 0 || d->field.type > 6) return bad("unknown field type");

@@ -25,9 +25,9 @@ constexpr int kReduceThreads = 256; // threads per (sample, component) in the wi
 
 enum ProblemId : int { kNeel = 0, kNeelSpherical = 1, kBrownNeelEuler = 2, kBrownNeel = 3 };
 enum AnisoId : int { kUniaxial = 0, kCubic = 1 };
-enum SolverId : int { kEulerMaruyama = 0, kHeun = 1, kMillstein = 2, kImplicitMidpoint = 3 };
+enum SolverId : int { kEulerMaruyama = 0, kHeun = 1, kMillstein = 2, kImplicitMidpoint = 3, kEulerMaruyamaNormalized = 4 };
 // kernel-table slot of ImplicitMidpoint with the analytic Newton matrix (SP_JACOBIAN_EXACT)
-constexpr int kImplicitMidpointExact = 4;
+constexpr int kImplicitMidpointExact = 5;
 
 // number of derived parameters per problem
 constexpr int kParamsNeel = 16;

@@ -20,7 +20,7 @@ import pytest
 import oracle
 import stochasticphysics_b200 as sp
 from stochasticphysics_b200 import provider
-from stochasticphysics_b200._abi import Anisotropy, Jacobian, Noise, Precision, Problem, Solver
+from stochasticphysics_b200._abi import Anisotropy, FieldSpec, Jacobian, Noise, Precision, Problem, Solver
 
 pytestmark = pytest.mark.gpu
 
@@ -170,6 +170,43 @@ def test_exact_jacobian_fp32_state_with_fp64_acceptance(ctx):
     d = np.abs(r32.mean - r64.mean)
     assert d[1].max() < 1e-4
     assert d.max() < 4 * math.sqrt(2.0 / (3.0 * base.n))
+
+
+FIELDS = {
+    "triangular": FieldSpec.triangular((0.0, 0.0, 0.01), 2e-9, 3e-10, (1e-3, 0.0, 0.0)),
+    "rectangular": FieldSpec.rectangular((0.0, 0.004, 0.01), 2e-9, 1e-10, 3e-10, False),
+    "rectangular_alternating": FieldSpec.rectangular((0.0, 0.004, 0.01), 2e-9, 1e-10, 3e-10, True),
+    "sinc": FieldSpec.sinc((0.0, 0.0, 0.02), 2e-9, (0.0, 1e-3, 0.0)),
+}
+
+
+@pytest.mark.parametrize("name", list(FIELDS))
+def test_field_waveform_parity(ctx, name):
+    """Triangular, rectangular (plain and alternating) and sinc fields: the FP64 field
+    table and the window-mean field against the oracle, and a Heun run driven by them
+    (200 steps per period, 5 periods)."""
+    spec = dataclasses.replace(small_spec(Problem.Neel, Solver.Heun_Strong, steps=1000, W=50), field=FIELDS[name])
+    spec = provider.with_injected_noise(spec, seed=4)
+    gpu = ctx.simulate(spec, trajectories=True)
+    ref = oracle.simulate(spec, trajectories=True)
+    compare(gpu, ref)
+    assert np.ptp(ref["field"][1:], axis=0).max() > 1e-3  # the waveform actually varies
+
+
+@pytest.mark.parametrize("problem", [Problem.Neel, Problem.BrownAndNeel, Problem.NeelSpherical])
+def test_euler_maruyama_normalized_parity(ctx, problem):
+    """EulerMaruyama_Normalized: EulerMaruyama followed by the problem's normalize
+    (unit |m|, and |n| for the coupled Cartesian problem; no-op in spherical
+    coordinates), at a step where plain EulerMaruyama runs away for BrownAndNeel."""
+    spec = provider.with_injected_noise(small_spec(problem, Solver.EulerMaruyama_Normalized), seed=3)
+    gpu = ctx.simulate(spec, trajectories=True, final_state=True)
+    ref = oracle.simulate(spec, trajectories=True, final_state=True)
+    rel, mabs = conditioned_bars(spec, ref)
+    compare(gpu, ref, rel=rel, mean_abs=mabs)
+    assert gpu.stats["nonfinite_particles"] == 0
+    if problem != Problem.NeelSpherical:
+        fs = gpu.final_state.reshape(spec.n, -1, 3)
+        np.testing.assert_allclose(np.linalg.norm(fs, axis=2), 1.0, rtol=1e-14)
 
 
 def test_runaway_particles_match(ctx):

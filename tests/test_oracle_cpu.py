@@ -58,3 +58,16 @@ def test_op_counts_are_positive():
     assert 80 < ops["flops"] < 400
     ops_bn = oracle.count_ops(provider.brown_neel_relaxation(n=1, steps=1000, oversampling=100))
     assert ops_bn["flops"] > ops["flops"] and ops_bn["transcendentals"] > 5
+
+
+def test_euler_maruyama_normalized_keeps_unit_vectors():
+    """EulerMaruyama_Normalized.inl:40-56 on the CPU: after every step |m| = 1 (and
+    |n| = 1 for the coupled Cartesian problem), while plain EulerMaruyama drifts."""
+    import dataclasses
+    from stochasticphysics_b200 import provider
+    from stochasticphysics_b200._abi import Problem, Solver
+    base = provider.neel_relaxation(n=32, steps=500, oversampling=100)
+    em = oracle.simulate(dataclasses.replace(base, solver=Solver.EulerMaruyama), final_state=True)
+    emn = oracle.simulate(dataclasses.replace(base, solver=Solver.EulerMaruyama_Normalized), final_state=True)
+    np.testing.assert_allclose(np.linalg.norm(emn["final_state"], axis=1), 1.0, rtol=1e-14)
+    assert np.abs(np.linalg.norm(em["final_state"], axis=1) - 1).max() > 1e-9
