@@ -189,7 +189,8 @@ def test_field_waveform_parity(ctx, name):
     spec = provider.with_injected_noise(spec, seed=4)
     gpu = ctx.simulate(spec, trajectories=True)
     ref = oracle.simulate(spec, trajectories=True)
-    compare(gpu, ref)
+    rel, mabs = conditioned_bars(spec, ref)
+    compare(gpu, ref, rel=rel, mean_abs=mabs)
     assert np.ptp(ref["field"][1:], axis=0).max() > 1e-3  # the waveform actually varies
 
 
