@@ -22,6 +22,8 @@ Heun) on the device-resident state, i.e. 2 x 65536 x 10000 particle-steps.
                Lissajous field) through sp_server_*, FP32; p50/p99 latency,
                aggregate particle-steps/s, and the same requests one at a time in
                FP64 as the serial baseline
+  batched      256 Neel parameter sets (uneven N and S) submitted at once, batched
+               per kernel key into shared launches (N=1)
   --impl reference  runs that CPU restatement as the reference arm
 
 Launch shapes come from the autotuner (sp_autotune) unless --no-autotune.
@@ -199,6 +201,41 @@ def serving_leg(ctx, seconds, rate, step_scale, seed=0x5EED0005, serial_sample=4
     }
 
 
+def batched_leg(ctx, count, step_scale, seed=0x5EED0004, serial_sample=32):
+    """Parameter-set batch: `count` Neel ensembles with the batched-set distributions
+    (N ~ logU[1e3, 6.4e4], S ~ logU[1e5, 1e7] x step_scale, Heun / Millstein
+    alternating, FP32), all submitted at once to the server, which runs each kernel
+    key's members as one launch per chunk over a shared tile work-list.  Launch shapes
+    from the autotuner.  The same sets one at a time (every k-th, FP32) give the
+    unbatched rate."""
+    import stochasticphysics_b200 as sp
+    from stochasticphysics_b200 import provider
+    from stochasticphysics_b200._abi import Precision
+
+    specs = provider.batched_sets(count=count, seed=seed, precision=Precision.FP32, step_scale=step_scale)
+    for s in specs[:2]:
+        ctx.autotune(s, probe_particles=32768)
+    ps = sum(s.n * s.integrated_steps for s in specs)
+    free, _ = __import__("torch").cuda.mem_get_info()
+    with sp.Server(ctx, memory_budget_bytes=int(min(150e9, 0.8 * free))) as srv:
+        t = time.perf_counter()
+        ids = [srv.submit(s) for s in specs]
+        lat = [srv.wait(i)[1] for i in ids]
+        wall = time.perf_counter() - t
+    k = max(1, count // serial_sample)
+    sample = specs[::k][:serial_sample]
+    t = time.perf_counter()
+    for s in sample:
+        ctx.simulate(s)
+    serial_s = time.perf_counter() - t
+    return {"sets": count, "value": ps / wall, "unit": UNIT, "wall_s": wall, "particle_steps": ps,
+            "max_latency_ms": max(lat),
+            "one_at_a_time": {"value": sum(s.n * s.integrated_steps for s in sample) / serial_s, "sets": len(sample)},
+            "workload": f"Neel, N ~ logU[1e3, 6.4e4], S ~ logU[1e5, 1e7] x {step_scale}, |B| ~ U[1, 25] mT, "
+                        "f ~ logU[1e4, 1e6] Hz, K ~ U[5e3, 3e4] J/m^3, alpha ~ U[0.02, 0.3], Heun / Millstein "
+                        "alternating, FP32, W = 1000, dt = 1e-11 s"}
+
+
 def cpu_baseline(steps_sample=2000, n=None):
     """The CPU oracle on all host cores for a bounded sample of the workload."""
     import oracle
@@ -308,6 +345,9 @@ def main():
     ap.add_argument("--serving-rate", type=float, default=50.0, help="mean Poisson arrival rate (requests/s)")
     ap.add_argument("--serving-step-scale", type=float, default=0.006,
                     help="scale of the request step counts (S ~ logU[1e5, 1e7] x scale)")
+    ap.add_argument("--batched-sets", type=int, default=256, help="parameter sets of the batched leg (0: skip)")
+    ap.add_argument("--batched-step-scale", type=float, default=0.02,
+                    help="scale of the batched sets' step counts (S ~ logU[1e5, 1e7] x scale)")
     args = ap.parse_args()
     globals()["N_PER_GPU"], globals()["CHUNK"] = args.n_particles, args.chunk
     args.warmup = max(args.warmup, 3)
@@ -397,9 +437,11 @@ def main():
         e2e_value = world * ps_per_step * args.steps / e2e_s
         h2d = sum(s.n * 13 * 8 for s in e2e_specs)
         d2h = sum(o.mean.nbytes + o.weight.nbytes + o.time.nbytes + o.field.nbytes for o in outs)
-        serving = None
+        serving = batched = None
         if world == 1 and args.serving_seconds > 0:
             serving = serving_leg(ctx, args.serving_seconds, args.serving_rate, args.serving_step_scale)
+        if world == 1 and args.batched_sets > 0:
+            batched = batched_leg(ctx, args.batched_sets, args.batched_step_scale)
 
     if rank == 0:
         tpp, tsrc = profiled_traffic_per_particle()
@@ -436,6 +478,7 @@ def main():
             "cpu_baseline": cpu,
             "launch_shapes": shapes,
             "serving": serving,
+            "batched": batched,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

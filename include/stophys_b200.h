@@ -34,7 +34,7 @@
 extern "C" {
 #endif
 
-#define SP_ABI_VERSION 3u
+#define SP_ABI_VERSION 4u
 
 #if defined(_WIN32)
 #define SP_API __declspec(dllexport)
@@ -69,7 +69,13 @@ typedef enum sp_problem {
 /* Particle_Simulation/Problems/Anisotropy/AnisotropyList.h:45 */
 typedef enum sp_anisotropy {
     SP_ANISOTROPY_UNIAXIAL = 0,
-    SP_ANISOTROPY_CUBIC = 1
+    SP_ANISOTROPY_CUBIC = 1,
+    /* UniaxialCubicAnisotropy.hpp: a uniaxial part whose axis is the particle's z axis
+     * rotated by uniaxial_rotation (Euler ZXZ), plus a cubic part on the particle axes;
+     * anisotropy_constant = K_uniaxial, cubic_constant = K_cubic.  Not for the coupled
+     * Cartesian problem, where the reference's cubic torque is evaluated with zero Euler
+     * angles and divides by sin(0). */
+    SP_ANISOTROPY_UNIAXIAL_CUBIC = 2
 } sp_anisotropy;
 
 /* Particle_Simulation/Fields/FieldList.h:48 */
@@ -132,6 +138,9 @@ typedef struct sp_particles {
     const double* viscosity;                /* Pa s; Brown problems only          */
     const double* orientation;              /* [n][3] Euler angles phi,theta,psi (ZXZ) */
     const double* magnetisation;            /* [n][3] initial magnetisation direction  */
+    const double* cubic_constant;           /* UNIAXIAL_CUBIC only: K_cubic, J/m^3 (else NULL) */
+    const double* uniaxial_rotation;        /* UNIAXIAL_CUBIC only: [n][3] Euler angles of the
+                                               uniaxial axis (Uniaxial_Rotation; else NULL)  */
 } sp_particles;
 
 /* External field B(t) in tesla.

@@ -380,6 +380,10 @@ inline ParticleIn particle_in(const sp_ensemble_desc& d, uint64_t p) {
     r.viscosity = q.viscosity ? q.viscosity[p] : 0.0;
     r.temperature = d.temperature;
     for (int i = 0; i < 3; ++i) { r.euler[i] = q.orientation[3 * p + i]; r.mag[i] = q.magnetisation[3 * p + i]; }
+    if (d.anisotropy == SP_ANISOTROPY_UNIAXIAL_CUBIC) {
+        r.K2 = q.cubic_constant[p];
+        for (int i = 0; i < 3; ++i) r.urot[i] = q.uniaxial_rotation[3 * p + i];
+    }
     return r;
 }
 
@@ -408,6 +412,15 @@ using SimFn = void (*)(const SimSpec&, const ParticleIn&, uint64_t, double*, dou
 template <class T>
 SimFn<T> pick(int problem, int aniso) {
     const bool cubic = aniso == SP_ANISOTROPY_CUBIC;
+    if (aniso == SP_ANISOTROPY_UNIAXIAL_CUBIC) {
+        switch (problem) {
+            case SP_PROBLEM_NEEL: return &simulate_particle<NeelProblem<T, UniaxialCubic<T>>, T>;
+            case SP_PROBLEM_NEEL_SPHERICAL: return &simulate_particle<NeelSphericalProblem<T, UniaxialCubic<T>>, T>;
+            case SP_PROBLEM_BROWN_AND_NEEL_EULER_SPHERICAL:
+                return &simulate_particle<BrownNeelEulerProblem<T, UniaxialCubic<T>>, T>;
+        }
+        return nullptr;  // not defined for the coupled Cartesian problem
+    }
     switch (problem) {
         case SP_PROBLEM_NEEL:
             return cubic ? &simulate_particle<NeelProblem<T, Cubic<T>>, T> : &simulate_particle<NeelProblem<T, Uniaxial<T>>, T>;
@@ -497,6 +510,7 @@ int oracle_simulate(const sp_ensemble_desc* d, double* mean, double* weight, dou
     if (d->solver == SP_SOLVER_IMPLICIT_MIDPOINT && d->problem == SP_PROBLEM_BROWN_AND_NEEL_EULER_SPHERICAL) return 2;
     if (d->solver == SP_SOLVER_IMPLICIT_MIDPOINT && d->jacobian == SP_JACOBIAN_EXACT && d->problem != SP_PROBLEM_NEEL)
         return 3;
+    if (!pick<double>(d->problem, d->anisotropy)) return 4;
     const SimSpec s = spec_of(*d);
     const int OUT = out_dim(d->problem), SD = state_dim(d->problem);
     const uint64_t K = s.steps / s.W, N = d->n_particles;

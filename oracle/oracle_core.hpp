@@ -253,7 +253,54 @@ struct ParticleIn {
     double radius, Ms, alpha, gamma, K, rh, viscosity, temperature;
     double euler[3];
     double mag[3];
+    double K2 = 0.0;                   // uniaxial+cubic: K_cubic
+    double urot[3] = {0.0, 0.0, 0.0};  // uniaxial+cubic: Uniaxial_Rotation (Euler ZXZ)
 };
+
+template <class T> M3<T> transpose(const M3<T>& m) {
+    M3<T> r; for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) r(i, j) = m(j, i); return r;
+}
+
+// Problems/Anisotropy/UniaxialCubicAnisotropy.hpp:38-133: a uniaxial part whose axis is
+// R^T z (R from Uniaxial_Rotation, calcRotation :57-83) and a cubic part on the body axes.
+// The reference takes the uniaxial torque of R m on the unrotated z (:112-121) and the
+// uniaxial Jacobian on the unrotated z (:125-131); both are restated as written.
+template <class T>
+struct UniaxialCubic {
+    Uniaxial<T> uni;
+    Cubic<T> cub;
+    M3<T> rot;
+    void init(const ParticleIn& p, double V) {
+        uni.init(p.K, p.Ms, V);
+        cub.init(p.K2, p.Ms, V);
+        const double sphi = std::sin(p.urot[0]), cphi = std::cos(p.urot[0]);
+        const double st = std::sin(p.urot[1]), ct = std::cos(p.urot[1]);
+        const double sps = std::sin(p.urot[2]), cps = std::cos(p.urot[2]);
+        const double cc = cphi * cps, sc = sphi * cps, cs = cphi * sps, ss = sphi * sps;
+        const double r[3][3] = {{cc - ct * ss, -sc - ct * cs, st * sps},
+                                {ct * sc + cs, ct * cc - ss, -st * cps},
+                                {st * sphi, st * cphi, ct}};
+        for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) rot(i, j) = T(r[i][j]);
+    }
+    void prepareField(const V3<T>& ei, const V3<T>& xi, const V3<T>& yi, const V3<T>& zi) const {
+        cub.prepareField(ei, xi, yi, zi);  // the uniaxial part prepares nothing
+    }
+    V3<T> getAnisotropyField(const V3<T>& ei, const V3<T>& xi, const V3<T>& yi, const V3<T>& zi) const {
+        return uni.getAnisotropyField(ei, xi, yi, transpose(rot) * zi) + cub.getAnisotropyField(ei, xi, yi, zi);
+    }
+    V3<T> getEffTorque(const V3<T>& ei, const V3<T>& xi, const V3<T>& yi, const V3<T>& zi, const T* s, const T* c) const {
+        return uni.getEffTorque(rot * ei, xi, yi, zi, s, c) + cub.getEffTorque(ei, xi, yi, zi, s, c);
+    }
+    M3<T> getJacobiAnisotropyField(const V3<T>& ei, const V3<T>& xi, const V3<T>& yi, const V3<T>& zi) const {
+        return uni.getJacobiAnisotropyField(ei, xi, yi, zi) + cub.getJacobiAnisotropyField(ei, xi, yi, zi);
+    }
+    M3<T> getJacobiAnisotropyFieldExact(const V3<T>& ei, const V3<T>& xi, const V3<T>& yi, const V3<T>& zi) const {
+        return uni.getJacobiAnisotropyFieldExact(ei, xi, yi, transpose(rot) * zi) + cub.getJacobiAnisotropyFieldExact(ei, xi, yi, zi);
+    }
+};
+template <class T> void init_anisotropy(Uniaxial<T>& a, const ParticleIn& p, double V) { a.init(p.K, p.Ms, V); }
+template <class T> void init_anisotropy(Cubic<T>& a, const ParticleIn& p, double V) { a.init(p.K, p.Ms, V); }
+template <class T> void init_anisotropy(UniaxialCubic<T>& a, const ParticleIn& p, double V) { a.init(p, V); }
 struct ProblemCfg {
     bool useRot = false;       double minAngle = 0.0;       // NeelSpherical
     bool useBrownRot = false;  double brownMinAngle = 0.0;  // BrownAndNeelEulerSpherical

@@ -35,7 +35,7 @@ struct NeelProblem {
         DriftPrefactor = T(np.DriftPrefactor); NoisePrefactor = T(np.NoisePrefactor); Damping = T(np.Damping);
         euler_to_axes<T>(p.euler, xAxis, yAxis, zAxis);  // calculateParticleAxes (:223-261)
         const double V = sphere_volume(p.radius);
-        mAnisotropy.init(p.K, p.Ms, V);
+        init_anisotropy(mAnisotropy, p, V);
         moment = V * p.Ms;
     }
     // getStart (:263-285): the given magnetisation direction, normalised
@@ -149,7 +149,7 @@ struct NeelSphericalProblem {
         DriftPrefactor = T(np.DriftPrefactor); NoisePrefactor = T(np.NoisePrefactor); Damping = T(np.Damping);
         euler_to_axes<T>(p.euler, xAxis, yAxis, zAxis);  // (:614-620)
         const double V = sphere_volume(p.radius);
-        mAnisotropy.init(p.K, p.Ms, V);
+        init_anisotropy(mAnisotropy, p, V);
         moment = V * p.Ms;
         RotateCoordinateSystem = cfg.useRot;  // (:113)
         MinAngleBeforeRotation = T(cfg.minAngle);
@@ -350,7 +350,7 @@ struct BrownNeelEulerProblem {
         const double V = sphere_volume(p.radius);
         moment = V * p.Ms;
         MagneticMoment = T(moment);
-        mAnisotropy.init(p.K, p.Ms, V);
+        init_anisotropy(mAnisotropy, p, V);
         brownRot = cfg.useBrownRot; brownMin = T(cfg.brownMinAngle); brownMax = T(kPi - cfg.brownMinAngle);  // :129
         neelRot = cfg.useNeelRot; neelMin = T(cfg.neelMinAngle); neelMax = T(kPi - cfg.neelMinAngle);        // :130
     }
@@ -574,7 +574,7 @@ struct BrownNeelProblem {
         const double V = sphere_volume(p.radius);
         moment = V * p.Ms;
         MagneticMoment = T(moment);
-        mAnisotropy.init(p.K, p.Ms, V);
+        init_anisotropy(mAnisotropy, p, V);
         simple = cfg.simpleModel;
     }
     // getStart (.inl:278-324) with Use_random_* = false

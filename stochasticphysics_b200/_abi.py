@@ -13,7 +13,7 @@ from typing import Optional
 
 import numpy as np
 
-ABI_VERSION = 3
+ABI_VERSION = 4
 
 
 class Status(IntEnum):
@@ -42,6 +42,7 @@ class Problem(IntEnum):
 class Anisotropy(IntEnum):
     Uniaxial = 0
     Cubic = 1
+    UniaxialCubic = 2
 
 
 class FieldType(IntEnum):
@@ -107,6 +108,8 @@ class sp_particles(C.Structure):
         ("viscosity", _dp),
         ("orientation", _dp),
         ("magnetisation", _dp),
+        ("cubic_constant", _dp),
+        ("uniaxial_rotation", _dp),
     ]
 
 
@@ -317,6 +320,8 @@ class EnsembleSpec:
     injected_dw: Optional[np.ndarray] = None
     record_trajectories: bool = False
     jacobian: Jacobian = Jacobian.Reference
+    cubic_constant: Optional[np.ndarray] = None      # UniaxialCubic: K_cubic (n)
+    uniaxial_rotation: Optional[np.ndarray] = None   # UniaxialCubic: Euler angles of the uniaxial axis (n, 3)
 
     @property
     def dims(self):
@@ -335,11 +340,13 @@ class EnsembleSpec:
         import dataclasses
         kw = {}
         for name in ("magnetic_radius", "saturation_magnetisation", "damping_constant", "gyromagnetic_ratio",
-                     "anisotropy_constant", "hydrodynamic_radius", "viscosity"):
+                     "anisotropy_constant", "hydrodynamic_radius", "viscosity", "cubic_constant"):
             v = getattr(self, name)
             kw[name] = None if v is None else np.asarray(v)[lo:hi]
         kw["orientation"] = np.asarray(self.orientation).reshape(-1, 3)[lo:hi]
         kw["magnetisation"] = np.asarray(self.magnetisation).reshape(-1, 3)[lo:hi]
+        if self.uniaxial_rotation is not None:
+            kw["uniaxial_rotation"] = np.asarray(self.uniaxial_rotation).reshape(-1, 3)[lo:hi]
         if self.injected_dw is not None:
             m = self.dims[1]
             kw["injected_dw"] = np.asarray(self.injected_dw).reshape(-1, m, self.n)[:, :, lo:hi]
@@ -361,6 +368,8 @@ class DescHolder:
             "viscosity": None if spec.viscosity is None else _f64(spec.viscosity, n),
             "orientation": _f64(spec.orientation, shape=(n, 3)),
             "magnetisation": _f64(spec.magnetisation, shape=(n, 3)),
+            "cubic_constant": None if spec.cubic_constant is None else _f64(spec.cubic_constant, n),
+            "uniaxial_rotation": None if spec.uniaxial_rotation is None else _f64(spec.uniaxial_rotation, shape=(n, 3)),
         }
         self.dw = None if spec.injected_dw is None else _f64(spec.injected_dw)
         d = sp_ensemble_desc()

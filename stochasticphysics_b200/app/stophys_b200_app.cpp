@@ -231,6 +231,11 @@ struct ParticleTemplate {
     bool random_orientation = false, random_magnetisation = false;
     double orientation[3] = {0, 0, 0}, magnetisation[3] = {0, 0, 1};
     Dist r_dist, shell_dist, K_dist;
+    // uniaxial+cubic (Properties/Anisotropy/UniaxialCubic.hpp): K_cubic, the uniaxial
+    // rotation and their distributions
+    double K2 = 0, urot[3] = {0, 0, 0};
+    Dist K2_dist;
+    bool random_urot = false;
 };
 
 void read_particle(const Ini& p, ParticleTemplate& t) {
@@ -248,11 +253,24 @@ void read_particle(const Ini& p, ParticleTemplate& t) {
         const std::string a = lower(Ini::str(*v));
         if (a == "uniaxial") t.aniso = SP_ANISOTROPY_UNIAXIAL;
         else if (a == "cubic") t.aniso = SP_ANISOTROPY_CUBIC;
+        else if (a == "uniaxialcubic") t.aniso = SP_ANISOTROPY_UNIAXIAL_CUBIC;
         else throw std::runtime_error("unsupported Type_of_anisotropy '" + a + "'");
     }
-    const char* kkey = t.aniso == SP_ANISOTROPY_CUBIC ? "K_cubic" : "K_uniaxial";
-    if (auto v = p.within("Magnetic_Properties", kkey)) t.K = Ini::num(*v);
-    else if (auto v1 = p.within("Magnetic_Properties", "Anisotropy_1")) t.K = Ini::num(*v1);  // older layout
+    if (t.aniso == SP_ANISOTROPY_UNIAXIAL_CUBIC) {  // UniaxialCubic.hpp:44-50
+        if (auto v = p.within("Uniaxial_Part", "K_uniaxial")) t.K = Ini::num(*v);
+        else throw std::runtime_error("uniaxialcubic anisotropy needs Uniaxial_Part K_uniaxial");
+        if (auto v = p.within("Cubic_Part", "K_cubic")) t.K2 = Ini::num(*v);
+        else throw std::runtime_error("uniaxialcubic anisotropy needs Cubic_Part K_cubic");
+        if (auto v = p.within("Magnetic_Properties", "Uniaxial_Rotation")) {
+            const auto a = Ini::vec(*v);
+            if (a.size() != 3) throw std::runtime_error("Uniaxial_Rotation needs three values");
+            std::copy(a.begin(), a.end(), t.urot);
+        }
+    } else {
+        const char* kkey = t.aniso == SP_ANISOTROPY_CUBIC ? "K_cubic" : "K_uniaxial";
+        if (auto v = p.within("Magnetic_Properties", kkey)) t.K = Ini::num(*v);
+        else if (auto v1 = p.within("Magnetic_Properties", "Anisotropy_1")) t.K = Ini::num(*v1);  // older layout
+    }
 
     const std::string init = "Particle_Simulation_Initialization";
     if (auto v = p.within(init, "Use_random_initial_particle_orientation")) t.random_orientation = Ini::boolean(*v);
@@ -285,9 +303,21 @@ void read_particle(const Ini& p, ParticleTemplate& t) {
               "Use_relative_distribution_width_for_anisotropy_constants");
     // current layout: [..Anisotropy_Distribution] Distribution_type / Sigma_K_* / Use_relative_distribution_width
     const char* skey = t.aniso == SP_ANISOTROPY_CUBIC ? "Sigma_K_cubic" : "Sigma_K_uniaxial";
-    if (auto v = p.within("Anisotropy_Distribution", skey)) t.K_dist.width = Ini::num(*v);
-    if (auto v = p.within("Anisotropy_Distribution", "Distribution_type")) t.K_dist.type = lower(Ini::str(*v));
-    if (auto v = p.within("Anisotropy_Distribution", "Use_relative_distribution_width")) t.K_dist.relative = Ini::boolean(*v);
+    if (t.aniso == SP_ANISOTROPY_UNIAXIAL_CUBIC) {  // UniaxialCubic.hpp:52-88
+        auto part = [&](const char* sec, const char* sigma, Dist& d) {
+            d.sigma_times_mean = false;
+            if (auto v = p.within(sec, sigma)) d.width = Ini::num(*v);
+            if (auto v = p.within(sec, "Distribution_type")) d.type = lower(Ini::str(*v));
+            if (auto v = p.within(sec, "Use_relative_distribution_width")) d.relative = Ini::boolean(*v);
+        };
+        part("Uniaxial_Distribution", "Sigma_K_uniaxial", t.K_dist);
+        part("Cubic_Distribution", "Sigma_K_cubic", t.K2_dist);
+        if (auto v = p.within("Anisotropy_Distribution", "UseRandomCubicOrientation")) t.random_urot = Ini::boolean(*v);
+    } else {
+        if (auto v = p.within("Anisotropy_Distribution", skey)) t.K_dist.width = Ini::num(*v);
+        if (auto v = p.within("Anisotropy_Distribution", "Distribution_type")) t.K_dist.type = lower(Ini::str(*v));
+        if (auto v = p.within("Anisotropy_Distribution", "Use_relative_distribution_width")) t.K_dist.relative = Ini::boolean(*v);
+    }
 }
 
 // Euler angles (ZXZ, psi = 0) whose rotated x axis is the unit vector d: the
@@ -303,7 +333,7 @@ void euler_of_direction(const double* d, double* e) {
 
 struct Run {
     sp_ensemble_desc d{};
-    std::vector<double> r, Ms, alpha, gamma, K, rh, eta, euler, mag;
+    std::vector<double> r, Ms, alpha, gamma, K, rh, eta, euler, mag, K2, urot;
     std::vector<ParticleTemplate> templates;
     std::vector<uint64_t> used;
     std::string savefile;
@@ -431,6 +461,14 @@ Run build(const std::string& path, unsigned long long seed, int precision) {
         // applySettingsToParticleProperties order: anisotropy, radius, then the shell
         // around the new radius (ParticleSimulationSettings.h:138-144, 78-92)
         const double K = p.K_dist.apply(g, p.K);
+        if (d.anisotropy == SP_ANISOTROPY_UNIAXIAL_CUBIC) {
+            run.K2.push_back(p.K2_dist.apply(g, p.K2));
+            double ur[3] = {p.urot[0], p.urot[1], p.urot[2]};
+            if (p.random_urot) {  // UniaxialCubic.hpp:66-75: U[0,2pi), U[0,pi), U[0,2pi)
+                ur[0] = u(g) * 2 * kPi; ur[1] = u(g) * kPi; ur[2] = u(g) * 2 * kPi;
+            }
+            for (double c : ur) run.urot.push_back(c);
+        }
         const double r = p.r_dist.apply(g, p.r);
         const double rh = p.shell_dist.apply(g, p.rh - r) + r;
         run.K.push_back(K); run.r.push_back(r); run.rh.push_back(rh);
@@ -464,8 +502,10 @@ Run build(const std::string& path, unsigned long long seed, int precision) {
         for (int c = 0; c < 3; ++c) { run.euler.push_back(e[c]); run.mag.push_back(m[c] / nm); }
     }
     d.n_particles = n;
+    const bool uc = d.anisotropy == SP_ANISOTROPY_UNIAXIAL_CUBIC;
     d.particles = {run.r.data(), run.Ms.data(), run.alpha.data(), run.gamma.data(), run.K.data(),
-                   run.rh.data(), run.eta.data(), run.euler.data(), run.mag.data()};
+                   run.rh.data(), run.eta.data(), run.euler.data(), run.mag.data(),
+                   uc ? run.K2.data() : nullptr, uc ? run.urot.data() : nullptr};
     if (auto v = opt("Result_Settings", "Savefile")) run.savefile = Ini::str(*v);
     return run;
 }
@@ -629,6 +669,12 @@ void write_description(std::ostream& o, const Run& run) {
     jrows(o, run.euler.data(), n, 3);
     o << ",\"magnetisation\":";
     jrows(o, run.mag.data(), n, 3);
+    if (d.anisotropy == SP_ANISOTROPY_UNIAXIAL_CUBIC) {
+        o << ",\"cubic_constant\":";
+        jarr(o, run.K2.data(), n);
+        o << ",\"uniaxial_rotation\":";
+        jrows(o, run.urot.data(), n, 3);
+    }
     o << "},\"savefile\":" << jstr(run.savefile) << "}\n";
 }
 

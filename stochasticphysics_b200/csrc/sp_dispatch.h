@@ -24,7 +24,8 @@ constexpr int kSolverSlots = 6;
 inline int kernel_index(int aniso, int solver, int precision, int inject) {
     return ((aniso * kSolverSlots + solver) * 2 + precision) * 2 + inject;
 }
-constexpr int kKernelsPerProblem = 2 * kSolverSlots * 2 * 2;
+constexpr int kAnisoSlots = 3;
+constexpr int kKernelsPerProblem = kAnisoSlots * kSolverSlots * 2 * 2;
 // solver slot of a description: ImplicitMidpoint with SP_JACOBIAN_EXACT has its own kernels
 inline int solver_slot(int solver, int jacobian) {
     return (solver == kImplicitMidpoint && jacobian == 1) ? kImplicitMidpointExact : solver;

@@ -64,6 +64,7 @@ template <int PROB>
 void fill_problem(KernelSet* tab) {
     fill_aniso<PROB, kUniaxial>(tab);
     fill_aniso<PROB, kCubic>(tab);
+    if constexpr (PROB != kBrownNeel) fill_aniso<PROB, kUniaxialCubic>(tab);  // see SP_ANISOTROPY_UNIAXIAL_CUBIC
 }
 
 }  // namespace sp

@@ -22,10 +22,10 @@ namespace sp {
 
 // ------------------------------------------------------------------ problem traits
 template <int PROB, class R, int A> struct ProblemOf;
-template <class R, int A> struct ProblemOf<kNeel, R, A> { using type = NeelCart<R, A>; static constexpr int P = kParamsNeel; };
-template <class R, int A> struct ProblemOf<kNeelSpherical, R, A> { using type = NeelSph<R, A>; static constexpr int P = kParamsNeelSph; };
-template <class R, int A> struct ProblemOf<kBrownNeelEuler, R, A> { using type = BrownNeelEuler<R, A>; static constexpr int P = kParamsBrownNeelEuler; };
-template <class R, int A> struct ProblemOf<kBrownNeel, R, A> { using type = BrownNeelCart<R, A>; static constexpr int P = kParamsBrownNeel; };
+template <class R, int A> struct ProblemOf<kNeel, R, A> { using type = NeelCart<R, A>; static constexpr int P = param_count_of(kNeel, A); };
+template <class R, int A> struct ProblemOf<kNeelSpherical, R, A> { using type = NeelSph<R, A>; static constexpr int P = param_count_of(kNeelSpherical, A); };
+template <class R, int A> struct ProblemOf<kBrownNeelEuler, R, A> { using type = BrownNeelEuler<R, A>; static constexpr int P = param_count_of(kBrownNeelEuler, A); };
+template <class R, int A> struct ProblemOf<kBrownNeel, R, A> { using type = BrownNeelCart<R, A>; static constexpr int P = param_count_of(kBrownNeel, A); };
 
 // ------------------------------------------------------------------ FP64 parameter formulas
 constexpr double kBoltzmann = 1.3806485279E-23;  // ParameterCalculatorNeel.h:43
@@ -70,8 +70,21 @@ __device__ __forceinline__ void euler_axes(const double* e, double* x, double* y
     z[0] = stheta * sphi; z[1] = stheta * cphi; z[2] = ctheta;
 }
 
+// UniaxialCubicAnisotropy.hpp:57-83 calcRotation: rotation of the uniaxial part from its
+// Euler angles, row-major
+__device__ __forceinline__ void uniaxial_rotation(const double* e, double* Rm) {
+    double sphi, cphi, stheta, ctheta, spsi, cpsi;
+    sincos(e[0], &sphi, &cphi);
+    sincos(e[1], &stheta, &ctheta);
+    sincos(e[2], &spsi, &cpsi);
+    const double cphicpsi = cphi * cpsi, sphicpsi = sphi * cpsi, cphispsi = cphi * spsi, sphispsi = sphi * spsi;
+    Rm[0] = cphicpsi - ctheta * sphispsi; Rm[1] = -sphicpsi - ctheta * cphispsi; Rm[2] = stheta * spsi;
+    Rm[3] = ctheta * sphicpsi + cphispsi; Rm[4] = ctheta * cphicpsi - sphispsi; Rm[5] = -stheta * cpsi;
+    Rm[6] = stheta * sphi; Rm[7] = stheta * cphi; Rm[8] = ctheta;
+}
+
 // Fills params[k] (FP64) and the initial state y (FP64) of particle p.
-template <int PROB>
+template <int PROB, int A>
 __device__ __forceinline__ void particle_setup(const RawParticles& rp, unsigned long long p, double* prm, double* y,
                                                double& moment) {
     const double r = rp.radius[p], Ms = rp.Ms[p], alpha = rp.alpha[p], gamma = rp.gamma[p], K = rp.K[p];
@@ -95,6 +108,14 @@ __device__ __forceinline__ void particle_setup(const RawParticles& rp, unsigned 
             for (int i = 0; i < 3; ++i) { prm[6 + i] = z[i]; prm[9 + i] = x[i]; prm[12 + i] = yy[i]; }
             y[0] = acos(mg[2]); y[1] = atan2(mg[1], mg[0]);  // ParticleStateInitializer.h:132-144
         }
+        if constexpr (A == kUniaxialCubic) {
+            // cubic field prefactor and the uniaxial axis R^T z (UniaxialCubicAnisotropy.hpp:104-110)
+            const int o = (PROB == kNeel) ? kParamsNeel : kParamsNeelSph;
+            double Rm[9];
+            uniaxial_rotation(rp.urot + 3 * p, Rm);
+            prm[o] = -2.0 * rp.K2[p] / Ms;
+            for (int i = 0; i < 3; ++i) prm[o + 1 + i] = Rm[0 * 3 + i] * z[0] + Rm[1 * 3 + i] * z[1] + Rm[2 * 3 + i] * z[2];
+        }
     } else {
         const BrownP bp = brown_params(rp.rh[p], rp.viscosity[p], rp.temperature);
         const double a = np.NF1, b = np.NF2, DN = np.DN;
@@ -108,6 +129,13 @@ __device__ __forceinline__ void particle_setup(const RawParticles& rp, unsigned 
             prm[12] = 0.5 * bp.cF * bp.cF + 0.5 * (a * a + bpd * bpd) * (DN * DN);
             y[0] = e[0]; y[1] = e[1]; y[2] = e[2];  // BrownAndNeelRelaxationEulerSpherical.h:741-753
             y[3] = acos(mg[2]); y[4] = atan2(mg[1], mg[0]);
+            if constexpr (A == kUniaxialCubic) {
+                // cubic field and torque prefactors and the uniaxial rotation R
+                // (UniaxialCubicAnisotropy.hpp:104-121: field with R^T z, torque of R m)
+                prm[13] = -2.0 * rp.K2[p] / Ms;
+                prm[14] = bp.c * (-2.0 * rp.K2[p] * V);
+                uniaxial_rotation(rp.urot + 3 * p, prm + 15);
+            }
         } else {
             const bool simple = rp.simple_model != 0;
             prm[0] = a; prm[1] = bpd; prm[2] = d; prm[3] = cT; prm[4] = pF; prm[5] = bp.cF;
@@ -159,7 +187,7 @@ __global__ void __launch_bounds__(kMaxBlock) init_kernel(const EnsDev* __restric
     R* prm = const_cast<R*>(static_cast<const R*>(e.params));
     double yd[D], pd[P > 0 ? P : 1], moment = 0.0;
     if (active) {
-        particle_setup<PROB>(rp, p, pd, yd, moment);
+        particle_setup<PROB, A>(rp, p, pd, yd, moment);
     } else {
         for (int i = 0; i < D; ++i) yd[i] = 0.0;
         for (int i = 0; i < P; ++i) pd[i] = 0.0;

@@ -126,7 +126,7 @@ const KernelSet& kernel_set(int problem, int aniso, int solver, int precision, i
         fill_brown_neel(table[kBrownNeel]);
     });
     static const KernelSet invalid{};
-    if (problem < 0 || problem > 3 || aniso < 0 || aniso > 1 || solver < 0 || solver >= kSolverSlots || precision < 0 ||
+    if (problem < 0 || problem > 3 || aniso < 0 || aniso >= kAnisoSlots || solver < 0 || solver >= kSolverSlots || precision < 0 ||
         precision > 1 || inject < 0 || inject > 1)
         return invalid;
     return table[problem][kernel_index(aniso, solver, precision, inject)];

@@ -84,7 +84,8 @@ extern "C" SP_API sp_status sp_simulate_noalloc(const sp_ensemble_desc* desc, co
         const sp_particles& dp = *device_particles;
         const bool brown = desc->problem == SP_PROBLEM_BROWN_AND_NEEL || desc->problem == SP_PROBLEM_BROWN_AND_NEEL_EULER_SPHERICAL;
         if (!dp.magnetic_radius || !dp.saturation_magnetisation || !dp.damping_constant || !dp.gyromagnetic_ratio ||
-            !dp.anisotropy_constant || !dp.orientation || !dp.magnetisation || (brown && (!dp.hydrodynamic_radius || !dp.viscosity)))
+            !dp.anisotropy_constant || !dp.orientation || !dp.magnetisation || (brown && (!dp.hydrodynamic_radius || !dp.viscosity)) ||
+            (desc->anisotropy == SP_ANISOTROPY_UNIAXIAL_CUBIC && (!dp.cubic_constant || !dp.uniaxial_rotation)))
             return fail(SP_ERR_INVALID_ARG, "a required device per-particle array is NULL");
 
         int device = 0;
@@ -156,6 +157,7 @@ extern "C" SP_API sp_status sp_simulate_noalloc(const sp_ensemble_desc* desc, co
         rp.rh = brown ? dp.hydrodynamic_radius : dp.magnetic_radius;  // unread by the Neel problems
         rp.viscosity = brown ? dp.viscosity : dp.magnetic_radius;
         rp.euler = dp.orientation; rp.mag = dp.magnetisation;
+        rp.K2 = dp.cubic_constant; rp.urot = dp.uniaxial_rotation;
         rp.temperature = desc->temperature;
         rp.simple_model = desc->problem_settings.use_simple_model;
         ks.init(d_ens, rp, L.Np, s);

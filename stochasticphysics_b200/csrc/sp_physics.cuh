@@ -77,6 +77,14 @@ struct Aniso {
     }
 };
 
+// Uniaxial+cubic (UniaxialCubicAnisotropy.hpp:95-133): the uniaxial part on the rotated
+// axis zr = R^T z plus the cubic part on the body axes, then the external field.
+template <class R>
+__device__ __forceinline__ V3<R> heff_uniaxial_cubic(R pFu, V3<R> zr, R pFc, V3<R> m, V3<R> x, V3<R> y, V3<R> z, V3<R> B) {
+    const V3<R> zero = v3(R(0), R(0), R(0));
+    return (Aniso<R, kUniaxial>::heff(pFu, m, x, y, zr, zero) + Aniso<R, kCubic>::heff(pFc, m, x, y, z, zero)) + B;
+}
+
 // ======================================================================= Neel (Cartesian)
 template <class R, int A>
 struct NeelCart {
@@ -85,6 +93,8 @@ struct NeelCart {
     struct Par {
         R NF1, NF2, Dp, pre1, pre2, pF, twoalpha;
         V3<R> z, x, y;
+        R pF2;     // uniaxial+cubic: cubic field prefactor
+        V3<R> zr;  // uniaxial+cubic: rotated uniaxial axis R^T z
     };
     struct Cache {};
     static __device__ __forceinline__ Par load(const R* P, unsigned long long Np, unsigned long long p) {
@@ -92,20 +102,31 @@ struct NeelCart {
         q.NF1 = P[0 * Np + p]; q.NF2 = P[1 * Np + p]; q.Dp = P[2 * Np + p];
         q.pre1 = P[3 * Np + p]; q.pre2 = P[4 * Np + p]; q.pF = P[5 * Np + p]; q.twoalpha = P[6 * Np + p];
         q.z = v3(P[7 * Np + p], P[8 * Np + p], P[9 * Np + p]);
-        if constexpr (A == kCubic) {
+        if constexpr (A != kUniaxial) {
             q.x = v3(P[10 * Np + p], P[11 * Np + p], P[12 * Np + p]);
             q.y = v3(P[13 * Np + p], P[14 * Np + p], P[15 * Np + p]);
         } else {
             q.x = q.y = v3(R(0), R(0), R(0));
         }
+        if constexpr (A == kUniaxialCubic) {
+            q.pF2 = P[16 * Np + p];
+            q.zr = v3(P[17 * Np + p], P[18 * Np + p], P[19 * Np + p]);
+        } else {
+            q.pF2 = R(0);
+            q.zr = q.z;
+        }
         return q;
+    }
+    static __device__ __forceinline__ V3<R> heff(const Par& q, V3<R> m, const R* B) {
+        if constexpr (A == kUniaxialCubic) return heff_uniaxial_cubic(q.pF, q.zr, q.pF2, m, q.x, q.y, q.z, v3(B[0], B[1], B[2]));
+        else return Aniso<R, A>::heff(q.pF, m, q.x, q.y, q.z, v3(B[0], B[1], B[2]));
     }
     static __device__ __forceinline__ void prepare(const Par&, const Rot<R>&, R*, Cache&) {}
     static __device__ __forceinline__ void recompute(const Par&, const R*, Cache&) {}
     static __device__ __forceinline__ void finish(const Rot<R>&, R*, const Cache&) {}
     static __device__ __forceinline__ void det(const Par& q, const R* y, const Cache&, const R* B, R* a) {
         const V3<R> m = v3(y[0], y[1], y[2]);
-        const V3<R> H = Aniso<R, A>::heff(q.pF, m, q.x, q.y, q.z, v3(B[0], B[1], B[2]));
+        const V3<R> H = heff(q, m, B);
         const V3<R> mxH = cross(m, H);
         const V3<R> r = q.NF1 * mxH - q.NF2 * cross(m, mxH);
         a[0] = r.x; a[1] = r.y; a[2] = r.z;
@@ -133,11 +154,16 @@ struct NeelCart {
     static __device__ __forceinline__ void newton_matrix(const Par& q, const R* y, const Cache&, const R* B, const R* w,
                                                          R dt, R S[D][D]) {
         const V3<R> m = v3(y[0], y[1], y[2]);
-        const V3<R> H = Aniso<R, A>::heff(q.pF, m, q.x, q.y, q.z, v3(B[0], B[1], B[2]));
+        const V3<R> H = heff(q, m, B);
+        // uniaxial: pF z z^T; cubic: I; uniaxial+cubic: the sum, with the unrotated z
+        // (UniaxialCubicAnisotropy.hpp:125-131)
         R JH[3][3];
         const R zz[3] = {q.z.x, q.z.y, q.z.z};
         for (int i = 0; i < 3; ++i)
-            for (int j = 0; j < 3; ++j) JH[i][j] = (A == kUniaxial) ? (q.pF * zz[i]) * zz[j] : R(i == j ? 1 : 0);
+            for (int j = 0; j < 3; ++j) {
+                const R ju = (A != kCubic) ? (q.pF * zz[i]) * zz[j] : R(0);
+                JH[i][j] = (A == kUniaxial) ? ju : (A == kCubic ? R(i == j ? 1 : 0) : ju + R(i == j ? 1 : 0));
+            }
         const R mx[3][3] = {{R(0), -m.z, m.y}, {m.z, R(0), -m.x}, {-m.y, m.x, R(0)}};
         const R hx[3][3] = {{R(0), -H.z, H.y}, {H.z, R(0), -H.x}, {-H.y, H.x, R(0)}};
         const R wx[3][3] = {{R(0), -w[2], w[1]}, {w[2], R(0), -w[0]}, {-w[1], w[0], R(0)}};
@@ -159,9 +185,19 @@ struct NeelCart {
     static __device__ __forceinline__ void newton_matrix_exact(const Par& q, const R* y, const Cache&, const R* B,
                                                                const R* w, R dt, R S[D][D]) {
         const V3<R> m = v3(y[0], y[1], y[2]);
-        const V3<R> H = Aniso<R, A>::heff(q.pF, m, q.x, q.y, q.z, v3(B[0], B[1], B[2]));
+        const V3<R> H = heff(q, m, B);
         R JH[3][3];
-        Aniso<R, A>::jacobian(q.pF, m, q.x, q.y, q.z, JH);
+        if constexpr (A == kUniaxialCubic) {
+            R J2[3][3];
+            Aniso<R, kUniaxial>::jacobian(q.pF, m, q.x, q.y, q.zr, JH);
+            Aniso<R, kCubic>::jacobian(q.pF2, m, q.x, q.y, q.z, J2);
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+#pragma unroll
+                for (int j = 0; j < 3; ++j) JH[i][j] = JH[i][j] + J2[i][j];
+        } else {
+            Aniso<R, A>::jacobian(q.pF, m, q.x, q.y, q.z, JH);
+        }
         const V3<R> u = cross(m, H);
         const V3<R> W = v3(w[0], w[1], w[2]);
         const R mw = dot(m, W);
@@ -190,6 +226,8 @@ struct NeelSph {
     struct Par {
         R NF1, NF2, Dp, DN, pF, twoalpha;
         V3<R> z, x, y;
+        R pF2;     // uniaxial+cubic: cubic field prefactor
+        V3<R> zr;  // uniaxial+cubic: rotated uniaxial axis R^T z
     };
     struct Cache {
         bool rot;
@@ -202,13 +240,24 @@ struct NeelSph {
         q.NF1 = P[0 * Np + p]; q.NF2 = P[1 * Np + p]; q.Dp = P[2 * Np + p]; q.DN = P[3 * Np + p];
         q.pF = P[4 * Np + p]; q.twoalpha = P[5 * Np + p];
         q.z = v3(P[6 * Np + p], P[7 * Np + p], P[8 * Np + p]);
-        if constexpr (A == kCubic) {
+        if constexpr (A != kUniaxial) {
             q.x = v3(P[9 * Np + p], P[10 * Np + p], P[11 * Np + p]);
             q.y = v3(P[12 * Np + p], P[13 * Np + p], P[14 * Np + p]);
         } else {
             q.x = q.y = v3(R(0), R(0), R(0));
         }
+        if constexpr (A == kUniaxialCubic) {
+            q.pF2 = P[15 * Np + p];
+            q.zr = v3(P[16 * Np + p], P[17 * Np + p], P[18 * Np + p]);
+        } else {
+            q.pF2 = R(0);
+            q.zr = q.z;
+        }
         return q;
+    }
+    static __device__ __forceinline__ V3<R> heff(const Par& q, V3<R> m, const R* B) {
+        if constexpr (A == kUniaxialCubic) return heff_uniaxial_cubic(q.pF, q.zr, q.pF2, m, q.x, q.y, q.z, v3(B[0], B[1], B[2]));
+        else return Aniso<R, A>::heff(q.pF, m, q.x, q.y, q.z, v3(B[0], B[1], B[2]));
     }
     // NeelRelaxationSpherical.h:568-602
     static __device__ __forceinline__ void rotate(R* y) {
@@ -260,7 +309,7 @@ struct NeelSph {
         else { y[0] = wrap_two_pi(y[0]); y[1] = wrap_two_pi(y[1]); }
     }
     static __device__ __forceinline__ void det(const Par& q, const R*, const Cache& c, const R* B, R* a) {
-        const V3<R> H = Aniso<R, A>::heff(q.pF, c.md, q.x, q.y, q.z, v3(B[0], B[1], B[2]));
+        const V3<R> H = heff(q, c.md, B);
         a[0] = dot(c.P0, H);
         a[1] = dot(c.P1, H);
     }
@@ -290,14 +339,16 @@ struct NeelSph {
         const V3<R> Jth0 = (R(-1)) * c.md, Jth1 = cos_t * c.eph;
         const V3<R> Jph0 = v3(R(0), R(0), R(0));
         const V3<R> Jph1 = c.rot ? v3(R(0), c.eph.z, -c.eph.y) : v3(-c.eph.y, c.eph.x, R(0));
-        const V3<R> H = Aniso<R, A>::heff(q.pF, c.md, q.x, q.y, q.z, v3(B[0], B[1], B[2]));
+        const V3<R> H = heff(q, c.md, B);
         const R a = q.NF1, b = q.NF2;
-        // J_H J_er^T columns (3-vectors), c = 0, 1
+        // J_H J_er^T columns (3-vectors), c = 0, 1; J_H as in the reference: uniaxial
+        // pF z z^T, cubic I, uniaxial+cubic their sum with the unrotated z
         V3<R> HJer[2];
         const V3<R> Jer[2] = {Jer0, Jer1};
         for (int k = 0; k < 2; ++k) {
             if constexpr (A == kUniaxial) HJer[k] = (q.pF * dot(q.z, Jer[k])) * q.z;
-            else HJer[k] = Jer[k];
+            else if constexpr (A == kCubic) HJer[k] = Jer[k];
+            else HJer[k] = (q.pF * dot(q.z, Jer[k])) * q.z + Jer[k];
         }
         const V3<R> A0[2] = {(-a) * Jph0 + b * Jth0, (-a) * Jph1 + b * Jth1};  // rows of (-a J_phi + b J_theta)
         const V3<R> B1[2] = {c.odst * (a * Jth0 + b * Jph0), c.odst * (a * Jth1 + b * Jph1)};
@@ -312,7 +363,8 @@ struct NeelSph {
             // (P1 J_H) J_er^T
             V3<R> P1JH;
             if constexpr (A == kUniaxial) P1JH = (q.pF * dot(c.P1, q.z)) * q.z;
-            else P1JH = c.P1;
+            else if constexpr (A == kCubic) P1JH = c.P1;
+            else P1JH = (q.pF * dot(c.P1, q.z)) * q.z + c.P1;
             Jd[1][k] = dot(H, rowk) + dot(P1JH, Jer[k]);
             Js[1][k] = q.DN * dot(W, rowk);
         }
@@ -340,6 +392,8 @@ struct BrownNeelEuler {
     static constexpr bool kHasExactJacobian = false;
     struct Par {
         R a, bpd, d, cT, pF, cF, dDN, bpdDN, aDN, adDN2, d2fDN2, cF2h, nd;
+        R pF2, cT2;  // uniaxial+cubic: cubic field and torque prefactors
+        R Rm[9];     // uniaxial+cubic: rotation of the uniaxial part, row-major
     };
     struct Cache {
         bool br, nr;
@@ -353,6 +407,12 @@ struct BrownNeelEuler {
         q.pF = P[4 * Np + p]; q.cF = P[5 * Np + p]; q.dDN = P[6 * Np + p]; q.bpdDN = P[7 * Np + p];
         q.aDN = P[8 * Np + p]; q.adDN2 = P[9 * Np + p]; q.d2fDN2 = P[10 * Np + p]; q.cF2h = P[11 * Np + p];
         q.nd = P[12 * Np + p];
+        if constexpr (A == kUniaxialCubic) {
+            q.pF2 = P[13 * Np + p];
+            q.cT2 = P[14 * Np + p];
+#pragma unroll
+            for (int i = 0; i < 9; ++i) q.Rm[i] = P[(15 + i) * Np + p];
+        }
         return q;
     }
     // :859-899
@@ -430,19 +490,40 @@ struct BrownNeelEuler {
             o[1] = -v.x - (sp * ct * od) * v.y - (cp * ct * od) * v.z;
         }
     }
-    // c*Teff: uniaxial (UniaxialAnisotropy.h:146-150) or cubic (CubicAnisotropy.h:162-193)
+    // c*Teff of the cubic part (CubicAnisotropy.h:162-193)
+    static __device__ __forceinline__ V3<R> ctorque_cubic(R cT, const Cache& c, V3<R> m, V3<R> x, V3<R> y, V3<R> z) {
+        const R c1 = dot(m, x), c2 = dot(m, y), c3 = dot(m, z);
+        const R c1s = c1 * c1, c2s = c2 * c2;
+        const R ctheta = c.C[1], cpsi = c.C[2], stheta = c.S[1], spsi = c.S[2];
+        const V3<R> th = v3(ctheta * spsi, -ctheta * cpsi, -stheta);
+        const V3<R> sym = cross(z, (c3 * (c1s + c2s)) * m);
+        const V3<R> asdir = (ctheta / stheta) * th + z;
+        return cT * (sym + (c1 * c2 * (c2s - c1s)) * asdir);
+    }
+    static __device__ __forceinline__ V3<R> rot_apply(const Par& q, V3<R> v) {  // R v
+        return v3(q.Rm[0] * v.x + q.Rm[1] * v.y + q.Rm[2] * v.z, q.Rm[3] * v.x + q.Rm[4] * v.y + q.Rm[5] * v.z,
+                  q.Rm[6] * v.x + q.Rm[7] * v.y + q.Rm[8] * v.z);
+    }
+    static __device__ __forceinline__ V3<R> rot_apply_t(const Par& q, V3<R> v) {  // R^T v
+        return v3(q.Rm[0] * v.x + q.Rm[3] * v.y + q.Rm[6] * v.z, q.Rm[1] * v.x + q.Rm[4] * v.y + q.Rm[7] * v.z,
+                  q.Rm[2] * v.x + q.Rm[5] * v.y + q.Rm[8] * v.z);
+    }
+    // c*Teff: uniaxial (UniaxialAnisotropy.h:146-150), cubic, or uniaxial+cubic, whose
+    // uniaxial torque is taken of R m on the unrotated axis (UniaxialCubicAnisotropy.hpp:112-121)
     static __device__ __forceinline__ V3<R> ctorque(const Par& q, const Cache& c, V3<R> m, V3<R> x, V3<R> y, V3<R> z) {
         if constexpr (A == kUniaxial) {
             return (q.cT * dot(m, z)) * cross(z, m);
+        } else if constexpr (A == kCubic) {
+            return ctorque_cubic(q.cT, c, m, x, y, z);
         } else {
-            const R c1 = dot(m, x), c2 = dot(m, y), c3 = dot(m, z);
-            const R c1s = c1 * c1, c2s = c2 * c2;
-            const R ctheta = c.C[1], cpsi = c.C[2], stheta = c.S[1], spsi = c.S[2];
-            const V3<R> th = v3(ctheta * spsi, -ctheta * cpsi, -stheta);
-            const V3<R> sym = cross(z, (c3 * (c1s + c2s)) * m);
-            const V3<R> asdir = (ctheta / stheta) * th + z;
-            return q.cT * (sym + (c1 * c2 * (c2s - c1s)) * asdir);
+            const V3<R> rm = rot_apply(q, m);
+            return (q.cT * dot(rm, z)) * cross(z, rm) + ctorque_cubic(q.cT2, c, m, x, y, z);
         }
+    }
+    static __device__ __forceinline__ V3<R> heff(const Par& q, V3<R> m, V3<R> x, V3<R> y, V3<R> z, const R* B) {
+        if constexpr (A == kUniaxialCubic)
+            return heff_uniaxial_cubic(q.pF, rot_apply_t(q, z), q.pF2, m, x, y, z, v3(B[0], B[1], B[2]));
+        else return Aniso<R, A>::heff(q.pF, m, x, y, z, v3(B[0], B[1], B[2]));
     }
     static __device__ __forceinline__ void finish(const Rot<R>&, R* y, const Cache& c) {
         if (c.br) euler_unrotate(y);
@@ -454,7 +535,7 @@ struct BrownNeelEuler {
     static __device__ __forceinline__ void det(const Par& q, const R*, const Cache& c, const R* B, R* a) {
         V3<R> x, y, z;
         axes(c, x, y, z);
-        const V3<R> H = Aniso<R, A>::heff(q.pF, c.md, x, y, z, v3(B[0], B[1], B[2]));
+        const V3<R> H = heff(q, c.md, x, y, z, B);
         const V3<R> cTe = ctorque(q, c, c.md, x, y, z);
         const V3<R> mxH = cross(c.md, H);
         const V3<R> wb = eproj(c, cTe + q.d * mxH);

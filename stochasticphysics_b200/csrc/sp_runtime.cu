@@ -40,9 +40,7 @@ sp_status fail(sp_status s, const std::string& msg) {
 int state_dim(int p) { return p == 0 ? 3 : p == 1 ? 2 : p == 2 ? 5 : 6; }
 int noise_dim(int p) { return (p == 0 || p == 1) ? 3 : 6; }
 int out_dim(int p) { return p == 0 ? 3 : p == 1 ? 3 : p == 2 ? 9 : 6; }
-int param_count(int p) {
-    return p == 0 ? kParamsNeel : p == 1 ? kParamsNeelSph : p == 2 ? kParamsBrownNeelEuler : kParamsBrownNeel;
-}
+int param_count(int p, int aniso) { return param_count_of(p, aniso); }
 
 // ------------------------------------------------------------------ validation
 sp_status validate_desc(const sp_ensemble_desc* d, std::string& why) {
@@ -50,7 +48,7 @@ sp_status validate_desc(const sp_ensemble_desc* d, std::string& why) {
     if (!d) return bad("description is NULL");
     if (d->abi_version != SP_ABI_VERSION) return bad("abi_version mismatch");
     if (d->problem < 0 || d->problem > 3) return bad("unknown problem");
-    if (d->anisotropy < 0 || d->anisotropy > 1) return bad("unknown anisotropy");
+    if (d->anisotropy < 0 || d->anisotropy > 2) return bad("unknown anisotropy");
     if (d->solver < 0 || d->solver > 4) return bad("unknown solver");
     if (d->precision < 0 || d->precision > 1) return bad("unknown precision");
     if (d->noise < 0 || d->noise > 1) return bad("unknown noise mode");
@@ -72,6 +70,15 @@ sp_status validate_desc(const sp_ensemble_desc* d, std::string& why) {
         (!q.hydrodynamic_radius || !q.viscosity))
         return bad("Brown problems need hydrodynamic_radius and viscosity");
     if (d->noise == SP_NOISE_INJECTED && !d->injected_dw) return bad("injected noise mode needs injected_dw");
+    if (d->anisotropy == SP_ANISOTROPY_UNIAXIAL_CUBIC) {
+        if (!q.cubic_constant || !q.uniaxial_rotation)
+            return bad("uniaxial+cubic anisotropy needs cubic_constant and uniaxial_rotation");
+        if (d->problem == SP_PROBLEM_BROWN_AND_NEEL) {
+            why = "uniaxial+cubic anisotropy is not defined for the coupled Cartesian problem (the reference's cubic "
+                  "torque divides by the sine of zero Euler angles there)";
+            return SP_ERR_UNSUPPORTED_COMBO;
+        }
+    }
     if (d->solver == SP_SOLVER_IMPLICIT_MIDPOINT) {
         if (d->problem == SP_PROBLEM_BROWN_AND_NEEL_EULER_SPHERICAL) {
             why = "ImplicitMidpoint needs Jacobians, which BrownAndNeelEulerSpherical does not provide";
@@ -113,7 +120,7 @@ EnsembleLayout layout_of(const sp_ensemble_desc& d, const LaunchConfig& lc) {
     L.D = state_dim(d.problem);
     L.Mn = noise_dim(d.problem);
     L.OUT = out_dim(d.problem);
-    L.P = param_count(d.problem);
+    L.P = param_count(d.problem, d.anisotropy);
     L.real = d.precision == SP_PRECISION_FP32 ? 4 : 8;
     L.n = d.n_particles;
     L.Np = round_up(L.n, kPad);
@@ -275,14 +282,20 @@ void Ensemble::upload_and_init(const sp_ensemble_desc& d) {
     const size_t n = L.n;
     const sp_particles& q = d.particles;
     const bool brown = d.problem == SP_PROBLEM_BROWN_AND_NEEL || d.problem == SP_PROBLEM_BROWN_AND_NEEL_EULER_SPHERICAL;
-    // one staging buffer: 7 scalars + 6 vector components per particle
-    std::vector<double> host(n * 13, 0.0);
+    // one staging buffer: 7 scalars + 6 vector components per particle (+ K_cubic and the
+    // uniaxial rotation for the uniaxial+cubic anisotropy)
+    const bool uc = d.anisotropy == SP_ANISOTROPY_UNIAXIAL_CUBIC;
+    std::vector<double> host(n * (uc ? 17 : 13), 0.0);
     const double* src[7] = {q.magnetic_radius, q.saturation_magnetisation, q.damping_constant, q.gyromagnetic_ratio,
                             q.anisotropy_constant, brown ? q.hydrodynamic_radius : nullptr, brown ? q.viscosity : nullptr};
     for (int k = 0; k < 7; ++k)
         if (src[k]) std::memcpy(host.data() + k * n, src[k], n * 8);
     std::memcpy(host.data() + 7 * n, q.orientation, n * 24);
     std::memcpy(host.data() + 10 * n, q.magnetisation, n * 24);
+    if (uc) {
+        std::memcpy(host.data() + 13 * n, q.cubic_constant, n * 8);
+        std::memcpy(host.data() + 14 * n, q.uniaxial_rotation, n * 24);
+    }
     double* dev = nullptr;
     check_cuda(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&dev), host.size() * 8, ctx->pool, stream),
                "cudaMallocFromPoolAsync");
@@ -291,6 +304,8 @@ void Ensemble::upload_and_init(const sp_ensemble_desc& d) {
     RawParticles rp;
     rp.radius = dev; rp.Ms = dev + n; rp.alpha = dev + 2 * n; rp.gamma = dev + 3 * n; rp.K = dev + 4 * n;
     rp.rh = dev + 5 * n; rp.viscosity = dev + 6 * n; rp.euler = dev + 7 * n; rp.mag = dev + 10 * n;
+    rp.K2 = uc ? dev + 13 * n : nullptr;
+    rp.urot = uc ? dev + 14 * n : nullptr;
     rp.temperature = d.temperature;
     rp.simple_model = d.problem_settings.use_simple_model;
     ks->init(d_ens, rp, L.Np, stream);

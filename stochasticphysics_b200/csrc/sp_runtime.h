@@ -41,7 +41,7 @@ sp_status validate_desc(const sp_ensemble_desc* d, std::string& why);
 int state_dim(int p);
 int noise_dim(int p);
 int out_dim(int p);
-int param_count(int p);
+int param_count(int p, int aniso);
 FieldParams field_params(const sp_field_desc& f);
 void reference_times(unsigned long long K, unsigned long long W, double dt, double* times);
 

@@ -89,7 +89,7 @@ struct sp_server {
     std::map<int, Group> groups;  // key -> group
 
     static int key_of(const sp_ensemble_desc& d) {
-        return (((d.problem * 2 + d.anisotropy) * kSolverSlots + solver_slot(d.solver, d.jacobian)) * 2 + d.precision) * 2 +
+        return (((d.problem * kAnisoSlots + d.anisotropy) * kSolverSlots + solver_slot(d.solver, d.jacobian)) * 2 + d.precision) * 2 +
                (d.noise == SP_NOISE_INJECTED);
     }
 
@@ -266,7 +266,8 @@ void copy_desc_arrays(const sp_ensemble_desc& in, Request& r) {
     const int M = noise_dim(in.problem);
     const unsigned long long K = in.number_of_steps / in.oversampling;
     const size_t ndw = in.noise == SP_NOISE_INJECTED ? (K - 1) * in.oversampling * M * n : 0;
-    r.arrays.assign(n * (5 + (brown ? 2 : 0) + 6) + ndw, 0.0);
+    const bool uc = in.anisotropy == SP_ANISOTROPY_UNIAXIAL_CUBIC;
+    r.arrays.assign(n * (5 + (brown ? 2 : 0) + 6 + (uc ? 4 : 0)) + ndw, 0.0);
     double* p = r.arrays.data();
     auto put = [&](const double* src, size_t count) -> const double* {
         std::memcpy(p, src, count * 8);
@@ -290,6 +291,8 @@ void copy_desc_arrays(const sp_ensemble_desc& in, Request& r) {
     }
     q.orientation = put(in.particles.orientation, 3 * n);
     q.magnetisation = put(in.particles.magnetisation, 3 * n);
+    q.cubic_constant = uc ? put(in.particles.cubic_constant, n) : nullptr;
+    q.uniaxial_rotation = uc ? put(in.particles.uniaxial_rotation, 3 * n) : nullptr;
     r.desc.injected_dw = ndw ? put(in.injected_dw, ndw) : nullptr;
 }
 }  // namespace sp

@@ -24,7 +24,7 @@ constexpr int kFieldTile = 128;     // steps of B(t) each warp stages in shared 
 constexpr int kReduceThreads = 256; // threads per (sample, component) in the window reduction
 
 enum ProblemId : int { kNeel = 0, kNeelSpherical = 1, kBrownNeelEuler = 2, kBrownNeel = 3 };
-enum AnisoId : int { kUniaxial = 0, kCubic = 1 };
+enum AnisoId : int { kUniaxial = 0, kCubic = 1, kUniaxialCubic = 2 };
 enum SolverId : int { kEulerMaruyama = 0, kHeun = 1, kMillstein = 2, kImplicitMidpoint = 3, kEulerMaruyamaNormalized = 4 };
 // kernel-table slot of ImplicitMidpoint with the analytic Newton matrix (SP_JACOBIAN_EXACT)
 constexpr int kImplicitMidpointExact = 5;
@@ -34,6 +34,17 @@ constexpr int kParamsNeel = 16;
 constexpr int kParamsNeelSph = 15;
 constexpr int kParamsBrownNeelEuler = 13;
 constexpr int kParamsBrownNeel = 14;
+// extra parameters of the uniaxial+cubic anisotropy: Neel problems keep the cubic
+// field prefactor and the rotated uniaxial axis; the Euler problem adds the cubic
+// torque prefactor and the 3x3 rotation (its body axes move)
+constexpr int kParamsUniaxialCubicNeel = 4;
+constexpr int kParamsUniaxialCubicEuler = 11;
+__host__ __device__ constexpr int param_count_of(int problem, int aniso) {
+    return problem == kNeel            ? kParamsNeel + (aniso == kUniaxialCubic ? kParamsUniaxialCubicNeel : 0)
+           : problem == kNeelSpherical ? kParamsNeelSph + (aniso == kUniaxialCubic ? kParamsUniaxialCubicNeel : 0)
+           : problem == kBrownNeelEuler ? kParamsBrownNeelEuler + (aniso == kUniaxialCubic ? kParamsUniaxialCubicEuler : 0)
+                                        : kParamsBrownNeel;
+}
 
 struct FieldParams {
     int type;  // sp_field_type
@@ -105,6 +116,8 @@ struct RawParticles {
     const double* viscosity;
     const double* euler;  // [n][3]
     const double* mag;    // [n][3]
+    const double* K2;     // uniaxial+cubic: K_cubic
+    const double* urot;   // uniaxial+cubic: [n][3] Euler angles of the uniaxial axis
     double temperature;
     int simple_model;
 };

@@ -78,6 +78,8 @@ def spec_from_description(d: dict) -> EnsembleSpec:
         use_spherical_coordinate_transformation=bool(q["use_spherical_coordinate_transformation"]),
         neel_min_angle_before_transformation=float(q["neel_min_angle_before_transformation"]),
         use_simple_model=bool(q["use_simple_model"]),
+        cubic_constant=arr("cubic_constant") if "cubic_constant" in p else None,
+        uniaxial_rotation=arr("uniaxial_rotation").reshape(-1, 3) if "uniaxial_rotation" in p else None,
     )
 
 

@@ -210,6 +210,31 @@ def test_euler_maruyama_normalized_parity(ctx, problem):
         np.testing.assert_allclose(np.linalg.norm(fs, axis=2), 1.0, rtol=1e-14)
 
 
+UC_CASES = [(p, s) for p in (Problem.Neel, Problem.NeelSpherical, Problem.BrownAndNeelEulerSpherical)
+            for s in (Solver.EulerMaruyama, Solver.Heun_Strong)] + [(Problem.Neel, Solver.Implicit_Midpoint)]
+
+
+@pytest.mark.parametrize("problem,solver", UC_CASES, ids=[f"{p.name}-{s.name}" for p, s in UC_CASES])
+def test_uniaxial_cubic_parity(ctx, problem, solver):
+    """Uniaxial+cubic anisotropy (rotated uniaxial axis, K_u and K_c both set,
+    per-particle rotations) against the oracle on the same increments."""
+    base = small_spec(problem, solver)
+    rng = np.random.default_rng(8)
+    spec = dataclasses.replace(base, anisotropy=Anisotropy.UniaxialCubic, anisotropy_constant=np.full(base.n, -8e3),
+                               cubic_constant=np.full(base.n, -4e3),
+                               uniaxial_rotation=rng.uniform(0, 2 * math.pi, (base.n, 3)))
+    if solver == Solver.Implicit_Midpoint:
+        spec = dataclasses.replace(spec, max_iteration=20, accuracy_goal=1e-10)
+    spec = provider.with_injected_noise(spec, seed=3)
+    gpu = ctx.simulate(spec, trajectories=True)
+    ref = oracle.simulate(spec, trajectories=True)
+    rel, mabs = conditioned_bars(spec, ref)
+    compare(gpu, ref, rel=rel, mean_abs=mabs)
+    if solver == Solver.Implicit_Midpoint:
+        ex = dataclasses.replace(spec, jacobian=Jacobian.Exact)
+        compare(ctx.simulate(ex, trajectories=True), oracle.simulate(ex, trajectories=True), rel=rel, mean_abs=mabs)
+
+
 def test_runaway_particles_match(ctx):
     """Brown+Neel Cartesian with EulerMaruyama at dt = 1e-11: |m| is not renormalised in the
     reference's solver, so some particles diverge; the same particles diverge on both sides."""
