@@ -24,6 +24,8 @@ template <> struct M<double> {
     static __device__ __forceinline__ double fmod(double x, double y) { return ::fmod(x, y); }
     static __device__ __forceinline__ double sqrt(double x) { return ::sqrt(x); }
     static __device__ __forceinline__ double rcp(double x) { return 1.0 / x; }
+    // 1/sin of the spherical angles: exact division in FP64
+    static __device__ __forceinline__ double inv_sin(double x) { return 1.0 / x; }
     static __device__ __forceinline__ double abs(double x) { return ::fabs(x); }
     static __device__ __forceinline__ bool isinf(double x) { return ::isinf(x); }
     static __device__ __forceinline__ bool finite(double x) { return ::isfinite(x); }
@@ -40,6 +42,13 @@ template <> struct M<float> {
     static __device__ __forceinline__ float fmod(float x, float y) { return ::fmodf(x, y); }
     static __device__ __forceinline__ float sqrt(float x) { return ::sqrtf(x); }
     static __device__ __forceinline__ float rcp(float x) { return __frcp_rn(x); }
+    // 1/sin of the spherical angles in the FP32 form: the SFU reciprocal (rcp.approx,
+    // ~1 ulp) without the IEEE division's slow path; 1/0 stays +-inf
+    static __device__ __forceinline__ float inv_sin(float x) {
+        float r;
+        asm("rcp.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+        return r;
+    }
     static __device__ __forceinline__ float abs(float x) { return ::fabsf(x); }
     static __device__ __forceinline__ bool isinf(float x) { return ::isinf(x); }
     static __device__ __forceinline__ bool finite(float x) { return ::isfinite(x); }
@@ -115,11 +124,20 @@ __device__ __forceinline__ void box_muller(uint4 w, int npairs, double* z) {
         z[3] = r * s;
     }
 }
+// sqrt of -2 ln u as x * rsqrt(x) on the SFU (rsqrt.approx, ~1 ulp).  In FP32,
+// u = (w + 1/2) 2^-32 rounds to exactly 1 for the top 128 words, where -2 ln u is 0
+// (and rsqrt(0) = inf); x is kept at or above 1e-30, which gives a radius of 1e-15.
+__device__ __forceinline__ float sqrt_pos(float x) {
+    x = fmaxf(x, 1e-30f);
+    float r;
+    asm("rsqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return x * r;
+}
 __device__ __forceinline__ void box_muller(uint4 w, int npairs, float* z) {
     const float inv = 2.3283064e-10f, half = 1.1641532e-10f;
     {
         const float u0 = fmaf(__uint2float_rn(w.x), inv, half), u1 = fmaf(__uint2float_rn(w.y), inv, half);
-        const float r = ::sqrtf(-2.0f * __logf(u0));
+        const float r = sqrt_pos(-2.0f * __logf(u0));
         float s, c;
         __sincosf(6.2831853f * u1, &s, &c);
         z[0] = r * c;
@@ -127,7 +145,7 @@ __device__ __forceinline__ void box_muller(uint4 w, int npairs, float* z) {
     }
     if (npairs > 1) {
         const float u2 = fmaf(__uint2float_rn(w.z), inv, half), u3 = fmaf(__uint2float_rn(w.w), inv, half);
-        const float r = ::sqrtf(-2.0f * __logf(u2));
+        const float r = sqrt_pos(-2.0f * __logf(u2));
         float s, c;
         __sincosf(6.2831853f * u3, &s, &c);
         z[2] = r * c;

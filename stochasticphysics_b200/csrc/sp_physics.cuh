@@ -285,7 +285,7 @@ struct NeelSph {
         M<R>::sincos(y[0], &st, &ct);
         M<R>::sincos(y[1], &sp, &cp);
         c.st = st; c.ct = ct;
-        R odst = R(1) / st;
+        R odst = M<R>::inv_sin(st);
         if (M<R>::isinf(odst)) odst = R(0);
         c.odst = odst;
         if (!c.rot) {
@@ -447,10 +447,10 @@ struct BrownNeelEuler {
     static __device__ __forceinline__ void recompute(const Par&, const R* y, Cache& c) {
 #pragma unroll
         for (int i = 0; i < 5; ++i) M<R>::sincos(y[i], &c.S[i], &c.C[i]);
-        R csc = R(1) / c.S[1];
+        R csc = M<R>::inv_sin(c.S[1]);
         if (M<R>::isinf(csc)) csc = R(0);
         c.csc = csc;
-        R odst = R(1) / c.S[3];
+        R odst = M<R>::inv_sin(c.S[3]);
         if (M<R>::isinf(odst)) odst = R(0);
         c.odst = odst;
         const R ct = c.C[3], cp = c.C[4], st = c.S[3], sp = c.S[4];
