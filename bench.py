@@ -24,6 +24,8 @@ Heun) on the device-resident state, i.e. 2 x 65536 x 10000 particle-steps.
                FP64 as the serial baseline
   batched      256 Neel parameter sets (uneven N and S) submitted at once, batched
                per kernel key into shared launches (N=1)
+  stiff        the cubic ImplicitMidpoint workload (262144 particles, dt = 1e-10 s):
+               FP64 with the reference's Newton matrix, FP64 and FP32 with the exact one
   --impl reference  runs that CPU restatement as the reference arm
 
 Launch shapes come from the autotuner (sp_autotune) unless --no-autotune.
@@ -236,6 +238,42 @@ def batched_leg(ctx, count, step_scale, seed=0x5EED0004, serial_sample=32):
                         "alternating, FP32, W = 1000, dt = 1e-11 s"}
 
 
+def stiff_leg(ctx, torch, n=262144, timed_steps=2000):
+    """The stiff cubic workload (ImplicitMidpoint, Newton tolerance 1e-10, at most 20
+    iterations; 262144 Neel particles with cubic K1 = -1.1e4, dt = 1e-10 s) in three
+    forms: FP64 with the reference's Newton matrix (the drop-in), FP64 with the exact
+    Newton matrix, and the FP32 state with FP64 acceptance and the exact matrix.
+    Device-resident, CUDA-event timed after one warm-up chunk."""
+    from stochasticphysics_b200 import provider
+    from stochasticphysics_b200._abi import Jacobian, Precision
+
+    out = {}
+    st = torch.cuda.Stream()
+    for name, prec, jac in (("fp64_reference_jacobian", Precision.FP64, Jacobian.Reference),
+                            ("fp64_exact_jacobian", Precision.FP64, Jacobian.Exact),
+                            ("fp32_exact_jacobian", Precision.FP32, Jacobian.Exact)):
+        spec = dataclasses.replace(provider.cubic_implicit(n=n, steps=timed_steps + 2000, oversampling=1000),
+                                   precision=prec, jacobian=jac)
+        with ctx.ensemble(spec) as e:
+            e.advance(1000, st.cuda_stream)
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(st)
+            e.advance(timed_steps, st.cuda_stream)
+            b.record(st)
+            torch.cuda.synchronize()
+            r = e.read()
+        ms = a.elapsed_time(b)
+        ps = r.stats["particle_steps"]
+        out[name] = {"value": n * timed_steps / (ms / 1e3), "unit": UNIT,
+                     "newton_iterations_per_step": r.stats["newton_iterations"] / ps,
+                     "unconverged_fraction": r.stats["newton_unconverged"] / ps}
+    out["workload"] = (f"cubic_implicit: Neel, cubic K1 = -1.1e4 J/m^3, Haar axes, alpha = 0.05, r ~ 12 nm lognormal "
+                       f"(sigma 0.15), 12 mT at 25 kHz, dt = 1e-10 s, ImplicitMidpoint tol 1e-10 max 20; {n} "
+                       f"particles x {timed_steps} timed steps")
+    return out
+
+
 def cpu_baseline(steps_sample=2000, n=None):
     """The CPU oracle on all host cores for a bounded sample of the workload."""
     import oracle
@@ -346,6 +384,7 @@ def main():
     ap.add_argument("--serving-step-scale", type=float, default=0.006,
                     help="scale of the request step counts (S ~ logU[1e5, 1e7] x scale)")
     ap.add_argument("--batched-sets", type=int, default=256, help="parameter sets of the batched leg (0: skip)")
+    ap.add_argument("--no-stiff", action="store_true", help="skip the stiff ImplicitMidpoint leg")
     ap.add_argument("--batched-step-scale", type=float, default=0.02,
                     help="scale of the batched sets' step counts (S ~ logU[1e5, 1e7] x scale)")
     args = ap.parse_args()
@@ -442,6 +481,7 @@ def main():
             serving = serving_leg(ctx, args.serving_seconds, args.serving_rate, args.serving_step_scale)
         if world == 1 and args.batched_sets > 0:
             batched = batched_leg(ctx, args.batched_sets, args.batched_step_scale)
+        stiff = None if (world > 1 or args.no_stiff) else stiff_leg(ctx, torch)
 
     if rank == 0:
         tpp, tsrc = profiled_traffic_per_particle()
@@ -479,6 +519,7 @@ def main():
             "launch_shapes": shapes,
             "serving": serving,
             "batched": batched,
+            "stiff": stiff,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

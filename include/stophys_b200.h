@@ -34,7 +34,7 @@
 extern "C" {
 #endif
 
-#define SP_ABI_VERSION 4u
+#define SP_ABI_VERSION 5u
 
 #if defined(_WIN32)
 #define SP_API __declspec(dllexport)
@@ -179,6 +179,52 @@ typedef struct sp_problem_settings {
     double neel_min_angle_before_transformation;      /* rad                        */
 } sp_problem_settings;
 
+/* ---- device-side particle provider -------------------------------------
+ * Particle properties and initial states drawn on the device instead of being
+ * passed in: the reference's provider (Provider/ParticleProvider.h:194-217) selects a
+ * particle template per particle, its ParticleSimulationSettings
+ * (Settings/ParticleSimulationSettings.h:51-152, Properties/Anisotropy/Uniaxial.hpp:41-85)
+ * apply the size and anisotropy distributions, and the problem's initialiser draws
+ * random orientations and magnetisations (NeelRelaxation.h:226-283,
+ * BrownAndNeelRelaxation.inl:288-315, ParticleStateInitializer.h:50-123).  Draws come
+ * from Philox4x32-10 keyed by the provider's seed, so a provided ensemble is
+ * reproducible; the reference's generators are seeded from std::random_device. */
+typedef enum sp_distribution {
+    SP_DIST_DELTA = 0,
+    SP_DIST_NORMAL = 1,    /* N(mean, sigma)                                  */
+    SP_DIST_LOGNORMAL = 2  /* lognormal with the given mean and sigma          */
+} sp_distribution;
+
+typedef struct sp_dist {
+    int32_t type;     /* sp_distribution                                                    */
+    int32_t relative; /* 1: value * X, X from (1, width); 0: drawn around the value itself  */
+    double width;     /* relative sigma, or for radius/shell sigma/mean, for K the sigma    */
+} sp_dist;
+
+typedef struct sp_particle_template {
+    double weight;  /* Particle_Numbers entry: selection weight, or count when sequential */
+    double magnetic_radius, saturation_magnetisation, damping_constant, gyromagnetic_ratio;
+    double anisotropy_constant, hydrodynamic_radius, viscosity;
+    double cubic_constant;          /* uniaxial+cubic only                              */
+    double orientation[3];          /* Initial_particle_orientation (Euler ZXZ)         */
+    double magnetisation[3];        /* Initial_magnetisation_direction                  */
+    double uniaxial_rotation[3];    /* uniaxial+cubic only                              */
+    int32_t random_orientation;     /* Use_random_initial_particle_orientation          */
+    int32_t random_magnetisation;   /* Use_random_initial_particle_magnetisation        */
+    int32_t random_uniaxial_rotation; /* UseRandomCubicOrientation (uniaxial+cubic)     */
+    int32_t reserved;
+    sp_dist magnetic_radius_dist, hydrodynamic_shell_dist, anisotropy_dist, cubic_dist;
+} sp_particle_template;
+
+typedef struct sp_provider_desc {
+    uint64_t seed;        /* key of the provider's draws                                  */
+    int32_t n_templates;  /* 1..64                                                        */
+    int32_t sequential;   /* 1: fill each template's count in order, then template 0
+                             (Use_discrete_distribution_to_select_particle = false); 0: draw
+                             each particle's template with probability weight / sum      */
+    const sp_particle_template* templates;
+} sp_provider_desc;
+
 typedef struct sp_ensemble_desc {
     uint32_t abi_version; /* SP_ABI_VERSION */
     int32_t problem;      /* sp_problem     */
@@ -206,6 +252,9 @@ typedef struct sp_ensemble_desc {
      * layout [integrated_steps][noise_dim][n_particles] with
      * integrated_steps = (number_of_steps/oversampling - 1) * oversampling. */
     const double* injected_dw;
+    /* Optional: when set, `particles` is ignored and every particle is drawn on the
+     * device by this provider (particle i of the provider is particle_id_offset + i). */
+    const sp_provider_desc* provider;
 } sp_ensemble_desc;
 
 /* Outputs.  n_samples = number_of_steps / oversampling (SingleParticleSimulator.h:125);
@@ -336,6 +385,14 @@ SP_API sp_status sp_launch_config_for(sp_context* ctx, const sp_ensemble_desc* d
 SP_API sp_status sp_tuning_save(const char* path);
 SP_API sp_status sp_tuning_load(const char* path);
 SP_API sp_status sp_tuning_reset(void);
+
+/* ---- provider ------------------------------------------------------------
+ * The particles `desc->provider` draws for this description, copied to the host:
+ * out[n_particles][20] with columns magnetic_radius, saturation_magnetisation,
+ * damping_constant, gyromagnetic_ratio, anisotropy_constant, hydrodynamic_radius,
+ * viscosity, orientation[3], magnetisation[3] (unit), cubic_constant,
+ * uniaxial_rotation[3], template index, reserved. */
+SP_API sp_status sp_provide_particles(sp_context* ctx, const sp_ensemble_desc* desc, double* out);
 
 /* ---- allocation-free run ----------------------------------------------------
  * No counterpart in the reference: an addition for hosts whose plug-ins may not

@@ -51,6 +51,8 @@ def lib():
         L.oracle_eval_problem.restype = C.c_int
         L.oracle_eval_problem.argtypes = [C.c_int, C.c_int, _dp, _dp, _dp, _dp, _dp, C.c_double, _dp,
                                           _dp, _dp, _dp, _dp, _dp, _dp, _dp, C.POINTER(C.c_int), C.c_int]
+        L.oracle_provide_particles.restype = None
+        L.oracle_provide_particles.argtypes = [C.c_void_p, _dp]
         L.oracle_field_eval.restype = None
         L.oracle_field_eval.argtypes = [C.c_void_p, _dp, C.c_uint64, _dp]
         L.oracle_neel_exact_jacobians.restype = None
@@ -151,6 +153,14 @@ def eval_problem(problem: int, aniso: int, props, euler, settings, state, field=
     if rc != 0:
         raise RuntimeError(f"oracle_eval_problem failed ({rc})")
     out["rotated"] = (bool(rot[0]), bool(rot[1]))
+    return out
+
+
+def provide_particles(spec: EnsembleSpec) -> np.ndarray:
+    """The particles spec.provider draws: [n][20] as sp_provide_particles writes them."""
+    h = DescHolder(spec)
+    out = np.zeros((int(spec.n), 20))
+    lib().oracle_provide_particles(C.addressof(h.desc), _p(out))
     return out
 
 

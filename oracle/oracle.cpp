@@ -92,6 +92,122 @@ inline void philox_normals(uint64_t seed, uint64_t pid, uint64_t step, int m, do
     }
 }
 
+// ====================================================================== provider
+// Particles drawn by an sp_provider_desc, restated from the reference's provider and
+// initialisers (ParticleProvider.h:196-215, ParticleSimulationSettings.h:62-101,138-144,
+// Uniaxial.hpp:41-85, UniaxialCubic.hpp:52-75, NeelRelaxation.h:226-283,
+// BrownAndNeelRelaxation.inl:288-315, ParticleStateInitializer.h:50-123).  Draw k of
+// particle i is the Philox block with counter {k, 0x50524F56, i_lo, i_hi} and the
+// provider's seed as key: uniform (x + 1/2) 2^-32, normal sqrt(-2 ln u(x)) cos(2 pi u(y)).
+// Draws: 0 template, 1 K, 2 K_cubic, 3-5 rotation, 6 radius, 7 shell, 8-10 orientation,
+// 11-13 magnetisation.
+struct ProviderDraws {
+    uint64_t seed, i;
+    void block(uint32_t k, uint32_t* c) const {
+        c[0] = k; c[1] = 0x50524F56u; c[2] = static_cast<uint32_t>(i); c[3] = static_cast<uint32_t>(i >> 32);
+        philox4x32_10(c, static_cast<uint32_t>(seed), static_cast<uint32_t>(seed >> 32));
+    }
+    static double u01(uint32_t w) { return (w + 0.5) * 2.3283064365386963e-10; }
+    double uniform(uint32_t k) const { uint32_t c[4]; block(k, c); return u01(c[0]); }
+    double normal(uint32_t k) const {
+        uint32_t c[4];
+        block(k, c);
+        return std::sqrt(-2.0 * std::log(u01(c[0]))) * std::cos(kTwoPi * u01(c[1]));
+    }
+};
+inline double provider_sample(int type, double mean, double sigma, double z) {
+    if (type == SP_DIST_DELTA || !(sigma > 0.0)) return mean;
+    if (type == SP_DIST_NORMAL) return mean + sigma * z;
+    const double s2 = std::log1p((sigma * sigma) / (mean * mean));  // lognormal with this mean and sigma
+    return std::exp((std::log(mean) - 0.5 * s2) + std::sqrt(s2) * z);
+}
+inline double provider_apply(const sp_dist& d, double value, double z, bool sigma_times_mean) {
+    if (d.relative) return value * provider_sample(d.type, 1.0, d.width, z);
+    return provider_sample(d.type, value, sigma_times_mean ? value * d.width : d.width, z);
+}
+// o[20]: r Ms alpha gamma K rh eta euler[3] mag[3] K2 urot[3] template reserved[2]
+void provide_particle(const sp_provider_desc& pv, uint64_t i, int problem, int aniso, double* o) {
+    const ProviderDraws ds{pv.seed, i};
+    int t = 0;
+    if (pv.sequential) {
+        double cum = 0.0;
+        for (int k = 0; k < pv.n_templates; ++k) {
+            cum += pv.templates[k].weight;
+            if (static_cast<double>(i) < cum) { t = k; break; }
+        }
+    } else {
+        double total = 0.0;
+        for (int k = 0; k < pv.n_templates; ++k) total += pv.templates[k].weight;
+        const double u = ds.uniform(0) * total;
+        double cum = 0.0;
+        t = pv.n_templates - 1;
+        for (int k = 0; k < pv.n_templates; ++k) {
+            cum += pv.templates[k].weight;
+            if (u < cum) { t = k; break; }
+        }
+    }
+    const sp_particle_template& T = pv.templates[t];
+    const bool uc = aniso == SP_ANISOTROPY_UNIAXIAL_CUBIC;
+    o[4] = provider_apply(T.anisotropy_dist, T.anisotropy_constant, ds.normal(1), false);
+    o[13] = uc ? provider_apply(T.cubic_dist, T.cubic_constant, ds.normal(2), false) : 0.0;
+    for (int c = 0; c < 3; ++c) o[14 + c] = uc ? T.uniaxial_rotation[c] : 0.0;
+    if (uc && T.random_uniaxial_rotation) {
+        o[14] = ds.uniform(3) * kTwoPi; o[15] = ds.uniform(4) * kPi; o[16] = ds.uniform(5) * kTwoPi;
+    }
+    const double r = provider_apply(T.magnetic_radius_dist, T.magnetic_radius, ds.normal(6), true);
+    o[0] = r;
+    o[5] = provider_apply(T.hydrodynamic_shell_dist, T.hydrodynamic_radius - r, ds.normal(7), true) + r;
+    o[1] = T.saturation_magnetisation; o[2] = T.damping_constant; o[3] = T.gyromagnetic_ratio; o[6] = T.viscosity;
+    double* e = o + 7;
+    for (int c = 0; c < 3; ++c) e[c] = T.orientation[c];
+    if (T.random_orientation) {
+        if (problem == SP_PROBLEM_NEEL) {
+            for (int c = 0; c < 3; ++c) e[c] = ds.uniform(8 + c) * kTwoPi;
+        } else if (problem == SP_PROBLEM_BROWN_AND_NEEL) {
+            double d[3] = {ds.normal(8), ds.normal(9), ds.normal(10)};
+            const double nd = std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+            for (double& c : d) c /= nd;
+            e[0] = std::acos(std::min(1.0, std::max(-1.0, d[0]))); e[1] = std::atan2(d[2], -d[1]); e[2] = 0.0;
+        } else {
+            e[0] = ds.uniform(8) * kTwoPi; e[1] = ds.uniform(9) * kPi; e[2] = ds.uniform(10) * kTwoPi;
+        }
+    }
+    double* m = o + 10;
+    for (int c = 0; c < 3; ++c) m[c] = T.magnetisation[c];
+    if (T.random_magnetisation) {
+        if (problem == SP_PROBLEM_NEEL || problem == SP_PROBLEM_BROWN_AND_NEEL) {
+            for (int c = 0; c < 3; ++c) m[c] = ds.normal(11 + c);
+        } else {
+            const double ph = ds.uniform(11) * kTwoPi, th = ds.uniform(12) * kPi;
+            m[0] = std::cos(ph) * std::sin(th); m[1] = std::sin(ph) * std::sin(th); m[2] = std::cos(th);
+        }
+    }
+    const double nm = std::sqrt(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]);
+    if (nm > 0.0) for (int c = 0; c < 3; ++c) m[c] /= nm;
+    o[17] = t; o[18] = 0.0; o[19] = 0.0;
+}
+
+// Host arrays of a provided ensemble, kept alive beside a description that points at them
+struct ProvidedArrays {
+    std::vector<double> r, Ms, alpha, gamma, K, rh, eta, euler, mag, K2, urot;
+    sp_ensemble_desc desc;
+    explicit ProvidedArrays(const sp_ensemble_desc& d) : desc(d) {
+        const uint64_t n = d.n_particles;
+        for (auto* v : {&r, &Ms, &alpha, &gamma, &K, &rh, &eta, &K2}) v->resize(n);
+        euler.resize(3 * n); mag.resize(3 * n); urot.resize(3 * n);
+        double o[20];
+        for (uint64_t p = 0; p < n; ++p) {
+            provide_particle(*d.provider, d.particle_id_offset + p, d.problem, d.anisotropy, o);
+            r[p] = o[0]; Ms[p] = o[1]; alpha[p] = o[2]; gamma[p] = o[3]; K[p] = o[4]; rh[p] = o[5]; eta[p] = o[6];
+            K2[p] = o[13];
+            for (int c = 0; c < 3; ++c) { euler[3 * p + c] = o[7 + c]; mag[3 * p + c] = o[10 + c]; urot[3 * p + c] = o[14 + c]; }
+        }
+        desc.particles = sp_particles{r.data(), Ms.data(), alpha.data(), gamma.data(), K.data(), rh.data(), eta.data(),
+                                      euler.data(), mag.data(), K2.data(), urot.data()};
+        desc.provider = nullptr;
+    }
+};
+
 // ====================================================================== fields
 // Fields/SinusoidalField.h:47-51, Fields/LissajousField.h:98-101, ConstantField.h:43, ZeroField.h:39
 // Fields/TriangularField.h:52-70, Fields/RectangularField.h:30-63, Fields/SincField.h:32-48
@@ -499,14 +615,17 @@ using namespace orc;
 
 extern "C" {
 
-int oracle_abi_version(void) { return 3; }
+int oracle_abi_version(void) { return 5; }
 
 // Runs the ensemble described by desc.  mean[K][OUT], weight[OUT], time[K],
 // field[K][3], traj[N][K][OUT] and final_state[N][D] are optional (NULL).
 // precision_mode: 0 = double, 1 = long double.  Returns 0 on success.
-int oracle_simulate(const sp_ensemble_desc* d, double* mean, double* weight, double* time, double* field,
+int oracle_simulate(const sp_ensemble_desc* d_in, double* mean, double* weight, double* time, double* field,
                     double* traj, double* final_state, uint64_t* newton_stats, int nthreads, int precision_mode) {
-    if (!d || d->oversampling == 0 || d->number_of_steps < d->oversampling) return 1;
+    if (!d_in || d_in->oversampling == 0 || d_in->number_of_steps < d_in->oversampling) return 1;
+    std::unique_ptr<ProvidedArrays> provided;
+    if (d_in->provider) provided = std::make_unique<ProvidedArrays>(*d_in);
+    const sp_ensemble_desc* d = provided ? &provided->desc : d_in;
     if (d->solver == SP_SOLVER_IMPLICIT_MIDPOINT && d->problem == SP_PROBLEM_BROWN_AND_NEEL_EULER_SPHERICAL) return 2;
     if (d->solver == SP_SOLVER_IMPLICIT_MIDPOINT && d->jacobian == SP_JACOBIAN_EXACT && d->problem != SP_PROBLEM_NEEL)
         return 3;
@@ -583,6 +702,12 @@ void oracle_philox_normals(uint64_t seed, uint64_t pid0, uint64_t n, uint64_t st
             philox_normals(seed, pid0 + p, step0 + s, m, z);
             for (int j = 0; j < m; ++j) out[(s * m + j) * n + p] = z[j];
         }
+}
+
+// The particles of a provider: out[n][20] as sp_provide_particles writes them.
+void oracle_provide_particles(const sp_ensemble_desc* d, double* out) {
+    for (uint64_t p = 0; p < d->n_particles; ++p)
+        provide_particle(*d->provider, d->particle_id_offset + p, d->problem, d->anisotropy, out + 20 * p);
 }
 
 // Raw Philox4x32-10 block for a given counter/key (known-answer tests).

@@ -6,11 +6,12 @@ anisotropy; zero, constant, sinusoidal and Lissajous fields; EulerMaruyama,
 Heun, Millstein and ImplicitMidpoint steppers) behind the C ABI in
 include/stophys_b200.h.
 """
-from ._abi import (Anisotropy, EnsembleSpec, FieldSpec, FieldType, Jacobian, Noise, Precision,  # noqa: F401
+from ._abi import (Anisotropy, DistSpec, Distribution, EnsembleSpec, FieldSpec, FieldType, Jacobian,  # noqa: F401
+                   Noise, ParticleTemplateSpec, Precision, ProviderSpec,
                    Problem, RequestState, Solver, Status, DIMS)
 from .lib import SPError, load  # noqa: F401
 from .simulator import Context, DeviceEnsemble, Server, SimulationResult, kernel_launch_count  # noqa: F401
 
-__all__ = ["Anisotropy", "EnsembleSpec", "FieldSpec", "FieldType", "Jacobian", "Noise", "Precision", "Problem", "RequestState",
+__all__ = ["Anisotropy", "DistSpec", "Distribution", "ParticleTemplateSpec", "ProviderSpec", "EnsembleSpec", "FieldSpec", "FieldType", "Jacobian", "Noise", "Precision", "Problem", "RequestState",
            "Solver", "Status", "DIMS", "SPError", "load", "Context", "DeviceEnsemble", "Server", "SimulationResult",
            "kernel_launch_count"]

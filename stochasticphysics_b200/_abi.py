@@ -13,7 +13,7 @@ from typing import Optional
 
 import numpy as np
 
-ABI_VERSION = 4
+ABI_VERSION = 5
 
 
 class Status(IntEnum):
@@ -139,6 +139,30 @@ class sp_problem_settings(C.Structure):
     ]
 
 
+class sp_dist(C.Structure):
+    _fields_ = [("type", C.c_int32), ("relative", C.c_int32), ("width", C.c_double)]
+
+
+class sp_particle_template(C.Structure):
+    _fields_ = [
+        ("weight", C.c_double),
+        ("magnetic_radius", C.c_double), ("saturation_magnetisation", C.c_double),
+        ("damping_constant", C.c_double), ("gyromagnetic_ratio", C.c_double),
+        ("anisotropy_constant", C.c_double), ("hydrodynamic_radius", C.c_double), ("viscosity", C.c_double),
+        ("cubic_constant", C.c_double),
+        ("orientation", C.c_double * 3), ("magnetisation", C.c_double * 3), ("uniaxial_rotation", C.c_double * 3),
+        ("random_orientation", C.c_int32), ("random_magnetisation", C.c_int32),
+        ("random_uniaxial_rotation", C.c_int32), ("reserved", C.c_int32),
+        ("magnetic_radius_dist", sp_dist), ("hydrodynamic_shell_dist", sp_dist),
+        ("anisotropy_dist", sp_dist), ("cubic_dist", sp_dist),
+    ]
+
+
+class sp_provider_desc(C.Structure):
+    _fields_ = [("seed", C.c_uint64), ("n_templates", C.c_int32), ("sequential", C.c_int32),
+                ("templates", C.POINTER(sp_particle_template))]
+
+
 class sp_ensemble_desc(C.Structure):
     _fields_ = [
         ("abi_version", C.c_uint32),
@@ -163,6 +187,7 @@ class sp_ensemble_desc(C.Structure):
         ("seed", C.c_uint64),
         ("particle_id_offset", C.c_uint64),
         ("injected_dw", _dp),
+        ("provider", C.POINTER(sp_provider_desc)),
     ]
 
 
@@ -278,6 +303,70 @@ class FieldSpec:
         return f
 
 
+class Distribution(IntEnum):
+    Delta = 0
+    Normal = 1
+    Lognormal = 2
+
+
+@dataclass
+class DistSpec:
+    """One size or anisotropy distribution (ParticleSimulationSettings.h:62-101)."""
+    type: Distribution = Distribution.Delta
+    width: float = 0.0
+    relative: bool = True
+
+    def to_c(self) -> sp_dist:
+        return sp_dist(int(self.type), int(bool(self.relative)), float(self.width))
+
+
+@dataclass
+class ParticleTemplateSpec:
+    """One particle template of the device-side provider (a Particle_List entry)."""
+    magnetic_radius: float
+    saturation_magnetisation: float
+    damping_constant: float
+    gyromagnetic_ratio: float
+    anisotropy_constant: float
+    weight: float = 1.0
+    hydrodynamic_radius: float = 0.0
+    viscosity: float = 0.0
+    cubic_constant: float = 0.0
+    orientation: tuple = (0.0, 0.0, 0.0)
+    magnetisation: tuple = (0.0, 0.0, 1.0)
+    uniaxial_rotation: tuple = (0.0, 0.0, 0.0)
+    random_orientation: bool = False
+    random_magnetisation: bool = False
+    random_uniaxial_rotation: bool = False
+    magnetic_radius_dist: DistSpec = field(default_factory=DistSpec)
+    hydrodynamic_shell_dist: DistSpec = field(default_factory=DistSpec)
+    anisotropy_dist: DistSpec = field(default_factory=DistSpec)
+    cubic_dist: DistSpec = field(default_factory=DistSpec)
+
+    def to_c(self) -> sp_particle_template:
+        t = sp_particle_template()
+        for k in ("weight", "magnetic_radius", "saturation_magnetisation", "damping_constant", "gyromagnetic_ratio",
+                  "anisotropy_constant", "hydrodynamic_radius", "viscosity", "cubic_constant"):
+            setattr(t, k, float(getattr(self, k)))
+        for k in ("orientation", "magnetisation", "uniaxial_rotation"):
+            v = getattr(self, k)
+            for i in range(3):
+                getattr(t, k)[i] = float(v[i])
+        for k in ("random_orientation", "random_magnetisation", "random_uniaxial_rotation"):
+            setattr(t, k, int(bool(getattr(self, k))))
+        for k in ("magnetic_radius_dist", "hydrodynamic_shell_dist", "anisotropy_dist", "cubic_dist"):
+            setattr(t, k, getattr(self, k).to_c())
+        return t
+
+
+@dataclass
+class ProviderSpec:
+    """Device-side provider: particles drawn on the GPU from these templates."""
+    templates: list
+    seed: int = 0
+    sequential: bool = False
+
+
 @dataclass
 class EnsembleSpec:
     """Everything one ensemble simulation needs; mirrors sp_ensemble_desc.
@@ -322,6 +411,7 @@ class EnsembleSpec:
     jacobian: Jacobian = Jacobian.Reference
     cubic_constant: Optional[np.ndarray] = None      # UniaxialCubic: K_cubic (n)
     uniaxial_rotation: Optional[np.ndarray] = None   # UniaxialCubic: Euler angles of the uniaxial axis (n, 3)
+    provider: Optional[ProviderSpec] = None          # particles drawn on the device (arrays unused)
 
     @property
     def dims(self):
@@ -358,16 +448,17 @@ class DescHolder:
 
     def __init__(self, spec: EnsembleSpec):
         n = int(spec.n)
+        opt = lambda v, **kw: None if v is None else _f64(v, **kw)  # noqa: E731
         self.arrays = {
-            "magnetic_radius": _f64(spec.magnetic_radius, n),
-            "saturation_magnetisation": _f64(spec.saturation_magnetisation, n),
-            "damping_constant": _f64(spec.damping_constant, n),
-            "gyromagnetic_ratio": _f64(spec.gyromagnetic_ratio, n),
-            "anisotropy_constant": _f64(spec.anisotropy_constant, n),
-            "hydrodynamic_radius": None if spec.hydrodynamic_radius is None else _f64(spec.hydrodynamic_radius, n),
-            "viscosity": None if spec.viscosity is None else _f64(spec.viscosity, n),
-            "orientation": _f64(spec.orientation, shape=(n, 3)),
-            "magnetisation": _f64(spec.magnetisation, shape=(n, 3)),
+            "magnetic_radius": opt(spec.magnetic_radius, n=n),
+            "saturation_magnetisation": opt(spec.saturation_magnetisation, n=n),
+            "damping_constant": opt(spec.damping_constant, n=n),
+            "gyromagnetic_ratio": opt(spec.gyromagnetic_ratio, n=n),
+            "anisotropy_constant": opt(spec.anisotropy_constant, n=n),
+            "hydrodynamic_radius": opt(spec.hydrodynamic_radius, n=n),
+            "viscosity": opt(spec.viscosity, n=n),
+            "orientation": opt(spec.orientation, shape=(n, 3)),
+            "magnetisation": opt(spec.magnetisation, shape=(n, 3)),
             "cubic_constant": None if spec.cubic_constant is None else _f64(spec.cubic_constant, n),
             "uniaxial_rotation": None if spec.uniaxial_rotation is None else _f64(spec.uniaxial_rotation, shape=(n, 3)),
         }
@@ -403,6 +494,13 @@ class DescHolder:
         d.seed = int(spec.seed) & 0xFFFFFFFFFFFFFFFF
         d.particle_id_offset = int(spec.particle_id_offset)
         d.injected_dw = _ptr(self.dw)
+        self.provider = self.templates = None
+        if spec.provider is not None:
+            pv = spec.provider
+            self.templates = (sp_particle_template * len(pv.templates))(*[t.to_c() for t in pv.templates])
+            self.provider = sp_provider_desc(int(pv.seed) & 0xFFFFFFFFFFFFFFFF, len(pv.templates), int(bool(pv.sequential)),
+                                             C.cast(self.templates, C.POINTER(sp_particle_template)))
+            d.provider = C.pointer(self.provider)
         self.desc = d
         self.spec = spec
 

@@ -81,6 +81,7 @@ extern "C" SP_API sp_status sp_simulate_noalloc(const sp_ensemble_desc* desc, co
         if (desc->noise == SP_NOISE_INJECTED)
             return fail(SP_ERR_INVALID_ARG, "sp_simulate_noalloc draws its noise in-kernel (SP_NOISE_PHILOX only)");
         if (desc->record_trajectories) return fail(SP_ERR_INVALID_ARG, "sp_simulate_noalloc keeps no trajectories");
+        if (desc->provider) return fail(SP_ERR_INVALID_ARG, "sp_simulate_noalloc takes its particles from device_particles");
         const sp_particles& dp = *device_particles;
         const bool brown = desc->problem == SP_PROBLEM_BROWN_AND_NEEL || desc->problem == SP_PROBLEM_BROWN_AND_NEEL_EULER_SPHERICAL;
         if (!dp.magnetic_radius || !dp.saturation_magnetisation || !dp.damping_constant || !dp.gyromagnetic_ratio ||

@@ -63,15 +63,31 @@ sp_status validate_desc(const sp_ensemble_desc* d, std::string& why) {
     if (!(d->timestep > 0.0) || !std::isfinite(d->timestep)) return bad("timestep must be finite and > 0");
     if (!(d->temperature >= 0.0) || !std::isfinite(d->temperature)) return bad("temperature must be finite and >= 0");
     const sp_particles& q = d->particles;
-    if (!q.magnetic_radius || !q.saturation_magnetisation || !q.damping_constant || !q.gyromagnetic_ratio ||
-        !q.anisotropy_constant || !q.orientation || !q.magnetisation)
-        return bad("a required per-particle array is NULL");
-    if ((d->problem == SP_PROBLEM_BROWN_AND_NEEL || d->problem == SP_PROBLEM_BROWN_AND_NEEL_EULER_SPHERICAL) &&
-        (!q.hydrodynamic_radius || !q.viscosity))
-        return bad("Brown problems need hydrodynamic_radius and viscosity");
+    if (d->provider) {
+        const sp_provider_desc& pv = *d->provider;
+        if (pv.n_templates < 1 || pv.n_templates > 64 || !pv.templates) return bad("provider needs 1..64 templates");
+        double total = 0.0;
+        for (int k = 0; k < pv.n_templates; ++k) {
+            const sp_particle_template& t = pv.templates[k];
+            if (!(t.weight >= 0.0) || !std::isfinite(t.weight)) return bad("provider template weights must be finite and >= 0");
+            total += t.weight;
+            if (!(t.magnetic_radius > 0.0) || !(t.saturation_magnetisation > 0.0)) return bad("provider template needs radius and Ms > 0");
+            for (const sp_dist* ds : {&t.magnetic_radius_dist, &t.hydrodynamic_shell_dist, &t.anisotropy_dist, &t.cubic_dist})
+                if (ds->type < SP_DIST_DELTA || ds->type > SP_DIST_LOGNORMAL || !(ds->width >= 0.0))
+                    return bad("provider template distribution: unknown type or negative width");
+        }
+        if (!pv.sequential && !(total > 0.0)) return bad("provider template weights must not all be zero");
+    } else {
+        if (!q.magnetic_radius || !q.saturation_magnetisation || !q.damping_constant || !q.gyromagnetic_ratio ||
+            !q.anisotropy_constant || !q.orientation || !q.magnetisation)
+            return bad("a required per-particle array is NULL");
+        if ((d->problem == SP_PROBLEM_BROWN_AND_NEEL || d->problem == SP_PROBLEM_BROWN_AND_NEEL_EULER_SPHERICAL) &&
+            (!q.hydrodynamic_radius || !q.viscosity))
+            return bad("Brown problems need hydrodynamic_radius and viscosity");
+    }
     if (d->noise == SP_NOISE_INJECTED && !d->injected_dw) return bad("injected noise mode needs injected_dw");
     if (d->anisotropy == SP_ANISOTROPY_UNIAXIAL_CUBIC) {
-        if (!q.cubic_constant || !q.uniaxial_rotation)
+        if (!d->provider && (!q.cubic_constant || !q.uniaxial_rotation))
             return bad("uniaxial+cubic anisotropy needs cubic_constant and uniaxial_rotation");
         if (d->problem == SP_PROBLEM_BROWN_AND_NEEL) {
             why = "uniaxial+cubic anisotropy is not defined for the coupled Cartesian problem (the reference's cubic "
@@ -280,6 +296,20 @@ FieldParams field_params(const sp_field_desc& f) {
 
 void Ensemble::upload_and_init(const sp_ensemble_desc& d) {
     const size_t n = L.n;
+    if (d.provider) {  // particles drawn on the device: nothing to upload
+        double* dev = provide_particles(ctx, d, stream);
+        RawParticles rp = provided_raw(dev, n);
+        rp.temperature = d.temperature;
+        rp.simple_model = d.problem_settings.use_simple_model;
+        ks->init(d_ens, rp, L.Np, stream);
+        ks->reduce(d_ens, 1, 2, 1, stream);
+        launch_field_window(hdev.field, d.timestep, L.W, L.K, d_field, stream);
+        check_cuda(cudaGetLastError(), "init kernels");
+        launches += 4;
+        g_launch_count += 3;
+        check_cuda(cudaFreeAsync(dev, stream), "cudaFreeAsync");
+        return;
+    }
     const sp_particles& q = d.particles;
     const bool brown = d.problem == SP_PROBLEM_BROWN_AND_NEEL || d.problem == SP_PROBLEM_BROWN_AND_NEEL_EULER_SPHERICAL;
     // one staging buffer: 7 scalars + 6 vector components per particle (+ K_cubic and the

@@ -62,6 +62,11 @@ struct EnsembleLayout {
 };
 EnsembleLayout layout_of(const sp_ensemble_desc& d, const LaunchConfig& lc);
 
+// device-side provider (sp_provider.cu): draws the particles of d into a pooled
+// [18][n] buffer on stream s (the caller frees it); provided_raw views it
+double* provide_particles(sp_context* ctx, const sp_ensemble_desc& d, cudaStream_t s);
+RawParticles provided_raw(const double* dev, unsigned long long n);
+
 // One device-resident ensemble (one reference "simulation" of n particles).
 struct Ensemble {
     sp_context* ctx;

@@ -38,6 +38,8 @@ struct Request {
     uint64_t id = 0;
     sp_ensemble_desc desc{};
     std::vector<double> arrays;  // deep copy of every per-particle array and injected dW
+    sp_provider_desc provider{};  // deep copy of a device-side provider, if any
+    std::vector<sp_particle_template> templates;
     std::unique_ptr<Ensemble> ens;
     int state = SP_REQUEST_QUEUED;
     bool cancel = false;
@@ -267,6 +269,16 @@ void copy_desc_arrays(const sp_ensemble_desc& in, Request& r) {
     const unsigned long long K = in.number_of_steps / in.oversampling;
     const size_t ndw = in.noise == SP_NOISE_INJECTED ? (K - 1) * in.oversampling * M * n : 0;
     const bool uc = in.anisotropy == SP_ANISOTROPY_UNIAXIAL_CUBIC;
+    if (in.provider) {  // particles are drawn on the device: no arrays to keep
+        r.desc = in;
+        r.desc.particles = sp_particles{};
+        r.desc.injected_dw = nullptr;
+        r.provider = *in.provider;
+        r.templates.assign(in.provider->templates, in.provider->templates + in.provider->n_templates);
+        r.provider.templates = r.templates.data();
+        r.desc.provider = &r.provider;
+        return;
+    }
     r.arrays.assign(n * (5 + (brown ? 2 : 0) + 6 + (uc ? 4 : 0)) + ndw, 0.0);
     double* p = r.arrays.data();
     auto put = [&](const double* src, size_t count) -> const double* {

@@ -124,6 +124,16 @@ class Context:
     def tuning_reset() -> None:
         check(load().sp_tuning_reset())
 
+    def provide_particles(self, spec: EnsembleSpec) -> np.ndarray:
+        """The particles spec.provider draws on the device: [n][20] columns magnetic_radius,
+        saturation_magnetisation, damping_constant, gyromagnetic_ratio, anisotropy_constant,
+        hydrodynamic_radius, viscosity, orientation[3], magnetisation[3], cubic_constant,
+        uniaxial_rotation[3], template index, reserved[2]."""
+        out = np.zeros((int(spec.n), 20))
+        check(self._lib.sp_provide_particles(self.handle, DescHolder(spec).byref(),
+                                             out.ctypes.data_as(C.POINTER(C.c_double))))
+        return out
+
     @staticmethod
     def footprint(spec: EnsembleSpec) -> int:
         h = DescHolder(spec)

@@ -36,7 +36,8 @@ def test_library_exports_every_declared_symbol():
 
 def test_abi_version_and_dims():
     lib = load()
-    assert lib.sp_abi_version() == _abi.ABI_VERSION == 4
+    header_version = int(re.search(r"#define SP_ABI_VERSION (\d+)u", HEADER.read_text()).group(1))
+    assert lib.sp_abi_version() == _abi.ABI_VERSION == header_version
     for prob, dims in _abi.DIMS.items():
         a, b, c = C.c_int32(), C.c_int32(), C.c_int32()
         assert lib.sp_query_dims(int(prob), C.byref(a), C.byref(b), C.byref(c)) == 0
