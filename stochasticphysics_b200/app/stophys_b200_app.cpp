@@ -14,10 +14,12 @@
 // (Anisotropy_1, Anisotropy_constants_distribution_*).
 //
 // Usage: stophys_b200 -parfile:<ini> [-sysmatrix:<ini>] [-out:<json>] [-device:N]
-//                     [-seed:S] [-precision:fp64|fp32] [-print]
+//                     [-seed:S] [-precision:fp64|fp32] [-device-provider] [-print]
 //   -print parses the files, runs the provider and validates the description
 //   without touching a GPU; it writes the description and every particle (with
 //   -sysmatrix: the voxels and their offset fields).
+//   -device-provider draws the particles on the GPU from the same templates
+//   (sp_provider_desc) instead of passing the host-drawn arrays.
 //   -sysmatrix runs the system-matrix sweep of the reference
 //   (Settings/SystemMatrixSettings.h, Settings/SystemMatrix_SimulationManagerSettings_Factory.h,
 //   Simulator/SimulationApplication.cpp:80-128): one ensemble per voxel with the
@@ -337,7 +339,48 @@ struct Run {
     std::vector<ParticleTemplate> templates;
     std::vector<uint64_t> used;
     std::string savefile;
+    bool discrete = false;
+    // -device-provider: the templates as an sp_provider_desc (particles drawn on the GPU)
+    std::vector<sp_particle_template> dev_templates;
+    sp_provider_desc provider{};
 };
+
+sp_dist to_sp_dist(const Dist& d) {
+    sp_dist o{};
+    o.type = d.type == "normal" ? SP_DIST_NORMAL : d.type == "lognormal" ? SP_DIST_LOGNORMAL : SP_DIST_DELTA;
+    if (d.type != "normal" && d.type != "lognormal" && d.type != "delta")
+        throw std::runtime_error("unsupported distribution type '" + d.type + "'");
+    o.relative = d.relative ? 1 : 0;
+    o.width = d.width;
+    return o;
+}
+
+// Hands particle drawing to the device: one sp_particle_template per Particle_List entry
+void use_device_provider(Run& run, unsigned long long seed) {
+    run.dev_templates.clear();
+    for (const auto& t : run.templates) {
+        sp_particle_template o{};
+        o.weight = t.count;
+        o.magnetic_radius = t.r; o.saturation_magnetisation = t.Ms; o.damping_constant = t.alpha;
+        o.gyromagnetic_ratio = t.gamma; o.anisotropy_constant = t.K; o.hydrodynamic_radius = t.rh; o.viscosity = t.eta;
+        o.cubic_constant = t.K2;
+        for (int c = 0; c < 3; ++c) {
+            o.orientation[c] = t.orientation[c]; o.magnetisation[c] = t.magnetisation[c]; o.uniaxial_rotation[c] = t.urot[c];
+        }
+        o.random_orientation = t.random_orientation; o.random_magnetisation = t.random_magnetisation;
+        o.random_uniaxial_rotation = t.random_urot;
+        o.magnetic_radius_dist = to_sp_dist(t.r_dist);
+        o.hydrodynamic_shell_dist = to_sp_dist(t.shell_dist);
+        o.anisotropy_dist = to_sp_dist(t.K_dist);
+        o.cubic_dist = to_sp_dist(t.K2_dist);
+        run.dev_templates.push_back(o);
+    }
+    run.provider.seed = seed ^ 0xD1B54A32D192ED03ull;
+    run.provider.n_templates = static_cast<int32_t>(run.dev_templates.size());
+    run.provider.sequential = run.discrete ? 0 : 1;
+    run.provider.templates = run.dev_templates.data();
+    run.d.provider = &run.provider;
+}
 
 Run build(const std::string& path, unsigned long long seed, int precision) {
     const Ini ini = Ini::load(path);
@@ -412,6 +455,7 @@ Run build(const std::string& path, unsigned long long seed, int precision) {
     // Particle_Provider (ParticleProvider.h:243-292)
     bool discrete = false;
     if (auto v = opt("Particle_Provider", "Use_discrete_distribution_to_select_particle")) discrete = Ini::boolean(*v);
+    run.discrete = discrete;
     const Ini::Section* list = ini.section("Particle_Provider.Particle_List");
     if (!list || list->empty()) throw std::runtime_error("no [Particle_Provider.Particle_List]");
     for (const auto& kv : *list) {
@@ -794,7 +838,7 @@ int main(int argc, char** argv) {
     std::string par, out, sysmatrix;
     int device = 0, precision = SP_PRECISION_FP64;
     unsigned long long seed = 0x5EED;
-    bool print_only = false;
+    bool print_only = false, device_provider = false;
     for (int i = 1; i < argc; ++i) {
         const std::string a = argv[i];
         auto val = [&](const char* p) { return a.substr(std::string(p).size()); };
@@ -806,6 +850,7 @@ int main(int argc, char** argv) {
         else if (a == "-precision:fp32") precision = SP_PRECISION_FP32;
         else if (a == "-precision:fp64") precision = SP_PRECISION_FP64;
         else if (a == "-print") print_only = true;
+        else if (a == "-device-provider") device_provider = true;
         else {
             std::fprintf(stderr, "unknown argument %s\n", a.c_str());
             return 2;
@@ -813,11 +858,12 @@ int main(int argc, char** argv) {
     }
     if (par.empty()) {
         std::fprintf(stderr, "usage: stophys_b200 -parfile:<ini> [-sysmatrix:<ini>] [-out:<json>] [-device:N] "
-                             "[-seed:S] [-precision:fp64|fp32] [-print]\n");
+                             "[-seed:S] [-precision:fp64|fp32] [-device-provider] [-print]\n");
         return 2;
     }
     try {
-        const Run run = build(par, seed, precision);
+        Run run = build(par, seed, precision);
+        if (device_provider && !print_only) use_device_provider(run, seed);
         const sp_ensemble_desc& d = run.d;
         if (sp_validate(&d) != SP_OK) throw std::runtime_error(sp_last_error());
         std::ofstream fo;
@@ -840,6 +886,19 @@ int main(int argc, char** argv) {
         sp_context* ctx = nullptr;
         if (sp_create(&ctx, device) != SP_OK) throw std::runtime_error(sp_last_error());
         const sp_status s = sp_simulate(ctx, &d, &res, &st);
+        if (s == SP_OK && d.provider) {  // Mean_Properties of the particles the device drew
+            std::vector<double> p(20 * d.n_particles);
+            if (sp_provide_particles(ctx, &d, p.data()) != SP_OK) {
+                sp_destroy(ctx);
+                throw std::runtime_error(sp_last_error());
+            }
+            for (auto* v : {&run.r, &run.Ms, &run.alpha, &run.gamma, &run.K, &run.rh, &run.eta}) v->assign(d.n_particles, 0.0);
+            for (size_t i = 0; i < d.n_particles; ++i) {
+                const double* o = p.data() + 20 * i;
+                run.r[i] = o[0]; run.Ms[i] = o[1]; run.alpha[i] = o[2]; run.gamma[i] = o[3]; run.K[i] = o[4];
+                run.rh[i] = o[5]; run.eta[i] = o[6];
+            }
+        }
         sp_destroy(ctx);
         if (s != SP_OK) throw std::runtime_error(sp_last_error());
         os << "{\"Mean_Results\":";

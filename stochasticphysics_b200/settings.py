@@ -95,12 +95,14 @@ def load_ini(path, seed: int = 0x5EED, precision: Precision = Precision.FP64) ->
 
 
 def run_ini(path, seed: int = 0x5EED, precision: Precision = Precision.FP64, device: int = 0,
-            timeout: float = 3600.0, sysmatrix=None) -> dict:
+            timeout: float = 3600.0, sysmatrix=None, device_provider: bool = False) -> dict:
     """Runs the .ini on `device` through the driver; returns its JSON record.  With
     `sysmatrix` (a System_Matrix_Settings .ini) it runs the voxel sweep: one
     ensemble per voxel, offset field moved to the voxel's field, Philox key
     seed + voxel number, all batched through the server."""
     extra = [f"-sysmatrix:{sysmatrix}"] if sysmatrix else []
+    if device_provider:  # particles drawn on the GPU from the same templates
+        extra.append("-device-provider")
     return json.loads(_call(_flags(path, seed, precision) + extra + [f"-device:{int(device)}"], timeout))
 
 

@@ -69,3 +69,21 @@ def test_system_matrix_sweep_equals_per_voxel_runs(tmp_path):
             alone = ctx.simulate(spec)
             np.testing.assert_array_equal(np.array(v["Mean_Results"]["Results"], dtype=float), alone.mean)
             np.testing.assert_array_equal(np.array(v["Mean_Results"]["Field"], dtype=float), alone.field)
+
+
+def test_device_provider_run_agrees_statistically(tmp_path):
+    """-device-provider draws the particles on the GPU from the .ini's templates: a
+    different sample of the same distributions, so the mean agrees within Monte-Carlo
+    error with the host-provider run, and the drawn sizes follow the templates."""
+    path = _copy(tmp_path, "current_brown_neel.ini", 4000, ("current_particle.ini", "current_particle_b.ini"))
+    host = settings.run_ini(path, seed=5)
+    dev = settings.run_ini(path, seed=5, device_provider=True)
+    a = np.array(host["Mean_Results"]["Results"], dtype=float)
+    b = np.array(dev["Mean_Results"]["Results"], dtype=float)
+    assert np.all(np.isfinite(b))
+    se = np.sqrt(2.0 / (3.0 * 4000))
+    assert np.max(np.abs(a - b)) < 5 * se
+    mp = dev["Mean_Results"]["Mean_Properties"]
+    # templates 1e-8 and 1.4e-8 m at weights 3:1, lognormal 10 %: mean 1.1e-8 m
+    assert abs(mp["Magnetic_radius"] / 1.1e-8 - 1) < 0.02
+    assert dev["Stats"]["particle_steps"] == host["Stats"]["particle_steps"]
