@@ -129,6 +129,20 @@ def profiled_traffic_per_particle():
     return (float(m.group(1)), path.name) if m else (None, None)
 
 
+def profiled_instructions():
+    """Thread-instructions per particle-step of the FP32 step kernels (Millstein, Heun),
+    from the committed ncu summary."""
+    import re
+    path = ROOT / "profiles" / "step_kernel_instruction_counts_65536.md"
+    try:
+        text = path.read_text()
+    except OSError:
+        return None, None
+    m = re.search(r"thread_instructions_per_particle_step_millstein:\s*([0-9.]+)", text)
+    h = re.search(r"thread_instructions_per_particle_step_heun:\s*([0-9.]+)", text)
+    return ((float(m.group(1)), float(h.group(1))) if m and h else None), path.name
+
+
 def serving_leg(ctx, seconds, rate, step_scale, seed=0x5EED0005, serial_sample=48):
     """Poisson arrivals of mixed Neel / BrownAndNeelEulerSpherical requests with the
     batched-set distributions and the 2D Lissajous field, served by the continuous-
@@ -485,6 +499,19 @@ def main():
 
     if rank == 0:
         tpp, tsrc = profiled_traffic_per_particle()
+        ipp, isrc = profiled_instructions()
+        issue = None
+        if ipp is not None:
+            # peak issue: 4 schedulers per SM, one warp-instruction per cycle each, at the
+            # median SM clock sampled during the timed region
+            sms = torch.cuda.get_device_properties(local).multi_processor_count
+            clk = results["FP32"]["clocks"].get("sm_mhz") or 1965.0
+            peak_ti = sms * 4 * 32 * clk * 1e6 / 1e12  # tera thread-instructions/s
+            ach_ti = v32 / world * (ipp[0] + ipp[1]) / 2 / 1e12
+            issue = {"achieved": ach_ti, "peak": peak_ti, "unit": "T thread-instructions/s", "frac": ach_ti / peak_ti,
+                     "instructions_per_particle_step": {"Millstein": ipp[0], "Heun": ipp[1]},
+                     "source": f"profiles/{isrc}: ncu smsp__inst_executed per particle-step x measured FP32 rate; "
+                               "peak = SMs x 4 schedulers x 32 lanes x median SM clock"}
         cpu = None if args.no_cpu_baseline else cpu_baseline()
         c32 = results["FP32"]["clocks"]
         line = {
@@ -511,7 +538,8 @@ def main():
                          f"profiles/{tsrc}: DRAM bytes per particle per launch x {N_PER_GPU} particles",
                          "peak_source": "measured in bench.py: FMA-chain kernel on this GPU",
                          "flops_per_particle_step": {"Millstein": flops_step[0], "Heun": flops_step[1]},
-                         "fp64": {"achieved": sum(ach64) / 2, "peak": peak64, "frac": (sum(ach64) / 2) / peak64}},
+                         "fp64": {"achieved": sum(ach64) / 2, "peak": peak64, "frac": (sum(ach64) / 2) / peak64},
+                         "issue": issue},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": results["FP32"]["launches"],
             "clocks": c32,
