@@ -24,6 +24,8 @@ Heun) on the device-resident state, i.e. 2 x 65536 x 10000 particle-steps.
                FP64 as the serial baseline
   batched      256 Neel parameter sets (uneven N and S) submitted at once, batched
                per kernel key into shared launches (N=1)
+  plain_neel_1024  the 1024-particle FP64 Neel run of 1e6 steps (latency-bound small
+               ensemble), whole run on the device and end to end, beside the CPU
   stiff        the cubic ImplicitMidpoint workload (262144 particles, dt = 1e-10 s):
                FP64 with the reference's Newton matrix, FP64 and FP32 with the exact one
   --impl reference  runs that CPU restatement as the reference arm
@@ -250,6 +252,41 @@ def batched_leg(ctx, count, step_scale, seed=0x5EED0004, serial_sample=32):
             "workload": f"Neel, N ~ logU[1e3, 6.4e4], S ~ logU[1e5, 1e7] x {step_scale}, |B| ~ U[1, 25] mT, "
                         "f ~ logU[1e4, 1e6] Hz, K ~ U[5e3, 3e4] J/m^3, alpha ~ U[0.02, 0.3], Heun / Millstein "
                         "alternating, FP32, W = 1000, dt = 1e-11 s"}
+
+
+def plain_neel_leg(ctx, torch, cpu_steps=20000):
+    """The plain Neel workload as the reference runs it: 1024 particles, FP64 Heun, the
+    whole run of 1e6 steps with a sample every 100 steps (one field period at 100 kHz).
+    A small ensemble: 32 warps, so each step's latency, not throughput, sets the time.
+    Timed on the device (resident, CUDA events) and end to end through sp_simulate;
+    the CPU restatement runs the first `cpu_steps` steps of the same particles on all
+    host cores for comparison."""
+    import oracle
+    from stochasticphysics_b200 import provider
+
+    spec = provider.neel_relaxation()
+    st = torch.cuda.Stream()
+    with ctx.ensemble(spec) as e:
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        e.advance(spec.integrated_steps, st.cuda_stream)
+        b.record(st)
+        torch.cuda.synchronize()
+        dev_s = a.elapsed_time(b) / 1e3
+    t = time.perf_counter()
+    ctx.simulate(spec)
+    e2e_s = time.perf_counter() - t
+    ps = spec.n * spec.integrated_steps
+    cpu = dataclasses.replace(spec, number_of_steps=cpu_steps + 100)
+    t = time.perf_counter()
+    oracle.simulate(cpu, threads=os.cpu_count() or 1)
+    cpu_s = time.perf_counter() - t
+    cpu_rate = spec.n * cpu_steps / cpu_s
+    return {"value": ps / dev_s, "unit": UNIT, "run_s": dev_s, "e2e_run_s": e2e_s,
+            "cpu": {"value": cpu_rate, "unit": UNIT, "cores": os.cpu_count() or 1,
+                    "estimated_run_s": ps / cpu_rate, "sample": f"1024 particles x {cpu_steps} steps"},
+            "workload": "neel_relaxation: Neel, FP64 Heun, 1024 particles, K = 1e4 J/m^3 easy axis, r = 10 nm, "
+                        "alpha = 0.1, 10 mT at 100 kHz, dt = 1e-11 s, 1e6 steps, sample every 100 steps"}
 
 
 def stiff_leg(ctx, torch, n=262144, timed_steps=2000):
@@ -496,6 +533,7 @@ def main():
         if world == 1 and args.batched_sets > 0:
             batched = batched_leg(ctx, args.batched_sets, args.batched_step_scale)
         stiff = None if (world > 1 or args.no_stiff) else stiff_leg(ctx, torch)
+        plain_neel = None if (world > 1 or args.no_cpu_baseline) else plain_neel_leg(ctx, torch)
 
     if rank == 0:
         tpp, tsrc = profiled_traffic_per_particle()
@@ -548,6 +586,7 @@ def main():
             "serving": serving,
             "batched": batched,
             "stiff": stiff,
+            "plain_neel_1024": plain_neel,
         }
         print(json.dumps(line), flush=True)
     if world > 1:
