@@ -273,6 +273,7 @@ def plain_neel_leg(ctx, torch, cpu_steps=20000):
         b.record(st)
         torch.cuda.synchronize()
         dev_s = a.elapsed_time(b) / 1e3
+        res = e.read()
     t = time.perf_counter()
     ctx.simulate(spec)
     e2e_s = time.perf_counter() - t
@@ -283,6 +284,11 @@ def plain_neel_leg(ctx, torch, cpu_steps=20000):
     cpu_s = time.perf_counter() - t
     cpu_rate = spec.n * cpu_steps / cpu_s
     return {"value": ps / dev_s, "unit": UNIT, "run_s": dev_s, "e2e_run_s": e2e_s,
+            "nonfinite_particles": res.stats["nonfinite_particles"],
+            "note": "the Cartesian Heun step does not renormalise |m| (the reference's own norm handling); "
+                    "at dt = 1e-11 s the precession step omega dt is ~0.09, |m| drifts and some particles "
+                    "overflow within 1e6 steps on the CPU restatement too, so the late windows of the mean "
+                    "are not finite; the figure is a timing of the configuration as specified",
             "cpu": {"value": cpu_rate, "unit": UNIT, "cores": os.cpu_count() or 1,
                     "estimated_run_s": ps / cpu_rate, "sample": f"1024 particles x {cpu_steps} steps"},
             "workload": "neel_relaxation: Neel, FP64 Heun, 1024 particles, K = 1e4 J/m^3 easy axis, r = 10 nm, "

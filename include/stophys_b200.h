@@ -338,7 +338,9 @@ SP_API sp_status sp_server_create(sp_context* ctx, const sp_server_config* cfg, 
 /* The description (and every array it points to) is copied at submit. */
 SP_API sp_status sp_server_submit(sp_server* srv, const sp_ensemble_desc* desc, uint64_t* request_id);
 SP_API sp_status sp_server_poll(sp_server* srv, uint64_t request_id, int32_t* state);
-/* Blocks up to timeout_ms (<0: forever) and copies results of a finished request. */
+/* Blocks up to timeout_ms (<0: forever) and copies results of a finished request.
+ * A finished, failed or cancelled request is reported once: afterwards its id is
+ * unknown (SP_ERR_NOT_FOUND).  SP_ERR_NOT_READY leaves it pending. */
 SP_API sp_status sp_server_wait(sp_server* srv, uint64_t request_id, double timeout_ms, sp_result* out,
                          sp_stats* stats, double* latency_ms);
 SP_API sp_status sp_server_cancel(sp_server* srv, uint64_t request_id);

@@ -139,6 +139,10 @@ struct sp_server {
             try {
                 r->ens = std::make_unique<Ensemble>(ctx, r->desc, launch_for(r->desc));
                 r->ens->last_stream = nullptr;
+                // the ensemble holds its inputs on the device now: drop the host copies
+                std::vector<double>().swap(r->arrays);
+                r->desc.particles = sp_particles{};
+                r->desc.injected_dw = nullptr;
                 r->state = SP_REQUEST_RUNNING;
                 used_bytes += r->bytes;
                 active.push_back(r);
@@ -378,7 +382,12 @@ sp_status sp_server_wait(sp_server* s, uint64_t id, double timeout_ms, sp_result
     if (timeout_ms < 0) s->cv_done.wait(lk, terminal);
     else if (!s->cv_done.wait_for(lk, std::chrono::duration<double, std::milli>(timeout_ms), terminal))
         return fail(SP_ERR_NOT_READY, "request still running");
-    if (r->state != SP_REQUEST_DONE) return fail(r->error, r->message);
+    if (r->state != SP_REQUEST_DONE) {
+        const sp_status err = r->error;
+        const std::string msg = r->message;
+        s->all.erase(it);  // a failed or cancelled request is reported once
+        return fail(err, msg);
+    }
     if (out) {
         if (out->mean) std::memcpy(out->mean, r->mean.data(), r->mean.size() * 8);
         if (out->weight) std::memcpy(out->weight, r->weight.data(), r->weight.size() * 8);
@@ -389,6 +398,7 @@ sp_status sp_server_wait(sp_server* s, uint64_t id, double timeout_ms, sp_result
     }
     if (stats) *stats = r->stats;
     if (latency_ms) *latency_ms = std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count();
+    s->all.erase(it);  // results are handed over once; the id is forgotten
     return SP_OK;
     SP_GUARD_END
 }

@@ -1,0 +1,79 @@
+"""Server life cycle on the GPU: admission refusal, queueing behind max_active, wait
+timeouts, cancellation while queued and while running, and results handed over once."""
+import dataclasses
+
+import numpy as np
+import pytest
+
+import stochasticphysics_b200 as sp
+from stochasticphysics_b200 import provider
+from stochasticphysics_b200._abi import RequestState, Solver, Status
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = sp.Context(0)
+    yield c
+    c.close()
+
+
+def small(n=2000, steps=4000, seed=1):
+    return provider.neel_relaxation(n=n, steps=steps, oversampling=100, solver=Solver.Heun_Strong, seed=seed)
+
+
+def test_admission_refused_when_the_request_exceeds_the_budget(ctx):
+    with sp.Server(ctx, memory_budget_bytes=1 << 20) as srv:
+        with pytest.raises(sp.SPError) as e:
+            srv.submit(small(n=200000))
+        assert e.value.status == Status.ADMISSION_REFUSED
+
+
+def test_wait_timeout_then_result_once(ctx):
+    long = small(n=65536, steps=200000)
+    with sp.Server(ctx) as srv:
+        rid = srv.submit(long)
+        with pytest.raises(sp.SPError) as e:
+            srv.wait(rid, timeout_ms=1.0)
+        assert e.value.status == Status.NOT_READY
+        res, lat = srv.wait(rid)
+        assert lat > 0 and res.mean.shape == (long.n_samples, 3)
+        assert res.stats["particle_steps"] == long.n * long.integrated_steps
+        with pytest.raises(sp.SPError) as e2:
+            srv.wait(rid)
+        assert e2.value.status == Status.NOT_FOUND
+
+
+def test_queue_behind_max_active_and_cancel(ctx):
+    with sp.Server(ctx, max_active=1) as srv:
+        first = srv.submit(small(n=65536, steps=300000, seed=2))
+        queued = srv.submit(small(seed=3))
+        assert srv.poll(queued) == RequestState.QUEUED
+        srv.cancel(queued)
+        with pytest.raises(sp.SPError) as e:
+            srv.wait(queued)
+        assert e.value.status == Status.CANCELLED
+        assert srv.poll(first) in (RequestState.QUEUED, RequestState.RUNNING)
+        srv.cancel(first)
+        with pytest.raises(sp.SPError) as e2:
+            srv.wait(first)
+        assert e2.value.status == Status.CANCELLED
+        # the server keeps serving after cancellations
+        spec = small(seed=4)
+        done = srv.submit(spec)
+        res, _ = srv.wait(done)
+        np.testing.assert_array_equal(res.mean, ctx.simulate(spec).mean)
+
+
+def test_many_requests_release_their_memory(ctx):
+    """Host copies are dropped at admission and results at hand-over, so a long
+    stream of requests does not accumulate state in the server."""
+    with sp.Server(ctx) as srv:
+        for k in range(3):
+            ids = [srv.submit(small(n=1000, steps=1000, seed=10 * k + j)) for j in range(20)]
+            for i in ids:
+                srv.wait(i)
+            for i in ids:
+                with pytest.raises(sp.SPError):
+                    srv.poll(i)
