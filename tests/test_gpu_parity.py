@@ -310,8 +310,11 @@ def test_fp32_form_close_to_fp64(ctx):
     itself equally fast); afterwards the FP32 ensemble is a statistically equivalent sample.
     Checks: the first window within 1e-4, and every window within 4 standard errors of the
     difference of two N-particle means (|m_i| <= 1, so sigma^2 <= 1/3 per component)."""
-    for problem, solver in ((Problem.Neel, Solver.Heun_Strong), (Problem.BrownAndNeelEulerSpherical, Solver.Millstein),
-                            (Problem.BrownAndNeelEulerSpherical, Solver.Heun_Strong)):
+    for problem, solver in ((Problem.Neel, Solver.Heun_Strong), (Problem.Neel, Solver.Millstein),
+                            (Problem.NeelSpherical, Solver.Heun_Strong), (Problem.NeelSpherical, Solver.EulerMaruyama),
+                            (Problem.BrownAndNeelEulerSpherical, Solver.Millstein),
+                            (Problem.BrownAndNeelEulerSpherical, Solver.Heun_Strong),
+                            (Problem.BrownAndNeel, Solver.Heun_Strong)):
         n = 4096
         spec = small_spec(problem, solver, n=n, steps=20000, W=1000)
         r64 = ctx.simulate(spec)
@@ -322,20 +325,36 @@ def test_fp32_form_close_to_fp64(ctx):
         assert np.nanmax(d) < bound, f"{problem.name}/{solver.name}: FP32 mean error {np.nanmax(d):.2e}"
 
 
-def test_langevin_equilibrium(ctx):
-    """Zero anisotropy, constant field: <m.B/|B|> -> coth(xi) - 1/xi, xi = Ms V |B| / (kB T)."""
+LANGEVIN = [(p, prec) for p in (Problem.Neel, Problem.NeelSpherical, Problem.BrownAndNeelEulerSpherical)
+            for prec in (Precision.FP64, Precision.FP32)]
+
+
+@pytest.mark.parametrize("problem,precision", LANGEVIN, ids=[f"{p.name}-{q.name}" for p, q in LANGEVIN])
+def test_langevin_equilibrium(ctx, problem, precision):
+    """Zero anisotropy, constant field, Heun: <m.B/|B|> -> coth(xi) - 1/xi with
+    xi = Ms V |B| / (kB T), for every problem that carries a magnetisation direction and in
+    both precisions (the Euler problem's magnetisation is outputs 7-9).  Heun, because the
+    reference's Millstein formula (Millstein.inl:43, D |dW|^2) does not keep this
+    equilibrium (test_oracle_cpu.py pins that)."""
     n, B = 16384, 0.01
     rng = np.random.default_rng(21)
     v = rng.standard_normal((n, 3))
     m0 = v / np.linalg.norm(v, axis=1, keepdims=True)
-    spec = dataclasses.replace(provider.neel_relaxation(n=n, steps=60000, oversampling=1000),
-                               anisotropy_constant=np.zeros(n), magnetisation=m0,
+    if problem == Problem.BrownAndNeelEulerSpherical:
+        base = provider.brown_neel_relaxation(n=n, steps=60000, oversampling=1000, solver=Solver.Heun_Strong)
+        base = dataclasses.replace(base, magnetic_radius=np.full(n, 10e-9), hydrodynamic_radius=np.full(n, 30e-9))
+    else:
+        base = provider.neel_relaxation(n=n, steps=60000, oversampling=1000, solver=Solver.Heun_Strong)
+        if problem == Problem.NeelSpherical:
+            base = dataclasses.replace(base, problem=problem, use_coordinate_transformation=True,
+                                       min_angle_before_transformation=math.pi / 36)
+    spec = dataclasses.replace(base, anisotropy_constant=np.zeros(n), magnetisation=m0, precision=precision,
                                field=sp.FieldSpec.constant((0.0, 0.0, B)))
     r = ctx.simulate(spec)
     V = 4.0 / 3.0 * math.pi * (10e-9) ** 3
     xi = 4.8e5 * V * B / (1.3806485279e-23 * 295.0)
     langevin = 1.0 / math.tanh(xi) - 1.0 / xi
-    tail = r.mean[30:, 2]  # after ~5 relaxation times
+    tail = r.mean[30:, -1]  # m_z after ~5 relaxation times
     se = 1.0 / math.sqrt(3.0 * n)  # per-window standard error bound (|m_z| <= 1, variance <= 1/3)
     assert abs(tail.mean() - langevin) < 3 * se + 2e-3, (tail.mean(), langevin)
 

@@ -71,3 +71,32 @@ def test_euler_maruyama_normalized_keeps_unit_vectors():
     emn = oracle.simulate(dataclasses.replace(base, solver=Solver.EulerMaruyama_Normalized), final_state=True)
     np.testing.assert_allclose(np.linalg.norm(emn["final_state"], axis=1), 1.0, rtol=1e-14)
     assert np.abs(np.linalg.norm(em["final_state"], axis=1) - 1).max() > 1e-9
+
+
+def test_reference_millstein_does_not_keep_the_langevin_equilibrium():
+    """The reference's Millstein step (Millstein.inl:35-44) adds the Ito-Stratonovich
+    drift as D |dW|^2 summed over all noise components, where a consistent scheme adds
+    D dt.  With zero anisotropy in a constant field the Heun step relaxes to the
+    Langevin value coth(xi) - 1/xi; the Millstein step as written does not (the
+    Cartesian magnetisation even shrinks).  The engine keeps the reference's formula;
+    this test pins the behaviour so that it stays documented."""
+    import dataclasses
+    import math
+    import stochasticphysics_b200 as sp
+    from stochasticphysics_b200 import provider
+    from stochasticphysics_b200._abi import Solver
+    n, B = 512, 0.01
+    rng = np.random.default_rng(21)
+    v = rng.standard_normal((n, 3))
+    m0 = v / np.linalg.norm(v, axis=1, keepdims=True)
+    V = 4 / 3 * math.pi * (10e-9) ** 3
+    xi = 4.8e5 * V * B / (1.3806485279e-23 * 295)
+    langevin = 1 / math.tanh(xi) - 1 / xi
+    out = {}
+    for solver in (Solver.Heun_Strong, Solver.Millstein):
+        spec = dataclasses.replace(provider.neel_relaxation(n=n, steps=20000, oversampling=1000, solver=solver),
+                                   anisotropy_constant=np.zeros(n), magnetisation=m0,
+                                   field=sp.FieldSpec.constant((0.0, 0.0, B)))
+        out[solver] = oracle.simulate(spec)["mean"][10:, 2].mean()
+    assert abs(out[Solver.Heun_Strong] - langevin) < 4 / math.sqrt(3 * n)
+    assert out[Solver.Millstein] < 0.5 * langevin
