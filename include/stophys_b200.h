@@ -34,7 +34,7 @@
 extern "C" {
 #endif
 
-#define SP_ABI_VERSION 5u
+#define SP_ABI_VERSION 6u
 
 #if defined(_WIN32)
 #define SP_API __declspec(dllexport)
@@ -95,7 +95,14 @@ typedef enum sp_solver {
     SP_SOLVER_HEUN_STRONG = 1,
     SP_SOLVER_MILLSTEIN = 2,
     SP_SOLVER_IMPLICIT_MIDPOINT = 3,
-    SP_SOLVER_EULER_MARUYAMA_NORMALIZED = 4  /* EulerMaruyama_Normalized.inl:40-56 */
+    SP_SOLVER_EULER_MARUYAMA_NORMALIZED = 4, /* EulerMaruyama_Normalized.inl:40-56 */
+    /* The next three exist in the reference but are switched off in its manager
+     * (SimulationManager.h:325-328).  They take in-kernel (Philox) noise only.
+     * Each evaluates its support points in the chart prepareCalculations chose for
+     * y_n and finishes once, like HEUN_STRONG. */
+    SP_SOLVER_HEUN_NOT_CONSISTENT = 5, /* Heun_NotConsistent.inl:35-47: two independent dW */
+    SP_SOLVER_WEAK_TEST = 6,           /* WeakTest.inl:18-63 + double noise matrix        */
+    SP_SOLVER_EXPLICIT_STRONG_1 = 7    /* Explicit_Strong_1.inl:20-78 + double noise matrix */
 } sp_solver;
 
 typedef enum sp_precision {
@@ -237,7 +244,10 @@ typedef struct sp_ensemble_desc {
     int32_t record_trajectories; /* keep per-particle window means on the device (parity
                                     runs; the reference's per-particle result vectors) */
     int32_t jacobian;            /* sp_jacobian (ImplicitMidpoint only)               */
-    int32_t reserved0;
+    int32_t double_noise_approx; /* Solver_Settings Approximation_of_double_noise_integral
+                                    (WeakTest, ExplicitStrong_1.0): order p of the double
+                                    Stratonovich integral approximation, -1..10
+                                    (SimulationManager.h:503-525, DoubleNoiseMatrix.h) */
     double accuracy_goal;        /* Solver_Settings Accuracy_Goal (ImplicitMidpoint)  */
     uint64_t number_of_steps;    /* Simulation_Settings Number_of_steps               */
     uint64_t oversampling;       /* Simulation_Settings OverSampling (window W)       */

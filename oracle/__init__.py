@@ -57,6 +57,9 @@ def lib():
         L.oracle_field_eval.argtypes = [C.c_void_p, _dp, C.c_uint64, _dp]
         L.oracle_neel_exact_jacobians.restype = None
         L.oracle_neel_exact_jacobians.argtypes = [C.c_int] + [_dp] * 7
+        L.oracle_double_noise_matrix.restype = None
+        L.oracle_double_noise_matrix.argtypes = [C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64, C.c_int, C.c_double,
+                                                 C.c_int, _dp, _dp]
         L.oracle_count_ops.restype = C.c_int
         L.oracle_count_ops.argtypes = [C.c_void_p, _dp]
         _lib = L
@@ -94,6 +97,14 @@ def philox_normals(seed: int, pid0: int, n: int, step0: int, nsteps: int, m: int
     out = np.zeros((nsteps, m, n))
     lib().oracle_philox_normals(seed, pid0, n, step0, nsteps, m, _p(out))
     return out
+
+
+def double_noise_matrix(seed: int, pid0: int, n: int, step: int, p: int, dt: float, m: int):
+    """(dW[n][m], J[n][m][m]) of WeakTest / ExplicitStrong_1.0 at one step."""
+    dw = np.zeros((n, m))
+    J = np.zeros((n, m, m))
+    lib().oracle_double_noise_matrix(seed, pid0, n, step, p, dt, m, _p(dw), _p(J))
+    return dw, J
 
 
 def philox4x32_10(ctr, key) -> list:

@@ -73,21 +73,28 @@ inline void philox4x32_10(uint32_t ctr[4], uint32_t k0, uint32_t k1) {
         k0 += 0x9E3779B9u; k1 += 0xBB67AE85u;
     }
 }
-// Unit normals for (seed, particle id, step): Box-Muller on uniforms
-// u = (w + 1/2) 2^-32; call j yields z[4j..4j+3].
-inline void philox_normals(uint64_t seed, uint64_t pid, uint64_t step, int m, double* z) {
+// The four unit normals of Philox call `call` for (seed, particle id, step):
+// Box-Muller on uniforms u = (w + 1/2) 2^-32.
+inline void philox_call_normals(uint64_t seed, uint64_t pid, uint64_t step, uint32_t call, double* v) {
+    uint32_t c[4] = {static_cast<uint32_t>(step), static_cast<uint32_t>(step >> 32), static_cast<uint32_t>(pid),
+                     (static_cast<uint32_t>(pid >> 32) & 0xFFFFFFu) | (call << 24)};
+    philox4x32_10(c, static_cast<uint32_t>(seed), static_cast<uint32_t>(seed >> 32));
+    const double inv = 2.3283064365386963e-10;  // 2^-32
+    const double u0 = (c[0] + 0.5) * inv, u1 = (c[1] + 0.5) * inv;
+    const double u2 = (c[2] + 0.5) * inv, u3 = (c[3] + 0.5) * inv;
+    const double r0 = std::sqrt(-2.0 * std::log(u0));
+    const double r1 = std::sqrt(-2.0 * std::log(u2));
+    const double t0 = kTwoPi * u1, t1 = kTwoPi * u3;
+    v[0] = r0 * std::cos(t0); v[1] = r0 * std::sin(t0); v[2] = r1 * std::cos(t1); v[3] = r1 * std::sin(t1);
+}
+// m unit normals for (seed, particle id, step) from calls call0, call0 + 1:
+// call call0 + j yields z[4j..4j+3].  Calls 0-1 carry dW, calls 2-3
+// Heun_NotConsistent's second increment, calls 2.. the double-noise draws.
+inline void philox_normals(uint64_t seed, uint64_t pid, uint64_t step, int m, double* z, uint32_t call0 = 0) {
     const int calls = (m + 3) / 4;
     for (int j = 0; j < calls; ++j) {
-        uint32_t c[4] = {static_cast<uint32_t>(step), static_cast<uint32_t>(step >> 32), static_cast<uint32_t>(pid),
-                         (static_cast<uint32_t>(pid >> 32) & 0xFFFFFFu) | (static_cast<uint32_t>(j) << 24)};
-        philox4x32_10(c, static_cast<uint32_t>(seed), static_cast<uint32_t>(seed >> 32));
-        const double inv = 2.3283064365386963e-10;  // 2^-32
-        const double u0 = (c[0] + 0.5) * inv, u1 = (c[1] + 0.5) * inv;
-        const double u2 = (c[2] + 0.5) * inv, u3 = (c[3] + 0.5) * inv;
-        const double r0 = std::sqrt(-2.0 * std::log(u0));
-        const double r1 = std::sqrt(-2.0 * std::log(u2));
-        const double t0 = kTwoPi * u1, t1 = kTwoPi * u3;
-        const double v[4] = {r0 * std::cos(t0), r0 * std::sin(t0), r1 * std::cos(t1), r1 * std::sin(t1)};
+        double v[4];
+        philox_call_normals(seed, pid, step, call0 + static_cast<uint32_t>(j), v);
         for (int i = 0; i < 4 && 4 * j + i < m; ++i) z[4 * j + i] = v[i];
     }
 }
@@ -365,6 +372,90 @@ struct Stepper {
         pr.finishCalculations(res);
         return res;
     }
+    // SDEFramework/Solver/Heun_NotConsistent.inl:35-47 (Stratonovich): support point
+    // with dW, corrector with the mean of b at both points times an independent dW2;
+    // both points in the chart prepareCalculations chose for y_n, finished once.
+    static Dep heun_not_consistent(P& pr, const Dep& yi_in, const V3<T>& xi, const Vec<T, M>& dW,
+                                   const Vec<T, M>& dW2, const T& dt) {
+        Dep yi = yi_in;
+        pr.prepareCalculations(yi);
+        const Dep ayi = pr.getDeterministicVector(yi, xi) + pr.getDrift(yi);
+        const auto byi = pr.getStochasticMatrix(yi);
+        const Dep bdW = byi * dW;
+        const Dep Support = yi + ayi * dt + bdW;
+        pr.recomputeCache(Support);
+        const Dep a2 = pr.getDeterministicVector(Support, xi) + pr.getDrift(Support);
+        const auto bS = pr.getStochasticMatrix(Support);
+        Dep res = yi + (T(0.5) * (a2 + ayi)) * dt + T(0.5) * ((bS + byi) * dW2);
+        pr.finishCalculations(res);
+        return res;
+    }
+    // SDEFramework/Solver/Explicit_Strong_1.inl:20-78 (no drift correction): support
+    // points tmp +- b.col(j1) sqrt(dt) for j1 < D around tmp = y + a dt,
+    //   y' = sum_j1 (b(S+) - b(S-)) J.col(j1) / sqrt(dt) + (tmp + b dW).
+    static Dep explicit_strong_1(P& pr, const Dep& yi_in, const V3<T>& xi, const Vec<T, M>& dW,
+                                 const Mat<T, M, M>& J, const T& dt, const T& sqrtdt) {
+        Dep yi = yi_in;
+        pr.prepareCalculations(yi);
+        const Dep a = pr.getDeterministicVector(yi, xi);
+        const auto b = pr.getStochasticMatrix(yi);
+        const Dep tmpvec = yi + a * dt;
+        Dep tmpvec2 = Dep::zero();
+        for (int j1 = D; j1--;) {
+            Dep col;
+            for (int i = 0; i < D; ++i) col[i] = b(i, j1);
+            Vec<T, M> Jc;
+            for (int r = 0; r < M; ++r) Jc[r] = J(r, j1);
+            const Dep Sp = tmpvec + col * sqrtdt, Sm = tmpvec - col * sqrtdt;
+            pr.recomputeCache(Sp);
+            const auto bSp = pr.getStochasticMatrix(Sp);
+            pr.recomputeCache(Sm);
+            const auto bSm = pr.getStochasticMatrix(Sm);
+            tmpvec2 = tmpvec2 + (bSp - bSm) * Jc;
+        }
+        for (int i = 0; i < D; ++i) tmpvec2[i] = tmpvec2[i] / sqrtdt;
+        Dep res = tmpvec2 + (tmpvec + b * dW);
+        pr.finishCalculations(res);
+        return res;
+    }
+    // SDEFramework/Solver/WeakTest.inl:18-63
+    static Dep weak_test(P& pr, const Dep& yi_in, const V3<T>& xi, const Vec<T, M>& dW, const Mat<T, M, M>& J,
+                         const T& dt, const T& sqrtdt) {
+        Dep yi = yi_in;
+        pr.prepareCalculations(yi);
+        const Dep a = pr.getDeterministicVector(yi, xi);
+        const auto b = pr.getStochasticMatrix(yi);
+        const Dep adt = a * dt;
+        const Dep tmpvec = yi + adt;
+        const Dep bdW = b * dW;
+        const Dep ys = tmpvec + bdW;
+        pr.recomputeCache(ys);
+        const Dep as = pr.getDeterministicVector(ys, xi);
+        Dep tmpvec2 = Dep::zero();
+        for (int j1 = D; j1--;) {
+            Dep col;
+            for (int i = 0; i < D; ++i) col[i] = b(i, j1);
+            Vec<T, M> Jc;
+            for (int r = 0; r < M; ++r) Jc[r] = J(r, j1);
+            const Dep Sp = tmpvec + col * sqrtdt, Sm = tmpvec - col * sqrtdt;
+            pr.recomputeCache(Sp);
+            const auto bSp = pr.getStochasticMatrix(Sp);
+            pr.recomputeCache(Sm);
+            const auto bSm = pr.getStochasticMatrix(Sm);
+            Dep diff = (bSp - bSm) * Jc;
+            for (int i = 0; i < D; ++i) diff[i] = diff[i] / sqrtdt;
+            tmpvec2 = tmpvec2 + diff;
+            tmpvec2 = tmpvec2 + (bSp + bSm) * dW;
+        }
+        for (int i = 0; i < D; ++i) tmpvec2[i] = tmpvec2[i] / T(4.0);
+        tmpvec2 = tmpvec2 + T(0.5) * bdW;
+        const Dep ys2 = ((yi + (T(0.5) * as) * dt) + T(0.5) * adt) + tmpvec2;
+        pr.recomputeCache(ys2);
+        const Dep as2 = pr.getDeterministicVector(ys2, xi);
+        Dep res = ((yi + (T(0.5) * as2) * dt) + T(0.5) * adt) + tmpvec2;
+        pr.finishCalculations(res);
+        return res;
+    }
     // SDEFramework/Solver/Implicit_Midpoint.inl:40-188: Newton on
     //   f(y) = finish(prepare((y+y_n)/2) + a dt + b dW) + y_n/2 - 3y/2
     // with S = -I + dt/2 J_a + 1/2 J_b (:83-98), initial guess y_n (:56),
@@ -406,12 +497,63 @@ struct Stepper {
     }
 };
 
+// ====================================================================== double noise matrix
+// SDEFramework/DoubleNoiseMatrix.h getNoiseMatrix (orders p >= 1, p = 0, p = -1),
+// after Kloeden & Platen 1992, sec. 5.8: J(j1, j2) = dW_j1 dW_j2 / 2 +- A for j1 > j2,
+// J(j1, j1) = dW_j1^2 / 2, with
+//   A = -1/(2 pi) sum_{r=1}^{p} 1/r [z1 (sqrt2 dW_j2 - z2) - z3 (sqrt2 dW_j1 - z4)]
+//       + rho_p (mu1 dW_j2 - mu2 dW_j1),   rho_p = sqrt(1/12 - sum_{r<=p} 1/(2 pi^2 r^2)).
+// Every z and mu is a fresh N(0, dt) draw per pair, as the reference's generators
+// advance on every call.  Draw order: pairs j1 = M-1..1, j2 = j1-1..0; per pair one
+// Philox call (4 normals) per r, then one call whose first two normals are mu1, mu2;
+// calls start at 2.
+inline double double_noise_rho(int p) {
+    double s = 0.0;
+    for (int r = 1; r <= p; ++r) s += 1.0 / (static_cast<double>(r) * r);
+    return std::sqrt(1.0 / 12.0 - s / (2.0 * kPi * kPi));
+}
+template <class T, int M>
+Mat<T, M, M> double_noise_matrix(uint64_t seed, uint64_t pid, uint64_t step, int p, const T& sqrtdt,
+                                 const Vec<T, M>& dW) {
+    const T sqrt2 = T(1.4142135623730951), inv2pi = T(0.15915494309189535);
+    const T rho = T(double_noise_rho(p));
+    Mat<T, M, M> J = Mat<T, M, M>::zero();
+    uint32_t call = 2;
+    for (int j1 = M; j1--;) {
+        for (int j2 = j1; j2--;) {
+            J(j1, j2) = (T(0.5) * dW[j1]) * dW[j2];
+            J(j2, j1) = J(j1, j2);
+            T tmp = T(0.0);
+            if (p >= 1) {
+                T sum = T(0.0);
+                for (int r = 1; r <= p; ++r) {
+                    double z[4];
+                    philox_call_normals(seed, pid, step, call++, z);
+                    const T z1 = T(z[0]) * sqrtdt, z2 = T(z[1]) * sqrtdt, z3 = T(z[2]) * sqrtdt, z4 = T(z[3]) * sqrtdt;
+                    sum = sum + (T(1.0) / T(r)) * (z1 * (sqrt2 * dW[j2] - z2) - z3 * (sqrt2 * dW[j1] - z4));
+                }
+                tmp = -sum * inv2pi;
+            }
+            if (p >= 0) {
+                double u[4];
+                philox_call_normals(seed, pid, step, call++, u);
+                tmp = tmp + rho * ((T(u[0]) * sqrtdt) * dW[j2] - (T(u[1]) * sqrtdt) * dW[j1]);
+            }
+            J(j1, j2) = J(j1, j2) + tmp;
+            J(j2, j1) = J(j2, j1) - tmp;
+        }
+        J(j1, j1) = (T(0.5) * dW[j1]) * dW[j1];
+    }
+    return J;
+}
+
 // ====================================================================== simulation
 struct SimSpec {
     int problem, aniso, solver;
     ProblemCfg cfg;
     int maxIter; double tol;
     bool exactJacobian;
+    int doubleNoiseApprox;
     uint64_t steps, W; double dt;
     FieldEval field;
     uint64_t seed, pid_offset;
@@ -463,6 +605,22 @@ void simulate_particle(const SimSpec& sp, const ParticleIn& pin, uint64_t p, dou
                 for (int i = 0; i < 3; ++i) xi[i] = T(B[i]);
                 switch (sp.solver) {
                     case SP_SOLVER_EULER_MARUYAMA: yi = Stepper<P, T>::euler_maruyama(pr, yi, xi, dW, dt); break;
+                    case SP_SOLVER_HEUN_NOT_CONSISTENT: {
+                        philox_normals(sp.seed, sp.pid_offset + p, n, M, z, 2);
+                        Vec<T, M> dW2;
+                        for (int j = 0; j < M; ++j) dW2[j] = T(sqrt_dt * z[j]);
+                        yi = Stepper<P, T>::heun_not_consistent(pr, yi, xi, dW, dW2, dt);
+                        break;
+                    }
+                    case SP_SOLVER_WEAK_TEST:
+                    case SP_SOLVER_EXPLICIT_STRONG_1: {
+                        const T sqdt = T(sqrt_dt);
+                        const Mat<T, M, M> J =
+                            double_noise_matrix<T, M>(sp.seed, sp.pid_offset + p, n, sp.doubleNoiseApprox, sqdt, dW);
+                        yi = sp.solver == SP_SOLVER_WEAK_TEST ? Stepper<P, T>::weak_test(pr, yi, xi, dW, J, dt, sqdt)
+                                                              : Stepper<P, T>::explicit_strong_1(pr, yi, xi, dW, J, dt, sqdt);
+                        break;
+                    }
                     case SP_SOLVER_HEUN_STRONG: yi = Stepper<P, T>::heun(pr, yi, xi, dW, dt); break;
                     case SP_SOLVER_EULER_MARUYAMA_NORMALIZED:
                         yi = Stepper<P, T>::euler_maruyama_normalized(pr, yi, xi, dW, dt);
@@ -577,6 +735,7 @@ SimSpec spec_of(const sp_ensemble_desc& d) {
     s.cfg.simpleModel = d.problem_settings.use_simple_model != 0;
     s.maxIter = d.max_iteration; s.tol = d.accuracy_goal;
     s.exactJacobian = d.jacobian == SP_JACOBIAN_EXACT;
+    s.doubleNoiseApprox = d.double_noise_approx;
     s.steps = d.number_of_steps; s.W = d.oversampling; s.dt = d.timestep;
     s.field.init(d.field);
     s.seed = d.seed; s.pid_offset = d.particle_id_offset;
@@ -615,7 +774,7 @@ using namespace orc;
 
 extern "C" {
 
-int oracle_abi_version(void) { return 5; }
+int oracle_abi_version(void) { return 6; }
 
 // Runs the ensemble described by desc.  mean[K][OUT], weight[OUT], time[K],
 // field[K][3], traj[N][K][OUT] and final_state[N][D] are optional (NULL).
@@ -630,6 +789,10 @@ int oracle_simulate(const sp_ensemble_desc* d_in, double* mean, double* weight, 
     if (d->solver == SP_SOLVER_IMPLICIT_MIDPOINT && d->jacobian == SP_JACOBIAN_EXACT && d->problem != SP_PROBLEM_NEEL)
         return 3;
     if (!pick<double>(d->problem, d->anisotropy)) return 4;
+    if (d->solver >= SP_SOLVER_HEUN_NOT_CONSISTENT && d->noise == SP_NOISE_INJECTED) return 5;
+    if ((d->solver == SP_SOLVER_WEAK_TEST || d->solver == SP_SOLVER_EXPLICIT_STRONG_1) &&
+        (d->double_noise_approx < -1 || d->double_noise_approx > 10))
+        return 6;
     const SimSpec s = spec_of(*d);
     const int OUT = out_dim(d->problem), SD = state_dim(d->problem);
     const uint64_t K = s.steps / s.W, N = d->n_particles;
@@ -702,6 +865,28 @@ void oracle_philox_normals(uint64_t seed, uint64_t pid0, uint64_t n, uint64_t st
             philox_normals(seed, pid0 + p, step0 + s, m, z);
             for (int j = 0; j < m; ++j) out[(s * m + j) * n + p] = z[j];
         }
+}
+
+// Double noise matrices of particles pid0..pid0+n-1 at one step with the step's own
+// Philox dW (unit normals x sqrt(dt)): dw[n][m], J[n][m][m].  m = 3 or 6.
+void oracle_double_noise_matrix(uint64_t seed, uint64_t pid0, uint64_t n, uint64_t step, int p, double dt, int m,
+                                double* dw, double* J) {
+    const double sqdt = std::sqrt(dt);
+    for (uint64_t i = 0; i < n; ++i) {
+        double z[8];
+        philox_normals(seed, pid0 + i, step, m, z);
+        if (m == 3) {
+            Vec<double, 3> w;
+            for (int j = 0; j < 3; ++j) { w[j] = sqdt * z[j]; dw[i * 3 + j] = w[j]; }
+            const Mat<double, 3, 3> Jm = double_noise_matrix<double, 3>(seed, pid0 + i, step, p, sqdt, w);
+            for (int r = 0; r < 3; ++r) for (int c = 0; c < 3; ++c) J[(i * 3 + r) * 3 + c] = Jm(r, c);
+        } else {
+            Vec<double, 6> w;
+            for (int j = 0; j < 6; ++j) { w[j] = sqdt * z[j]; dw[i * 6 + j] = w[j]; }
+            const Mat<double, 6, 6> Jm = double_noise_matrix<double, 6>(seed, pid0 + i, step, p, sqdt, w);
+            for (int r = 0; r < 6; ++r) for (int c = 0; c < 6; ++c) J[(i * 6 + r) * 6 + c] = Jm(r, c);
+        }
+    }
 }
 
 // The particles of a provider: out[n][20] as sp_provide_particles writes them.

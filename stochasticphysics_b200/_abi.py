@@ -13,7 +13,7 @@ from typing import Optional
 
 import numpy as np
 
-ABI_VERSION = 5
+ABI_VERSION = 6
 
 
 class Status(IntEnum):
@@ -61,6 +61,10 @@ class Solver(IntEnum):
     Millstein = 2
     Implicit_Midpoint = 3
     EulerMaruyama_Normalized = 4
+    # switched off in the reference's manager (SimulationManager.h:325-328); in-kernel noise only
+    Heun_NotConsistent = 5
+    WeakTest = 6
+    ExplicitStrong_1 = 7
 
 
 class Precision(IntEnum):
@@ -175,7 +179,7 @@ class sp_ensemble_desc(C.Structure):
         ("max_iteration", C.c_int32),
         ("record_trajectories", C.c_int32),
         ("jacobian", C.c_int32),
-        ("reserved0", C.c_int32),
+        ("double_noise_approx", C.c_int32),
         ("accuracy_goal", C.c_double),
         ("number_of_steps", C.c_uint64),
         ("oversampling", C.c_uint64),
@@ -409,6 +413,7 @@ class EnsembleSpec:
     injected_dw: Optional[np.ndarray] = None
     record_trajectories: bool = False
     jacobian: Jacobian = Jacobian.Reference
+    double_noise_approx: int = -1                    # WeakTest / ExplicitStrong_1: order p, -1..10
     cubic_constant: Optional[np.ndarray] = None      # UniaxialCubic: K_cubic (n)
     uniaxial_rotation: Optional[np.ndarray] = None   # UniaxialCubic: Euler angles of the uniaxial axis (n, 3)
     provider: Optional[ProviderSpec] = None          # particles drawn on the device (arrays unused)
@@ -481,6 +486,7 @@ class DescHolder:
         d.max_iteration = int(spec.max_iteration)
         d.record_trajectories = int(bool(spec.record_trajectories))
         d.jacobian = int(spec.jacobian)
+        d.double_noise_approx = int(spec.double_noise_approx)
         d.accuracy_goal = float(spec.accuracy_goal)
         d.number_of_steps = int(spec.number_of_steps)
         d.oversampling = int(spec.oversampling)

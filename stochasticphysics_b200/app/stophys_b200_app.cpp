@@ -191,6 +191,10 @@ int solver_of(const std::string& s) {
     if (t == "millstein") return SP_SOLVER_MILLSTEIN;
     if (t == "implicit_midpoint") return SP_SOLVER_IMPLICIT_MIDPOINT;
     if (t == "eulermaruyama_normalized") return SP_SOLVER_EULER_MARUYAMA_NORMALIZED;
+    // SolverSettings.cpp:18-20
+    if (t == "heun_notconsistent") return SP_SOLVER_HEUN_NOT_CONSISTENT;
+    if (t == "weaktest") return SP_SOLVER_WEAK_TEST;
+    if (t == "explicitstrong_1.0") return SP_SOLVER_EXPLICIT_STRONG_1;
     throw std::runtime_error("unsupported Solver '" + s + "'");
 }
 
@@ -403,6 +407,11 @@ Run build(const std::string& path, unsigned long long seed, int precision) {
     d.solver = solver_of(Ini::str(need("Solver_Settings", "Solver")));
     d.max_iteration = opt("Solver_Settings", "Max_Iterations") ? static_cast<int32_t>(Ini::num(*opt("Solver_Settings", "Max_Iterations"))) : 20;
     d.accuracy_goal = opt("Solver_Settings", "Accuracy_Goal") ? Ini::num(*opt("Solver_Settings", "Accuracy_Goal")) : 1e-10;
+    // read only for the double-noise solvers (SolverSettings.h:113-116); the default is -1
+    d.double_noise_approx = -1;
+    if (d.solver == SP_SOLVER_WEAK_TEST || d.solver == SP_SOLVER_EXPLICIT_STRONG_1)
+        d.double_noise_approx =
+            static_cast<int32_t>(Ini::num(need("Solver_Settings", "Approximation_of_double_noise_integral")));
 
     // Problem_Settings (ProblemSettings.h:119-206)
     d.problem = problem_of(Ini::str(need("Problem_Settings", "Problem_type")));
@@ -676,7 +685,8 @@ void write_description(std::ostream& o, const Run& run) {
       << ",\"precision\":" << d.precision << ",\"n_particles\":" << n << ",\"number_of_steps\":" << d.number_of_steps
       << ",\"oversampling\":" << d.oversampling << ",\"timestep\":" << jnum(d.timestep)
       << ",\"temperature\":" << jnum(d.temperature) << ",\"max_iteration\":" << d.max_iteration
-      << ",\"accuracy_goal\":" << jnum(d.accuracy_goal) << ",\"field\":{\"type\":" << d.field.type << ",\"offset\":";
+      << ",\"accuracy_goal\":" << jnum(d.accuracy_goal) << ",\"double_noise_approx\":" << d.double_noise_approx
+      << ",\"field\":{\"type\":" << d.field.type << ",\"offset\":";
     jarr(o, d.field.offset, 3);
     o << ",\"amplitude\":";
     jarr(o, d.field.amplitude, 3);

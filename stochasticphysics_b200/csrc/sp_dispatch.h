@@ -17,18 +17,20 @@ struct KernelSet {
     const void* step_fn = nullptr;  // for cudaFuncGetAttributes / occupancy queries
 };
 
-// index: problem, anisotropy, solver slot (sp_solver, or kImplicitMidpointExact),
+// index: problem, anisotropy, solver slot (see solver_slot),
 // precision (0 FP64, 1 FP32), injected noise
 const KernelSet& kernel_set(int problem, int aniso, int solver, int precision, int inject);
-constexpr int kSolverSlots = 6;
+constexpr int kSolverSlots = 9;
 inline int kernel_index(int aniso, int solver, int precision, int inject) {
     return ((aniso * kSolverSlots + solver) * 2 + precision) * 2 + inject;
 }
 constexpr int kAnisoSlots = 3;
 constexpr int kKernelsPerProblem = kAnisoSlots * kSolverSlots * 2 * 2;
-// solver slot of a description: ImplicitMidpoint with SP_JACOBIAN_EXACT has its own kernels
+// solver slot of a description: sp_solver 0-4 as is, ImplicitMidpoint with
+// SP_JACOBIAN_EXACT in kImplicitMidpointExact, sp_solver 5-7 in slots 6-8
 inline int solver_slot(int solver, int jacobian) {
-    return (solver == kImplicitMidpoint && jacobian == 1) ? kImplicitMidpointExact : solver;
+    if (solver == kImplicitMidpoint && jacobian == 1) return kImplicitMidpointExact;
+    return solver >= 5 ? solver + 1 : solver;
 }
 
 void fill_neel(KernelSet* tab);

@@ -31,6 +31,8 @@ KernelSet make_set() {
         return k;  // not supported by the reference either
     } else if constexpr (SOLVER == kImplicitMidpointExact && !Prob::kHasExactJacobian) {
         return k;  // no analytic Newton matrix for this problem
+    } else if constexpr (SOLVER >= kHeunNotConsistent && INJ) {
+        return k;  // these take in-kernel noise only (their extra draws have no injection layout)
     } else {
         k.valid = true;
         k.D = Prob::D; k.Mn = Prob::Mn; k.OUT = Prob::OUT; k.P = ProblemOf<PROB, R, A>::P;
@@ -59,6 +61,9 @@ void fill_aniso(KernelSet* tab) {
     fill_solver<PROB, A, kImplicitMidpoint>(tab);
     fill_solver<PROB, A, kEulerMaruyamaNormalized>(tab);
     fill_solver<PROB, A, kImplicitMidpointExact>(tab);
+    fill_solver<PROB, A, kHeunNotConsistent>(tab);
+    fill_solver<PROB, A, kWeakTest>(tab);
+    fill_solver<PROB, A, kExplicitStrong1>(tab);
 }
 template <int PROB>
 void fill_problem(KernelSet* tab) {

@@ -289,7 +289,20 @@ __global__ void __launch_bounds__(kMaxBlock) step_kernel(const EnsDev* __restric
                         for (int j = 0; j < Mn; ++j) w[j] = w[j] * sqdt;
                     }
                     const R B[3] = {sB[i][0], sB[i][1], sB[i][2]};
-                    St::step(q, rot, y, B, w, dt, e.max_iter, e.tol, nc);
+                    if constexpr (SOLVER == kHeunNotConsistent) {
+                        R w2[Mn];
+                        philox_normals<R, Mn>(seed, pid, g, w2, 2u);
+#pragma unroll
+                        for (int j = 0; j < Mn; ++j) w2[j] = w2[j] * sqdt;
+                        St::step_heun_nc(q, rot, y, B, w, w2, dt);
+                    } else if constexpr (uses_double_noise(SOLVER)) {
+                        R A[Mn * (Mn - 1) / 2];
+                        double_noise_antisym<R, Mn>(seed, pid, g, e.dna, static_cast<R>(e.rho), sqdt, w, A);
+                        if constexpr (SOLVER == kWeakTest) St::step_weak(q, rot, y, B, w, A, dt, sqdt);
+                        else St::step_es1(q, rot, y, B, w, A, dt, sqdt);
+                    } else {
+                        St::step(q, rot, y, B, w, dt, e.max_iter, e.tol, nc);
+                    }
                     R o[OUT];
                     Prob::out(y, o);
 #pragma unroll

@@ -153,19 +153,21 @@ __device__ __forceinline__ void box_muller(uint4 w, int npairs, float* z) {
     }
 }
 
-// m unit normals (m = 3 or 6) for (seed, pid, step)
+// m unit normals (m = 3 or 6) for (seed, pid, step) from Philox calls call0 and
+// call0 + 1.  Calls 0-1 carry dW; Heun_NotConsistent's second increment takes
+// calls 2-3, the double-noise draws of WeakTest / ExplicitStrong_1.0 calls 2-166.
 template <class R, int Mdim>
 __device__ __forceinline__ void philox_normals(unsigned long long seed, unsigned long long pid, unsigned long long step,
-                                               R* z) {
+                                               R* z, uint32_t call0 = 0u) {
     R t[4];
-    box_muller(philox_block(seed, pid, step, 0u), 2, t);
+    box_muller(philox_block(seed, pid, step, call0), 2, t);
     z[0] = t[0];
     z[1] = t[1];
     z[2] = t[2];
     if (Mdim > 3) {
         z[3] = t[3];
         R u[4];
-        box_muller(philox_block(seed, pid, step, 1u), 1, u);
+        box_muller(philox_block(seed, pid, step, call0 + 1u), 1, u);
         z[4] = u[0];
         z[5] = u[1];
     }

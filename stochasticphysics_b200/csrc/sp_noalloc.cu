@@ -123,6 +123,7 @@ extern "C" SP_API sp_status sp_simulate_noalloc(const sp_ensemble_desc* desc, co
         e.dt = desc->timestep; e.sqrt_dt = std::sqrt(desc->timestep);
         e.field = field_params(desc->field);
         e.max_iter = desc->max_iteration; e.tol = desc->accuracy_goal;
+        e.dna = desc->double_noise_approx; e.rho = double_noise_rho(desc->double_noise_approx);
         const double kPi = 3.14159265358979323846;
         if (desc->problem == SP_PROBLEM_NEEL_SPHERICAL) {
             e.rot_brown = desc->problem_settings.use_coordinate_transformation;

@@ -728,6 +728,62 @@ __device__ __forceinline__ bool solve_small(R A[D][D], R* b, R* x) {
     return true;
 }
 
+// ------------------------------------------------------------ double noise matrix
+// Approximate double Stratonovich integrals J(j1, j2) of one step for WeakTest and
+// ExplicitStrong_1.0 (DoubleNoiseMatrix.h; Kloeden & Platen 1992, sec. 5.8).  The
+// symmetric part is dW_j1 dW_j2 / 2; the antisymmetric part A of each pair
+// j1 > j2 is, for order p >= 1,
+//   A = -1/(2 pi) sum_{r=1}^{p} 1/r [z1 (sqrt2 dW_j2 - z2) - z3 (sqrt2 dW_j1 - z4)]
+//       + rho_p (mu1 dW_j2 - mu2 dW_j1),
+// for p = 0 the rho term alone and for p = -1 zero.  As in the reference every
+// z and mu is a fresh N(0, dt) draw per pair (its generators advance on every
+// call).  Draws come from Philox calls 2, 3, ... of the step: per pair, one block
+// of four normals per r (z1..z4), then one block whose first two normals are mu1, mu2.
+// Pairs in the reference's loop order: j1 = Mn-1 .. 1, j2 = j1-1 .. 0.
+template <int Mn>
+__host__ __device__ constexpr int dn_pair(int j1, int j2) {
+    return (Mn - 1) * Mn / 2 - j1 * (j1 + 1) / 2 + (j1 - 1 - j2);
+}
+template <class R, int Mn>
+__device__ __forceinline__ void double_noise_antisym(unsigned long long seed, unsigned long long pid,
+                                                     unsigned long long step, int p, R rho, R sqdt, const R* w, R* A) {
+    const R kSqrt2 = R(1.4142135623730951), kInv2Pi = R(0.15915494309189535);
+    uint32_t call = 2u;
+#pragma unroll
+    for (int j1 = Mn - 1; j1 >= 1; --j1) {
+#pragma unroll
+        for (int j2 = j1 - 1; j2 >= 0; --j2) {
+            R t = R(0);
+            if (p >= 1) {
+                R s = R(0);
+                for (int r = 1; r <= p; ++r) {
+                    R z[4];
+                    box_muller(philox_block(seed, pid, step, call++), 2, z);
+                    const R z1 = z[0] * sqdt, z2 = z[1] * sqdt, z3 = z[2] * sqdt, z4 = z[3] * sqdt;
+                    s = s + (R(1) / R(r)) * (z1 * (kSqrt2 * w[j2] - z2) - z3 * (kSqrt2 * w[j1] - z4));
+                }
+                t = -s * kInv2Pi;
+            }
+            if (p >= 0) {
+                R u[4];
+                box_muller(philox_block(seed, pid, step, call++), 1, u);
+                t = t + rho * ((u[0] * sqdt) * w[j2] - (u[1] * sqdt) * w[j1]);
+            }
+            A[dn_pair<Mn>(j1, j2)] = t;
+        }
+    }
+}
+// column c of J: v[r] = J(r, c)
+template <class R, int Mn>
+__device__ __forceinline__ void dn_column(const R* w, const R* A, int c, R* v) {
+#pragma unroll
+    for (int r = 0; r < Mn; ++r) {
+        if (r == c) v[r] = (R(0.5) * w[r]) * w[r];
+        else if (r > c) v[r] = (R(0.5) * w[r]) * w[c] + A[dn_pair<Mn>(r, c)];
+        else v[r] = (R(0.5) * w[c]) * w[r] - A[dn_pair<Mn>(c, r)];
+    }
+}
+
 template <class P, class R, int SOLVER>
 struct Stepper {
     static constexpr int D = P::D, Mn = P::Mn;
@@ -840,6 +896,133 @@ struct Stepper {
                 for (int i = 0; i < D; ++i) y[i] = yj[i];
             }
         }
+    }
+
+    // Heun_NotConsistent.inl:35-47 (Stratonovich): the support point takes dW, the
+    // corrector the average of b at both points times an independent dW2.  Both
+    // points are evaluated in the chart prepareCalculations chose for y_n.
+    static __device__ __forceinline__ void step_heun_nc(const Par& q, const Rot<R>& rot, R* y, const R* B, const R* w,
+                                                        const R* w2, R dt) {
+        Cache c;
+        P::prepare(q, rot, y, c);
+        R a1[D], d[D], bw[D], s[D], b1[D];
+        P::det(q, y, c, B, a1);
+        P::drift(q, y, c, d);
+        P::bdw(q, y, c, w, bw);
+        P::bdw(q, y, c, w2, b1);
+#pragma unroll
+        for (int i = 0; i < D; ++i) {
+            a1[i] = a1[i] + d[i];
+            s[i] = (y[i] + a1[i] * dt) + bw[i];
+        }
+        P::recompute(q, s, c);
+        R a2[D], b2[D];
+        P::det(q, s, c, B, a2);
+        P::drift(q, s, c, d);
+        P::bdw(q, s, c, w2, b2);
+#pragma unroll
+        for (int i = 0; i < D; ++i) y[i] = (y[i] + (R(0.5) * ((a2[i] + d[i]) + a1[i])) * dt) + R(0.5) * (b2[i] + b1[i]);
+        P::finish(rot, y, c);
+    }
+
+    // b(y) e_j: column j of the noise matrix at the prepared point
+    static __device__ __forceinline__ void b_column(const Par& q, const R* y, const Cache& c, int j, R* col) {
+        R e[Mn];
+#pragma unroll
+        for (int k = 0; k < Mn; ++k) e[k] = R(k == j ? 1 : 0);
+        P::bdw(q, y, c, e, col);
+    }
+
+    // Explicit_Strong_1.inl:20-78: no drift correction; support points
+    // Y +- b_j sqrt(dt) around Y = y + a dt for the first D noise columns j, and
+    //   y' = Y + b dW + sum_j (b(Y + b_j sqrt dt) - b(Y - b_j sqrt dt)) J(:, j) / sqrt(dt).
+    static __device__ __forceinline__ void step_es1(const Par& q, const Rot<R>& rot, R* y, const R* B, const R* w,
+                                                    const R* A, R dt, R sqdt) {
+        Cache c;
+        P::prepare(q, rot, y, c);
+        R a[D], bw[D], t[D], acc[D];
+        P::det(q, y, c, B, a);
+        P::bdw(q, y, c, w, bw);
+#pragma unroll
+        for (int i = 0; i < D; ++i) { t[i] = y[i] + a[i] * dt; acc[i] = R(0); }
+#pragma unroll
+        for (int j = D - 1; j >= 0; --j) {
+            R col[D], v[Mn], sp[D], sm[D], bp[D], bm[D];
+            b_column(q, y, c, j, col);
+            dn_column<R, Mn>(w, A, j, v);
+#pragma unroll
+            for (int i = 0; i < D; ++i) { sp[i] = t[i] + col[i] * sqdt; sm[i] = t[i] - col[i] * sqdt; }
+            Cache cp = c, cm = c;
+            P::recompute(q, sp, cp);
+            P::recompute(q, sm, cm);
+            P::bdw(q, sp, cp, v, bp);
+            P::bdw(q, sm, cm, v, bm);
+#pragma unroll
+            for (int i = 0; i < D; ++i) acc[i] = acc[i] + (bp[i] - bm[i]);
+        }
+#pragma unroll
+        for (int i = 0; i < D; ++i) y[i] = acc[i] / sqdt + (t[i] + bw[i]);
+        P::finish(rot, y, c);
+    }
+
+    // WeakTest.inl:18-63: as ExplicitStrong_1.0 for the support points, plus the
+    // drift at Y + b dW, and a two-stage average:
+    //   T = (sum_j [(b(S+_j) - b(S-_j)) J(:, j) / sqrt(dt) + (b(S+_j) + b(S-_j)) dW]) / 4 + b dW / 2
+    //   y2 = y + a(Y + b dW) dt/2 + a dt/2 + T;   y' = y + a(y2) dt/2 + a dt/2 + T
+    static __device__ __forceinline__ void step_weak(const Par& q, const Rot<R>& rot, R* y, const R* B, const R* w,
+                                                     const R* A, R dt, R sqdt) {
+        Cache c;
+        P::prepare(q, rot, y, c);
+        R a[D], bw[D], adt[D], t[D], acc[D], ys[D], as[D];
+        P::det(q, y, c, B, a);
+        P::bdw(q, y, c, w, bw);
+#pragma unroll
+        for (int i = 0; i < D; ++i) {
+            adt[i] = a[i] * dt;
+            t[i] = y[i] + adt[i];
+            ys[i] = t[i] + bw[i];
+            acc[i] = R(0);
+        }
+        {
+            Cache cs = c;
+            P::recompute(q, ys, cs);
+            P::det(q, ys, cs, B, as);
+        }
+#pragma unroll
+        for (int j = D - 1; j >= 0; --j) {
+            R col[D], v[Mn], sp[D], sm[D], bpv[D], bmv[D], bpw[D], bmw[D];
+            b_column(q, y, c, j, col);
+            dn_column<R, Mn>(w, A, j, v);
+#pragma unroll
+            for (int i = 0; i < D; ++i) { sp[i] = t[i] + col[i] * sqdt; sm[i] = t[i] - col[i] * sqdt; }
+            Cache cp = c, cm = c;
+            P::recompute(q, sp, cp);
+            P::recompute(q, sm, cm);
+            P::bdw(q, sp, cp, v, bpv);
+            P::bdw(q, sm, cm, v, bmv);
+            P::bdw(q, sp, cp, w, bpw);
+            P::bdw(q, sm, cm, w, bmw);
+#pragma unroll
+            for (int i = 0; i < D; ++i) {
+                acc[i] = acc[i] + (bpv[i] - bmv[i]) / sqdt;
+                acc[i] = acc[i] + (bpw[i] + bmw[i]);
+            }
+        }
+        R y2[D];
+#pragma unroll
+        for (int i = 0; i < D; ++i) {
+            acc[i] = acc[i] / R(4) + R(0.5) * bw[i];
+            y2[i] = ((y[i] + (R(0.5) * as[i]) * dt) + R(0.5) * adt[i]) + acc[i];
+        }
+        R a2[D];
+        {
+            Cache c2 = c;
+            P::recompute(q, y2, c2);
+            P::det(q, y2, c2, B, a2);
+        }
+#pragma unroll
+        for (int i = 0; i < D; ++i) y[i] = ((y[i] + (R(0.5) * a2[i]) * dt) + R(0.5) * adt[i]) + acc[i];
+        P::finish(rot, y, c);
     }
 };
 

@@ -42,6 +42,16 @@ int noise_dim(int p) { return (p == 0 || p == 1) ? 3 : 6; }
 int out_dim(int p) { return p == 0 ? 3 : p == 1 ? 3 : p == 2 ? 9 : 6; }
 int param_count(int p, int aniso) { return param_count_of(p, aniso); }
 
+// sqrt(rho_p) of the double Stratonovich integral approximation (Kloeden & Platen
+// 1992, sec. 5.8): rho_p = 1/12 - 1/(2 pi^2) sum_{r=1}^{p} 1/r^2; p < 1 keeps 1/12
+// (DoubleNoiseMatrix.h sqrtpp<prec, p>)
+double double_noise_rho(int p) {
+    const double kPi = 3.14159265358979323846;
+    double s = 0.0;
+    for (int r = 1; r <= p; ++r) s += 1.0 / (static_cast<double>(r) * r);
+    return std::sqrt(1.0 / 12.0 - s / (2.0 * kPi * kPi));
+}
+
 // ------------------------------------------------------------------ validation
 sp_status validate_desc(const sp_ensemble_desc* d, std::string& why) {
     auto bad = [&](const std::string& m) { why = m; return SP_ERR_INVALID_ARG; };
@@ -49,7 +59,7 @@ sp_status validate_desc(const sp_ensemble_desc* d, std::string& why) {
     if (d->abi_version != SP_ABI_VERSION) return bad("abi_version mismatch");
     if (d->problem < 0 || d->problem > 3) return bad("unknown problem");
     if (d->anisotropy < 0 || d->anisotropy > 2) return bad("unknown anisotropy");
-    if (d->solver < 0 || d->solver > 4) return bad("unknown solver");
+    if (d->solver < 0 || d->solver > 7) return bad("unknown solver");
     if (d->precision < 0 || d->precision > 1) return bad("unknown precision");
     if (d->noise < 0 || d->noise > 1) return bad("unknown noise mode");
     if (d->field.type < 0 || d->field.type > 6) return bad("unknown field type");
@@ -108,6 +118,15 @@ sp_status validate_desc(const sp_ensemble_desc* d, std::string& why) {
         }
     }
     if (d->jacobian != SP_JACOBIAN_REFERENCE && d->jacobian != SP_JACOBIAN_EXACT) return bad("unknown jacobian mode");
+    if (d->solver >= SP_SOLVER_HEUN_NOT_CONSISTENT && d->noise == SP_NOISE_INJECTED) {
+        why = "Heun_NotConsistent, WeakTest and ExplicitStrong_1.0 draw extra normals per step and take in-kernel "
+              "(Philox) noise only";
+        return SP_ERR_UNSUPPORTED_COMBO;
+    }
+    // RuntimeDoubleNoiseMatrixSelection accepts -1..10 (SimulationManager.h:503-525)
+    if ((d->solver == SP_SOLVER_WEAK_TEST || d->solver == SP_SOLVER_EXPLICIT_STRONG_1) &&
+        (d->double_noise_approx < -1 || d->double_noise_approx > 10))
+        return bad("double_noise_approx must be in -1..10");
     const unsigned long long K = d->number_of_steps / d->oversampling;
     if (K > (1ull << 31)) return bad("too many samples");
     return SP_OK;
@@ -217,6 +236,7 @@ Ensemble::Ensemble(sp_context* c, const sp_ensemble_desc& d, const LaunchConfig&
     e.dt = d.timestep; e.sqrt_dt = std::sqrt(d.timestep);
     e.field = field_params(d.field);
     e.max_iter = d.max_iteration; e.tol = d.accuracy_goal;
+    e.dna = d.double_noise_approx; e.rho = double_noise_rho(d.double_noise_approx);
     const double kPi = 3.14159265358979323846;
     if (d.problem == SP_PROBLEM_NEEL_SPHERICAL) {
         e.rot_brown = d.problem_settings.use_coordinate_transformation;

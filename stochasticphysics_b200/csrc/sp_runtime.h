@@ -42,6 +42,7 @@ int state_dim(int p);
 int noise_dim(int p);
 int out_dim(int p);
 int param_count(int p, int aniso);
+double double_noise_rho(int p);
 FieldParams field_params(const sp_field_desc& f);
 void reference_times(unsigned long long K, unsigned long long W, double dt, double* times);
 

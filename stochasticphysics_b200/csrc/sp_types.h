@@ -28,6 +28,11 @@ enum AnisoId : int { kUniaxial = 0, kCubic = 1, kUniaxialCubic = 2 };
 enum SolverId : int { kEulerMaruyama = 0, kHeun = 1, kMillstein = 2, kImplicitMidpoint = 3, kEulerMaruyamaNormalized = 4 };
 // kernel-table slot of ImplicitMidpoint with the analytic Newton matrix (SP_JACOBIAN_EXACT)
 constexpr int kImplicitMidpointExact = 5;
+// kernel-table slots of SP_SOLVER_HEUN_NOT_CONSISTENT, _WEAK_TEST, _EXPLICIT_STRONG_1 (5, 6, 7)
+constexpr int kHeunNotConsistent = 6;
+constexpr int kWeakTest = 7;
+constexpr int kExplicitStrong1 = 8;
+constexpr bool uses_double_noise(int slot) { return slot == kWeakTest || slot == kExplicitStrong1; }
 
 // number of derived parameters per problem
 constexpr int kParamsNeel = 16;
@@ -78,6 +83,8 @@ struct EnsDev {
     FieldParams field;
     // solver / problem settings
     int max_iter;
+    int dna;        // WeakTest / ExplicitStrong_1: order p of the double-integral approximation
+    double rho;     // sqrt(1/12 - sum_{r<=p} 1/(2 pi^2 r^2)) (DoubleNoiseMatrix.h sqrtpp)
     int rot_brown;  // NeelSpherical: rotation enabled; BrownNeelEuler: Brown rotation enabled
     int rot_neel;   // BrownNeelEuler: Neel rotation enabled
     int slots;      // partial slots per chunk (max windows completing in a chunk)

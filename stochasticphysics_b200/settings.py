@@ -71,6 +71,7 @@ def spec_from_description(d: dict) -> EnsembleSpec:
                         tuple(f["phase"]), periode=float(f["periode"]), time_offset=float(f["time_offset"]),
                         tau=float(f["tau"]), alternating=bool(f["alternating"])),
         max_iteration=int(d["max_iteration"]), accuracy_goal=float(d["accuracy_goal"]),
+        double_noise_approx=int(d.get("double_noise_approx", -1)),
         use_coordinate_transformation=bool(q["use_coordinate_transformation"]),
         min_angle_before_transformation=float(q["min_angle_before_transformation"]),
         use_euler_coordinate_transformation=bool(q["use_euler_coordinate_transformation"]),

@@ -160,7 +160,8 @@ def test_spec_from_ini_builds_a_valid_description():
 
 
 @pytest.mark.parametrize("edit, message", [
-    (("'Heun_Strong'", "'WeakTest'"), "unsupported Solver 'WeakTest'"),
+    (("'Heun_Strong'", "'Implicit_Midpoint_GSL'"), "unsupported Solver 'Implicit_Midpoint_GSL'"),
+    (("'Heun_Strong'", "'WeakTest'"), "missing key Approximation_of_double_noise_integral"),
     (("Timestep = 2.0e-12", ""), "missing key Timestep"),
     (("'legacy_particle_large.ini'", "'no_such_particle.ini'"), "cannot open"),
     (("Type_of_field = 'sinusoidal'", "Type_of_field = 'sawtooth'"), "unsupported Type_of_field"),
@@ -176,6 +177,22 @@ def test_invalid_settings_are_reported(tmp_path, edit, message):
     bad.write_text(text.replace(edit[0], edit[1]))
     with pytest.raises(settings.SettingsError, match=message):
         settings.describe_ini(bad)
+
+
+@pytest.mark.parametrize("name, solver", [("WeakTest", Solver.WeakTest), ("ExplicitStrong_1.0", Solver.ExplicitStrong_1),
+                                          ("Heun_NotConsistent", Solver.Heun_NotConsistent)])
+def test_reference_disabled_solvers_parse(tmp_path, name, solver):
+    """SolverSettings.cpp:18-20 names; Approximation_of_double_noise_integral is read for
+    WeakTest and ExplicitStrong_1.0 only (SolverSettings.h:113-116), -1 otherwise."""
+    text = (INI / "legacy_neel_spherical.ini").read_text()
+    for f in ("legacy_particle_small.ini", "legacy_particle_large.ini"):
+        (tmp_path / f).write_text((INI / f).read_text())
+    text = text.replace("'Heun_Strong'", f"'{name}'\nApproximation_of_double_noise_integral = 3")
+    (tmp_path / "s.ini").write_text(text)
+    spec = settings.load_ini(tmp_path / "s.ini")
+    assert spec.solver == solver
+    assert spec.double_noise_approx == (-1 if solver == Solver.Heun_NotConsistent else 3)
+    assert load().sp_validate(DescHolder(spec).byref()) == 0, load().sp_last_error().decode()
 
 
 def test_system_matrix_voxels_and_fields():
