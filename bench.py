@@ -28,6 +28,8 @@ Heun) on the device-resident state, i.e. 2 x 65536 x 10000 particle-steps.
                ensemble), whole run on the device and end to end, beside the CPU
   stiff        the cubic ImplicitMidpoint workload (262144 particles, dt = 1e-10 s):
                FP64 with the reference's Newton matrix, FP64 and FP32 with the exact one
+  injected     injection mode (caller-supplied dW read from HBM every step), Neel Heun,
+               65536 particles, FP64 and FP32: particle-steps/s and dW GB/s vs HBM peak
   --impl reference  runs that CPU restatement as the reference arm
 
 Launch shapes come from the autotuner (sp_autotune) unless --no-autotune.
@@ -331,6 +333,48 @@ def stiff_leg(ctx, torch, n=262144, timed_steps=2000):
     return out
 
 
+def injected_leg(ctx, torch, n=65536, timed_steps=1000, warm_steps=100):
+    """Injection mode (Wiener increments supplied by the caller and read from HBM every
+    step, the parity mode): Neel Cartesian Heun, 65536 particles, FP64 (24 B of dW per
+    particle-step) and FP32 (12 B).  The dW array (steps x 3 x particles) is far larger
+    than L2, so each increment comes from HBM once.  Device-resident, CUDA-event timed
+    after a warm-up chunk; reports particle-steps/s and the dW read rate against the
+    measured HBM copy bandwidth."""
+    from stochasticphysics_b200 import provider
+    from stochasticphysics_b200._abi import Precision
+
+    hbm = None
+    try:
+        hbm = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()).get("hbm_gbs")
+    except (OSError, ValueError):
+        pass
+    base = provider.neel_relaxation(n=n, steps=timed_steps + warm_steps + 100, oversampling=100)
+    base = provider.with_injected_noise(base, seed=7)
+    out = {}
+    st = torch.cuda.Stream()
+    for prec in (Precision.FP64, Precision.FP32):
+        spec = dataclasses.replace(base, precision=prec)
+        with ctx.ensemble(spec) as e:
+            e.advance(warm_steps, st.cuda_stream)
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(st)
+            e.advance(timed_steps, st.cuda_stream)
+            b.record(st)
+            torch.cuda.synchronize()
+        sec = a.elapsed_time(b) / 1e3
+        ps = n * timed_steps / sec
+        dw_bytes = 3 * (8 if prec == Precision.FP64 else 4)
+        gbs = ps * dw_bytes / 1e9
+        out[prec.name] = {"value": ps, "unit": UNIT, "dw_bytes_per_particle_step": dw_bytes, "dw_read_gbs": gbs,
+                          "hbm_frac": None if not hbm else gbs / hbm}
+    out["hbm_peak_gbs"] = hbm
+    out["hbm_peak_source"] = "MEASURED_PEAKS.json hbm_gbs (copy bandwidth)"
+    out["workload"] = (f"neel_relaxation with injected dW: Neel, Heun, {n} particles, {timed_steps} timed steps "
+                       f"({3 * n * (timed_steps + warm_steps) * 8 / 1e9:.2f} GB of FP64 dW on the device)")
+    return out
+
+
 def cpu_baseline(steps_sample=2000, n=None):
     """The CPU oracle on all host cores for a bounded sample of the workload."""
     import oracle
@@ -442,6 +486,7 @@ def main():
                     help="scale of the request step counts (S ~ logU[1e5, 1e7] x scale)")
     ap.add_argument("--batched-sets", type=int, default=256, help="parameter sets of the batched leg (0: skip)")
     ap.add_argument("--no-stiff", action="store_true", help="skip the stiff ImplicitMidpoint leg")
+    ap.add_argument("--no-injected", action="store_true", help="skip the injected-noise (HBM) leg")
     ap.add_argument("--batched-step-scale", type=float, default=0.02,
                     help="scale of the batched sets' step counts (S ~ logU[1e5, 1e7] x scale)")
     args = ap.parse_args()
@@ -539,6 +584,7 @@ def main():
         if world == 1 and args.batched_sets > 0:
             batched = batched_leg(ctx, args.batched_sets, args.batched_step_scale)
         stiff = None if (world > 1 or args.no_stiff) else stiff_leg(ctx, torch)
+        injected = None if (world > 1 or args.no_injected) else injected_leg(ctx, torch)
         plain_neel = None if (world > 1 or args.no_cpu_baseline) else plain_neel_leg(ctx, torch)
 
     if rank == 0:
@@ -592,6 +638,7 @@ def main():
             "serving": serving,
             "batched": batched,
             "stiff": stiff,
+            "injected": injected,
             "plain_neel_1024": plain_neel,
         }
         print(json.dumps(line), flush=True)
