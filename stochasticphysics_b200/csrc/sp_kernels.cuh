@@ -264,6 +264,8 @@ __global__ void __launch_bounds__(kMaxBlock) step_kernel(const EnsDev* __restric
             q = Prob::load(static_cast<const R*>(e.params), Np, td.first);  // any valid slot; results are discarded
         }
         NewtonCount nc{0u, 0u};
+        typename Prob::Trig tr;  // sincos of y, carried from each step's output to the next prepare
+        Prob::trig(y, tr);
         // W < 2^31 (validated); the window position fits 32 bits.  Values used only
         // at a window end (once per W steps) are re-read there instead of being kept
         // live in registers across the step loop.
@@ -294,17 +296,17 @@ __global__ void __launch_bounds__(kMaxBlock) step_kernel(const EnsDev* __restric
                         philox_normals<R, Mn>(seed, pid, g, w2, 2u);
 #pragma unroll
                         for (int j = 0; j < Mn; ++j) w2[j] = w2[j] * sqdt;
-                        St::step_heun_nc(q, rot, y, B, w, w2, dt);
+                        St::step_heun_nc(q, rot, y, B, w, w2, dt, tr);
                     } else if constexpr (uses_double_noise(SOLVER)) {
                         R A[Mn * (Mn - 1) / 2];
                         double_noise_antisym<R, Mn>(seed, pid, g, e.dna, static_cast<R>(e.rho), sqdt, w, A);
-                        if constexpr (SOLVER == kWeakTest) St::step_weak(q, rot, y, B, w, A, dt, sqdt);
-                        else St::step_es1(q, rot, y, B, w, A, dt, sqdt);
+                        if constexpr (SOLVER == kWeakTest) St::step_weak(q, rot, y, B, w, A, dt, sqdt, tr);
+                        else St::step_es1(q, rot, y, B, w, A, dt, sqdt, tr);
                     } else {
-                        St::step(q, rot, y, B, w, dt, e.max_iter, e.tol, nc);
+                        St::step(q, rot, y, B, w, dt, e.max_iter, e.tol, nc, tr);
                     }
                     R o[OUT];
-                    Prob::out(y, o);
+                    Prob::out_t(y, o, tr);
 #pragma unroll
                     for (int c = 0; c < OUT; ++c) {  // Kahan summation (SingleParticleSimulator.h:148-153)
                         const R yv = o[c] - comp[c];

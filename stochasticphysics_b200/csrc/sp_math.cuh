@@ -15,10 +15,37 @@ namespace sp {
 
 template <class R> struct M;
 
+// The FP64 step kernels are bound by instruction fetch: every inlined copy of a double
+// transcendental adds a few hundred bytes of code to the step loop.  Their sines and
+// cosines and their Box-Muller pairs are therefore one shared, called routine each
+// (results are those of the same library calls).
+struct SinCosD {
+    double s, c;
+};
+static __device__ __noinline__ SinCosD sincos_d(double x) {
+    SinCosD r;
+    ::sincos(x, &r.s, &r.c);
+    return r;
+}
+// one Box-Muller pair on the words (a, b): u = (w + 1/2) 2^-32, r = sqrt(-2 ln u_a),
+// (r cos 2 pi u_b, r sin 2 pi u_b)
+static __device__ __noinline__ SinCosD box_muller_pair_d(uint32_t a, uint32_t b) {
+    const double inv = 2.3283064365386963e-10, half = 1.1641532182693481e-10;  // 2^-32, 2^-33
+    const double u0 = fma(static_cast<double>(a), inv, half), u1 = fma(static_cast<double>(b), inv, half);
+    const double r = ::sqrt(-2.0 * ::log(u0));
+    double s, c;
+    ::sincospi(2.0 * u1, &s, &c);
+    return SinCosD{r * s, r * c};
+}
+
 template <> struct M<double> {
     static __device__ __forceinline__ double sin(double x) { return ::sin(x); }
     static __device__ __forceinline__ double cos(double x) { return ::cos(x); }
-    static __device__ __forceinline__ void sincos(double x, double* s, double* c) { ::sincos(x, s, c); }
+    static __device__ __forceinline__ void sincos(double x, double* s, double* c) {
+        const SinCosD r = sincos_d(x);
+        *s = r.s;
+        *c = r.c;
+    }
     static __device__ __forceinline__ double acos(double x) { return ::acos(x); }
     static __device__ __forceinline__ double atan2(double y, double x) { return ::atan2(y, x); }
     static __device__ __forceinline__ double fmod(double x, double y) { return ::fmod(x, y); }
@@ -106,22 +133,13 @@ __device__ __forceinline__ uint4 philox_block(unsigned long long seed, unsigned 
 
 // Box-Muller on u = (w + 1/2) 2^-32.  npairs = 1 or 2 pairs of normals.
 __device__ __forceinline__ void box_muller(uint4 w, int npairs, double* z) {
-    const double inv = 2.3283064365386963e-10, half = 1.1641532182693481e-10;  // 2^-32, 2^-33
-    {
-        const double u0 = fma(static_cast<double>(w.x), inv, half), u1 = fma(static_cast<double>(w.y), inv, half);
-        const double r = ::sqrt(-2.0 * ::log(u0));
-        double s, c;
-        ::sincospi(2.0 * u1, &s, &c);
-        z[0] = r * c;
-        z[1] = r * s;
-    }
+    const SinCosD p = box_muller_pair_d(w.x, w.y);
+    z[0] = p.c;
+    z[1] = p.s;
     if (npairs > 1) {
-        const double u2 = fma(static_cast<double>(w.z), inv, half), u3 = fma(static_cast<double>(w.w), inv, half);
-        const double r = ::sqrt(-2.0 * ::log(u2));
-        double s, c;
-        ::sincospi(2.0 * u3, &s, &c);
-        z[2] = r * c;
-        z[3] = r * s;
+        const SinCosD q = box_muller_pair_d(w.z, w.w);
+        z[2] = q.c;
+        z[3] = q.s;
     }
 }
 // sqrt of -2 ln u as x * rsqrt(x) on the SFU (rsqrt.approx, ~1 ulp).  In FP32,

@@ -28,6 +28,68 @@ struct Rot {
     R min1, max1, min2, max2;
 };
 
+// ------------------------------------------------------------------ chart rotations
+// A chart rotation (coordinates within the configured angle of a pole) happens on few
+// steps.  In the FP64 kernels its transcendental code is called, not inlined, so the
+// per-step loop stays small enough for the instruction cache; FP32 inlines it.  The
+// rotations return the new angles with their sines and cosines (what prepare needs next).
+template <class R>
+struct SphRot {
+    R t, p, st, ct, sp, cp;
+};
+// NeelRelaxationSpherical.h:568-602 (INV: the inverse rotation)
+template <class R, bool INV>
+__device__ __forceinline__ SphRot<R> sph_rotate_impl(R t0, R p0) {
+    R st, ct, sp, cp;
+    M<R>::sincos(t0, &st, &ct);
+    M<R>::sincos(p0, &sp, &cp);
+    SphRot<R> r;
+    if constexpr (!INV) {
+        r.t = M<R>::acos(-cp * st); r.p = M<R>::atan2(sp * st, ct);
+    } else {
+        r.t = M<R>::acos(cp * st); r.p = M<R>::atan2(sp * st, -ct);
+    }
+    M<R>::sincos(r.t, &r.st, &r.ct);
+    M<R>::sincos(r.p, &r.sp, &r.cp);
+    return r;
+}
+template <class R, bool INV>
+__device__ __noinline__ SphRot<R> sph_rotate_cold(R t0, R p0) { return sph_rotate_impl<R, INV>(t0, p0); }
+template <class R, bool INV>
+__device__ __forceinline__ SphRot<R> sph_rotate(R t0, R p0) {
+    if constexpr (sizeof(R) == 8) return sph_rotate_cold<R, INV>(t0, p0);
+    else return sph_rotate_impl<R, INV>(t0, p0);
+}
+template <class R>
+struct EulerRot {
+    R e0, e1, e2, s0, s1, s2, c0, c1, c2;
+};
+// BrownAndNeelRelaxationEulerSpherical.h:859-899 (INV: the inverse rotation)
+template <class R, bool INV>
+__device__ __forceinline__ EulerRot<R> euler_rotate_impl(R a0, R a1, R a2) {
+    R S0, C0, S1, C1, S2, C2;
+    M<R>::sincos(a0, &S0, &C0); M<R>::sincos(a1, &S1, &C1); M<R>::sincos(a2, &S2, &C2);
+    EulerRot<R> r;
+    if constexpr (!INV) {
+        r.e0 = M<R>::atan2(-C2 * C0 + C1 * S0 * S2, S0 * C2 + C1 * C0 * S2);
+        r.e1 = M<R>::acos(-S1 * S2);
+        r.e2 = M<R>::atan2(C1, C2 * S1);
+    } else {
+        r.e0 = M<R>::atan2(C0 * C2 - C1 * S0 * S2, -C2 * S0 - C1 * C0 * S2);
+        r.e1 = M<R>::acos(S1 * S2);
+        r.e2 = M<R>::atan2(-C1, C2 * S1);
+    }
+    M<R>::sincos(r.e0, &r.s0, &r.c0); M<R>::sincos(r.e1, &r.s1, &r.c1); M<R>::sincos(r.e2, &r.s2, &r.c2);
+    return r;
+}
+template <class R, bool INV>
+__device__ __noinline__ EulerRot<R> euler_rotate_cold(R a0, R a1, R a2) { return euler_rotate_impl<R, INV>(a0, a1, a2); }
+template <class R, bool INV>
+__device__ __forceinline__ EulerRot<R> euler_rotate(R a0, R a1, R a2) {
+    if constexpr (sizeof(R) == 8) return euler_rotate_cold<R, INV>(a0, a1, a2);
+    else return euler_rotate_impl<R, INV>(a0, a1, a2);
+}
+
 // ------------------------------------------------------------------ anisotropy
 template <class R, int A>
 struct Aniso {
@@ -141,6 +203,13 @@ struct NeelCart {
         r[0] = o.x; r[1] = o.y; r[2] = o.z;
     }
     static __device__ __forceinline__ void out(const R* y, R* o) { o[0] = y[0]; o[1] = y[1]; o[2] = y[2]; }
+    // no angles: nothing to carry from one step's output to the next step's prepare
+    struct Trig {};
+    static __device__ __forceinline__ void trig(const R*, Trig&) {}
+    static __device__ __forceinline__ void out_t(const R* y, R* o, Trig&) { out(y, o); }
+    static __device__ __forceinline__ void prepare_t(const Par& q, const Rot<R>& r, R* y, Cache& c, const Trig&) {
+        prepare(q, r, y, c);
+    }
     // NeelRelaxation.h:204-208: m / |m| (Eigen normalize: unchanged when |m| = 0)
     static __device__ __forceinline__ void normalize(R* y) {
         const R n2 = (y[0] * y[0] + y[1] * y[1]) + y[2] * y[2];
@@ -261,18 +330,12 @@ struct NeelSph {
     }
     // NeelRelaxationSpherical.h:568-602
     static __device__ __forceinline__ void rotate(R* y) {
-        R st, ct, sp, cp;
-        M<R>::sincos(y[0], &st, &ct);
-        M<R>::sincos(y[1], &sp, &cp);
-        const R t = M<R>::acos(-cp * st), p = M<R>::atan2(sp * st, ct);
-        y[0] = t; y[1] = p;
+        const SphRot<R> r = sph_rotate<R, false>(y[0], y[1]);
+        y[0] = r.t; y[1] = r.p;
     }
     static __device__ __forceinline__ void unrotate(R* y) {
-        R st, ct, sp, cp;
-        M<R>::sincos(y[0], &st, &ct);
-        M<R>::sincos(y[1], &sp, &cp);
-        const R t = M<R>::acos(cp * st), p = M<R>::atan2(sp * st, -ct);
-        y[0] = t; y[1] = p;
+        const SphRot<R> r = sph_rotate<R, true>(y[0], y[1]);
+        y[0] = r.t; y[1] = r.p;
     }
     // :124-237
     static __device__ __forceinline__ void prepare(const Par& q, const Rot<R>& r, R* y, Cache& c) {
@@ -284,6 +347,33 @@ struct NeelSph {
         R st, ct, sp, cp;
         M<R>::sincos(y[0], &st, &ct);
         M<R>::sincos(y[1], &sp, &cp);
+        cache_from(q, st, ct, sp, cp, c);
+    }
+    // sines and cosines of theta and phi of the state the previous step ended in: the
+    // output of step n is evaluated at exactly the state step n+1 prepares, so its
+    // sincos are reused whenever prepare keeps the chart (bit-identical to recomputing)
+    struct Trig {
+        R st, ct, sp, cp;
+    };
+    static __device__ __forceinline__ void trig(const R* y, Trig& t) {
+        M<R>::sincos(y[0], &t.st, &t.ct);
+        M<R>::sincos(y[1], &t.sp, &t.cp);
+    }
+    static __device__ __forceinline__ void out_t(const R* y, R* o, Trig& t) {
+        trig(y, t);
+        o[0] = t.st * t.cp; o[1] = t.st * t.sp; o[2] = t.ct;
+    }
+    static __device__ __forceinline__ void prepare_t(const Par& q, const Rot<R>& r, R* y, Cache& c, const Trig& t) {
+        c.rot = r.rb && (y[0] < r.min1 || y[0] > r.max1);
+        if (c.rot) {
+            const SphRot<R> n = sph_rotate<R, false>(y[0], y[1]);
+            y[0] = n.t; y[1] = n.p;
+            cache_from(q, n.st, n.ct, n.sp, n.cp, c);
+        } else {
+            cache_from(q, t.st, t.ct, t.sp, t.cp, c);
+        }
+    }
+    static __device__ __forceinline__ void cache_from(const Par& q, R st, R ct, R sp, R cp, Cache& c) {
         c.st = st; c.ct = ct;
         R odst = M<R>::inv_sin(st);
         if (M<R>::isinf(odst)) odst = R(0);
@@ -384,6 +474,48 @@ struct NeelSph {
     }
 };
 
+// BrownAndNeelRelaxationEulerSpherical.h:559-594: the drift when exactly one of the two
+// charts is rotated (a rare step; called, not inlined, in FP64)
+template <class R>
+__device__ __forceinline__ V3<R> be_drift_mixed_impl(bool br, R adDN2, R d2fDN2, R cF2h, R csc, R ctheta, R cpsi,
+                                                     R spsi, R cos_t, R cos_p, R sin_t, R sin_p) {
+    const R cotb = csc * ctheta;
+    V3<R> r;
+    const R sin_2t = R(2) * cos_t * sin_t;
+    const R sin_t_2 = sin_t * sin_t;
+    const R cpsi_2 = cpsi * cpsi, spsi_2 = spsi * spsi;
+    const R c2psi = cpsi_2 - spsi_2, s2psi = R(2) * cpsi * spsi;
+    const R sin_2p = R(2) * cos_p * sin_p;
+    const R cos_t_2 = cos_t * cos_t, sin_p_2 = sin_p * sin_p, cos_p_2 = cos_p * cos_p;
+    if (br) {  // :559-576
+        r.x = csc * (adDN2 * (-spsi * cos_t + sin_p * cpsi * sin_t) +
+                      R(2) * d2fDN2 * (-c2psi * cotb * sin_2t * sin_p + cos_p * sin_t * (cos_t * cpsi + sin_t * sin_p * spsi) +
+                                         cotb * s2psi * (cos_t_2 - sin_t_2 * sin_p_2)));
+        r.y = cF2h * cotb + adDN2 * (-cos_t * cpsi - spsi * sin_t * sin_p) +
+               d2fDN2 * (R(2) * cpsi_2 * cotb * (cos_t_2 + cos_p_2 * sin_t_2) + cpsi * sin_t_2 * sin_2p +
+                           R(2) * spsi * (-sin_t * cos_t * cos_p + cotb * sin_t_2 * spsi) + cotb * sin_2t * sin_p * s2psi);
+        r.z = adDN2 * (sin_t * cos_p - cpsi * cotb * sin_t * sin_p + cotb * cos_t * spsi) -
+               d2fDN2 * (cos_t * cpsi + sin_t * sin_p * spsi) *
+                   (R(2) * cos_p * cotb * sin_t - (R(3) + c2psi) * csc * csc * (cpsi * sin_t * sin_p - cos_t * spsi));
+    } else {  // only Neel rotated, :577-594
+        r.x = csc * (adDN2 * (spsi * cos_t + sin_p * cpsi * sin_t) +
+                      R(2) * d2fDN2 * (c2psi * cotb * sin_2t * sin_p + cos_p * sin_t * (cos_t * cpsi - sin_t * sin_p * spsi) +
+                                         cotb * s2psi * (cos_t_2 - sin_t_2 * sin_p_2)));
+        r.y = cF2h * cotb + adDN2 * (cos_t * cpsi - spsi * sin_t * sin_p) +
+               d2fDN2 * (R(2) * cpsi_2 * cotb * (cos_t_2 + cos_p_2 * sin_t_2) - cpsi * sin_t_2 * sin_2p +
+                           R(2) * spsi * (-sin_t * cos_t * cos_p + cotb * sin_t_2 * spsi) - cotb * sin_2t * sin_p * s2psi);
+        r.z = adDN2 * (-sin_t * cos_p - cpsi * cotb * sin_t * sin_p - cotb * cos_t * spsi) -
+               d2fDN2 * (cos_t * cpsi - sin_t * sin_p * spsi) *
+                   (R(2) * cos_p * cotb * sin_t + (R(3) + c2psi) * csc * csc * (cpsi * sin_t * sin_p + cos_t * spsi));
+    }
+    return r;
+}
+template <class R>
+__device__ __noinline__ V3<R> be_drift_mixed_cold(bool br, R adDN2, R d2fDN2, R cF2h, R csc, R ctheta, R cpsi, R spsi,
+                                                  R cos_t, R cos_p, R sin_t, R sin_p) {
+    return be_drift_mixed_impl<R>(br, adDN2, d2fDN2, cF2h, csc, ctheta, cpsi, spsi, cos_t, cos_p, sin_t, sin_p);
+}
+
 // ======================================================================= Brown + Neel, Euler/spherical
 template <class R, int A>
 struct BrownNeelEuler {
@@ -417,20 +549,12 @@ struct BrownNeelEuler {
     }
     // :859-899
     static __device__ __forceinline__ void euler_rotate(R* e) {
-        R S0, C0, S1, C1, S2, C2;
-        M<R>::sincos(e[0], &S0, &C0); M<R>::sincos(e[1], &S1, &C1); M<R>::sincos(e[2], &S2, &C2);
-        const R np = M<R>::atan2(-C2 * C0 + C1 * S0 * S2, S0 * C2 + C1 * C0 * S2);
-        const R nt = M<R>::acos(-S1 * S2);
-        const R ns = M<R>::atan2(C1, C2 * S1);
-        e[0] = np; e[1] = nt; e[2] = ns;
+        const EulerRot<R> r = sp::euler_rotate<R, false>(e[0], e[1], e[2]);
+        e[0] = r.e0; e[1] = r.e1; e[2] = r.e2;
     }
     static __device__ __forceinline__ void euler_unrotate(R* e) {
-        R S0, C0, S1, C1, S2, C2;
-        M<R>::sincos(e[0], &S0, &C0); M<R>::sincos(e[1], &S1, &C1); M<R>::sincos(e[2], &S2, &C2);
-        const R np = M<R>::atan2(C0 * C2 - C1 * S0 * S2, -C2 * S0 - C1 * C0 * S2);
-        const R nt = M<R>::acos(S1 * S2);
-        const R ns = M<R>::atan2(-C1, C2 * S1);
-        e[0] = np; e[1] = nt; e[2] = ns;
+        const EulerRot<R> r = sp::euler_rotate<R, true>(e[0], e[1], e[2]);
+        e[0] = r.e0; e[1] = r.e1; e[2] = r.e2;
     }
     static __device__ __forceinline__ void neel_rotate(R* y) { NeelSph<R, A>::rotate(y); }
     static __device__ __forceinline__ void neel_unrotate(R* y) { NeelSph<R, A>::unrotate(y); }
@@ -447,6 +571,41 @@ struct BrownNeelEuler {
     static __device__ __forceinline__ void recompute(const Par&, const R* y, Cache& c) {
 #pragma unroll
         for (int i = 0; i < 5; ++i) M<R>::sincos(y[i], &c.S[i], &c.C[i]);
+        cache_from(c);
+    }
+    // sines and cosines of the five angles the previous step ended in (its output is
+    // evaluated there); reused by prepare for every angle whose chart it keeps
+    struct Trig {
+        R S[5], C[5];
+    };
+    static __device__ __forceinline__ void trig(const R* y, Trig& t) {
+#pragma unroll
+        for (int i = 0; i < 5; ++i) M<R>::sincos(y[i], &t.S[i], &t.C[i]);
+    }
+    static __device__ __forceinline__ void prepare_t(const Par&, const Rot<R>& r, R* y, Cache& c, const Trig& t) {
+        const R tb = M<R>::abs(y[1]);
+        c.br = r.rb && (tb < r.min1 || tb > r.max1);
+        if (c.br) {
+            const EulerRot<R> n = sp::euler_rotate<R, false>(y[0], y[1], y[2]);
+            y[0] = n.e0; y[1] = n.e1; y[2] = n.e2;
+            c.S[0] = n.s0; c.S[1] = n.s1; c.S[2] = n.s2; c.C[0] = n.c0; c.C[1] = n.c1; c.C[2] = n.c2;
+        } else {
+#pragma unroll
+            for (int i = 0; i < 3; ++i) { c.S[i] = t.S[i]; c.C[i] = t.C[i]; }
+        }
+        const R tn = M<R>::abs(y[3]);
+        c.nr = r.rn && (tn < r.min2 || tn > r.max2);
+        if (c.nr) {
+            const SphRot<R> n = sph_rotate<R, false>(y[3], y[4]);
+            y[3] = n.t; y[4] = n.p;
+            c.S[3] = n.st; c.C[3] = n.ct; c.S[4] = n.sp; c.C[4] = n.cp;
+        } else {
+#pragma unroll
+            for (int i = 3; i < 5; ++i) { c.S[i] = t.S[i]; c.C[i] = t.C[i]; }
+        }
+        cache_from(c);
+    }
+    static __device__ __forceinline__ void cache_from(Cache& c) {
         R csc = M<R>::inv_sin(c.S[1]);
         if (M<R>::isinf(csc)) csc = R(0);
         c.csc = csc;
@@ -570,46 +729,29 @@ struct BrownNeelEuler {
             r[2] = -(q.adDN2 * (cos_t + sin_t * cotb * sph) -
                      q.d2fDN2 * sin_t * (R(2) * cos_t * cotb * cph + (R(-1) + R(2) * csc * csc) * sin_t * s2));
         } else {
-            const R sin_2t = R(2) * cos_t * sin_t;
-            const R sin_t_2 = sin_t * sin_t;
-            const R cpsi_2 = cpsi * cpsi, spsi_2 = spsi * spsi;
-            const R c2psi = cpsi_2 - spsi_2, s2psi = R(2) * cpsi * spsi;
-            const R sin_2p = R(2) * cos_p * sin_p;
-            const R cos_t_2 = cos_t * cos_t, sin_p_2 = sin_p * sin_p, cos_p_2 = cos_p * cos_p;
-            if (c.br) {  // :559-576
-                r[0] = csc * (q.adDN2 * (-spsi * cos_t + sin_p * cpsi * sin_t) +
-                              R(2) * q.d2fDN2 * (-c2psi * cotb * sin_2t * sin_p + cos_p * sin_t * (cos_t * cpsi + sin_t * sin_p * spsi) +
-                                                 cotb * s2psi * (cos_t_2 - sin_t_2 * sin_p_2)));
-                r[1] = q.cF2h * cotb + q.adDN2 * (-cos_t * cpsi - spsi * sin_t * sin_p) +
-                       q.d2fDN2 * (R(2) * cpsi_2 * cotb * (cos_t_2 + cos_p_2 * sin_t_2) + cpsi * sin_t_2 * sin_2p +
-                                   R(2) * spsi * (-sin_t * cos_t * cos_p + cotb * sin_t_2 * spsi) + cotb * sin_2t * sin_p * s2psi);
-                r[2] = q.adDN2 * (sin_t * cos_p - cpsi * cotb * sin_t * sin_p + cotb * cos_t * spsi) -
-                       q.d2fDN2 * (cos_t * cpsi + sin_t * sin_p * spsi) *
-                           (R(2) * cos_p * cotb * sin_t - (R(3) + c2psi) * csc * csc * (cpsi * sin_t * sin_p - cos_t * spsi));
-            } else {  // only Neel rotated, :577-594
-                r[0] = csc * (q.adDN2 * (spsi * cos_t + sin_p * cpsi * sin_t) +
-                              R(2) * q.d2fDN2 * (c2psi * cotb * sin_2t * sin_p + cos_p * sin_t * (cos_t * cpsi - sin_t * sin_p * spsi) +
-                                                 cotb * s2psi * (cos_t_2 - sin_t_2 * sin_p_2)));
-                r[1] = q.cF2h * cotb + q.adDN2 * (cos_t * cpsi - spsi * sin_t * sin_p) +
-                       q.d2fDN2 * (R(2) * cpsi_2 * cotb * (cos_t_2 + cos_p_2 * sin_t_2) - cpsi * sin_t_2 * sin_2p +
-                                   R(2) * spsi * (-sin_t * cos_t * cos_p + cotb * sin_t_2 * spsi) - cotb * sin_2t * sin_p * s2psi);
-                r[2] = q.adDN2 * (-sin_t * cos_p - cpsi * cotb * sin_t * sin_p - cotb * cos_t * spsi) -
-                       q.d2fDN2 * (cos_t * cpsi - sin_t * sin_p * spsi) *
-                           (R(2) * cos_p * cotb * sin_t + (R(3) + c2psi) * csc * csc * (cpsi * sin_t * sin_p + cos_t * spsi));
-            }
+            V3<R> m;
+            if constexpr (sizeof(R) == 8)
+                m = be_drift_mixed_cold<R>(c.br, q.adDN2, q.d2fDN2, q.cF2h, csc, ctheta, cpsi, spsi, cos_t, cos_p, sin_t, sin_p);
+            else
+                m = be_drift_mixed_impl<R>(c.br, q.adDN2, q.d2fDN2, q.cF2h, csc, ctheta, cpsi, spsi, cos_t, cos_p, sin_t, sin_p);
+            r[0] = m.x; r[1] = m.y; r[2] = m.z;
         }
         r[3] = q.nd * c.odst * cos_t;  // :597
         r[4] = R(0);
     }
     // :673-735: x-axis, y-axis, magnetisation
-    static __device__ __forceinline__ void out(const R* y, R* o) {
-        R s[5], c[5];
-#pragma unroll
-        for (int i = 0; i < 5; ++i) M<R>::sincos(y[i], &s[i], &c[i]);
+    static __device__ __forceinline__ void out_t(const R* y, R* o, Trig& t) {
+        trig(y, t);
+        const R* s = t.S;
+        const R* c = t.C;
         const R cphicpsi = c[0] * c[2], sphicpsi = s[0] * c[2], cphispsi = c[0] * s[2], sphispsi = s[0] * s[2];
         o[0] = cphicpsi - c[1] * sphispsi; o[1] = c[1] * sphicpsi + cphispsi; o[2] = s[1] * s[0];
         o[3] = -sphicpsi - c[1] * cphispsi; o[4] = c[1] * cphicpsi - sphispsi; o[5] = s[1] * c[0];
         o[6] = s[3] * c[4]; o[7] = s[3] * s[4]; o[8] = c[3];
+    }
+    static __device__ __forceinline__ void out(const R* y, R* o) {
+        Trig t;
+        out_t(y, o, t);
     }
     static __device__ __forceinline__ void normalize(R*) {}  // BrownAndNeelRelaxationEulerSpherical.h:738-741
     static __device__ __forceinline__ void newton_matrix(const Par&, const R*, const Cache&, const R*, const R*, R,
@@ -672,6 +814,12 @@ struct BrownNeelCart {
     static __device__ __forceinline__ void out(const R* y, R* o) {
 #pragma unroll
         for (int i = 0; i < 6; ++i) o[i] = y[i];
+    }
+    struct Trig {};
+    static __device__ __forceinline__ void trig(const R*, Trig&) {}
+    static __device__ __forceinline__ void out_t(const R* y, R* o, Trig&) { out(y, o); }
+    static __device__ __forceinline__ void prepare_t(const Par& q, const Rot<R>& r, R* y, Cache& c, const Trig&) {
+        prepare(q, r, y, c);
     }
     // BrownAndNeelRelaxation.h:168-172: n and m normalised separately
     static __device__ __forceinline__ void normalize(R* y) {
@@ -789,12 +937,14 @@ struct Stepper {
     static constexpr int D = P::D, Mn = P::Mn;
     using Par = typename P::Par;
     using Cache = typename P::Cache;
+    using Trig = typename P::Trig;
 
+    // tr: sines and cosines of y (from the previous step's output), reused by prepare_t
     static __device__ __forceinline__ void step(const Par& q, const Rot<R>& rot, R* y, const R* B, const R* w, R dt,
-                                                int max_iter, double tol, NewtonCount& nc) {
+                                                int max_iter, double tol, NewtonCount& nc, const Trig& tr) {
         if constexpr (SOLVER == kEulerMaruyama) {
             Cache c;
-            P::prepare(q, rot, y, c);
+            P::prepare_t(q, rot, y, c, tr);
             R a[D], d[D], bw[D];
             P::det(q, y, c, B, a);
             P::drift(q, y, c, d);
@@ -804,7 +954,7 @@ struct Stepper {
             P::finish(rot, y, c);
         } else if constexpr (SOLVER == kHeun) {
             Cache c;
-            P::prepare(q, rot, y, c);
+            P::prepare_t(q, rot, y, c, tr);
             R a1[D], d[D], bw[D], s[D];
             P::det(q, y, c, B, a1);
             P::drift(q, y, c, d);
@@ -823,7 +973,7 @@ struct Stepper {
             P::finish(rot, y, c);
         } else if constexpr (SOLVER == kEulerMaruyamaNormalized) {
             Cache c;
-            P::prepare(q, rot, y, c);
+            P::prepare_t(q, rot, y, c, tr);
             R a[D], d[D], bw[D];
             P::det(q, y, c, B, a);
             P::drift(q, y, c, d);
@@ -834,7 +984,7 @@ struct Stepper {
             P::normalize(y);
         } else if constexpr (SOLVER == kMillstein) {
             Cache c;
-            P::prepare(q, rot, y, c);
+            P::prepare_t(q, rot, y, c, tr);
             R a[D], d[D], bw[D];
             P::det(q, y, c, B, a);
             P::drift(q, y, c, d);
@@ -902,9 +1052,9 @@ struct Stepper {
     // corrector the average of b at both points times an independent dW2.  Both
     // points are evaluated in the chart prepareCalculations chose for y_n.
     static __device__ __forceinline__ void step_heun_nc(const Par& q, const Rot<R>& rot, R* y, const R* B, const R* w,
-                                                        const R* w2, R dt) {
+                                                        const R* w2, R dt, const Trig& tr) {
         Cache c;
-        P::prepare(q, rot, y, c);
+        P::prepare_t(q, rot, y, c, tr);
         R a1[D], d[D], bw[D], s[D], b1[D];
         P::det(q, y, c, B, a1);
         P::drift(q, y, c, d);
@@ -937,9 +1087,9 @@ struct Stepper {
     // Y +- b_j sqrt(dt) around Y = y + a dt for the first D noise columns j, and
     //   y' = Y + b dW + sum_j (b(Y + b_j sqrt dt) - b(Y - b_j sqrt dt)) J(:, j) / sqrt(dt).
     static __device__ __forceinline__ void step_es1(const Par& q, const Rot<R>& rot, R* y, const R* B, const R* w,
-                                                    const R* A, R dt, R sqdt) {
+                                                    const R* A, R dt, R sqdt, const Trig& tr) {
         Cache c;
-        P::prepare(q, rot, y, c);
+        P::prepare_t(q, rot, y, c, tr);
         R a[D], bw[D], t[D], acc[D];
         P::det(q, y, c, B, a);
         P::bdw(q, y, c, w, bw);
@@ -970,9 +1120,9 @@ struct Stepper {
     //   T = (sum_j [(b(S+_j) - b(S-_j)) J(:, j) / sqrt(dt) + (b(S+_j) + b(S-_j)) dW]) / 4 + b dW / 2
     //   y2 = y + a(Y + b dW) dt/2 + a dt/2 + T;   y' = y + a(y2) dt/2 + a dt/2 + T
     static __device__ __forceinline__ void step_weak(const Par& q, const Rot<R>& rot, R* y, const R* B, const R* w,
-                                                     const R* A, R dt, R sqdt) {
+                                                     const R* A, R dt, R sqdt, const Trig& tr) {
         Cache c;
-        P::prepare(q, rot, y, c);
+        P::prepare_t(q, rot, y, c, tr);
         R a[D], bw[D], adt[D], t[D], acc[D], ys[D], as[D];
         P::det(q, y, c, B, a);
         P::bdw(q, y, c, w, bw);
