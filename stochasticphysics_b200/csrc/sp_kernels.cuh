@@ -238,6 +238,7 @@ __global__ void __launch_bounds__(kMaxBlock) step_kernel(const EnsDev* __restric
         const double dt_d = e.dt;
         const R dt = static_cast<R>(dt_d);
         const R sqdt = static_cast<R>(e.sqrt_dt);
+        const R m2dt = static_cast<R>(-2.0 * dt_d);  // FP32 Box-Muller radius scale
         const unsigned long long seed = e.seed, pid = e.pid_offset + p;
         const R* ftab = static_cast<const R*>(e.ftab);
         Rot<R> rot;
@@ -286,9 +287,7 @@ __global__ void __launch_bounds__(kMaxBlock) step_kernel(const EnsDev* __restric
 #pragma unroll
                         for (int j = 0; j < Mn; ++j) w[j] = dwp[(g * Mn + j) * Np + p];
                     } else {
-                        philox_normals<R, Mn>(seed, pid, g, w);
-#pragma unroll
-                        for (int j = 0; j < Mn; ++j) w[j] = w[j] * sqdt;
+                        philox_increments<R, Mn>(seed, pid, g, sqdt, m2dt, w);
                     }
                     const R B[3] = {sB[i][0], sB[i][1], sB[i][2]};
                     if constexpr (SOLVER == kHeunNotConsistent) {

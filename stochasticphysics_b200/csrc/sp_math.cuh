@@ -92,6 +92,13 @@ __device__ __forceinline__ R wrap_two_pi(R x) {
     if (M<R>::abs(x) < R(2) * tp) return x >= tp ? x - tp : (x <= -tp ? x + tp : x);
     return M<R>::fmod(x, tp);
 }
+// FP32 form: x - 2 pi trunc(x / 2 pi) in three instructions.  It equals the form above
+// except where x / 2 pi rounds up to the next integer (x within an ulp below a multiple
+// of 2 pi); there it returns the same angle less 2 pi.
+template <>
+__device__ __forceinline__ float wrap_two_pi<float>(float x) {
+    return fmaf(-M<float>::two_pi, truncf(x * 0.159154943f), x);
+}
 
 template <class R>
 struct V3 {
@@ -188,6 +195,36 @@ __device__ __forceinline__ void philox_normals(unsigned long long seed, unsigned
         box_muller(philox_block(seed, pid, step, call0 + 1u), 1, u);
         z[4] = u[0];
         z[5] = u[1];
+    }
+}
+
+// Wiener increments dW = sqrt(dt) z of one step (m = 3 or 6, calls 0-1).  FP64 scales
+// the unit normals; FP32 folds dt into the Box-Muller radius, sqrt(-2 dt ln u), which
+// saves the m multiplications.
+template <class R, int Mdim>
+__device__ __forceinline__ void philox_increments(unsigned long long seed, unsigned long long pid,
+                                                  unsigned long long step, R sqdt, R m2dt, R* w) {
+    if constexpr (sizeof(R) == 8) {
+        philox_normals<R, Mdim>(seed, pid, step, w);
+#pragma unroll
+        for (int j = 0; j < Mdim; ++j) w[j] = w[j] * sqdt;
+    } else {
+        const float inv = 2.3283064e-10f, half = 1.1641532e-10f;
+        const uint4 a = philox_block(seed, pid, step, 0u);
+        float r, s, c;
+        r = sqrt_pos(m2dt * __logf(fmaf(__uint2float_rn(a.x), inv, half)));
+        __sincosf(6.2831853f * fmaf(__uint2float_rn(a.y), inv, half), &s, &c);
+        w[0] = r * c; w[1] = r * s;
+        r = sqrt_pos(m2dt * __logf(fmaf(__uint2float_rn(a.z), inv, half)));
+        __sincosf(6.2831853f * fmaf(__uint2float_rn(a.w), inv, half), &s, &c);
+        w[2] = r * c;
+        if (Mdim > 3) {
+            w[3] = r * s;
+            const uint4 b = philox_block(seed, pid, step, 1u);
+            r = sqrt_pos(m2dt * __logf(fmaf(__uint2float_rn(b.x), inv, half)));
+            __sincosf(6.2831853f * fmaf(__uint2float_rn(b.y), inv, half), &s, &c);
+            w[4] = r * c; w[5] = r * s;
+        }
     }
 }
 

@@ -719,10 +719,10 @@ struct BrownNeelEuler {
             const R cos_2t = cos_t * cos_t - sin_t * sin_t;
             const R sin_2t = R(2) * cos_t * sin_t;
             const R sin_t_2 = sin_t * sin_t;
-            const R cph = cos_p * cpsi + spsi * sin_p;
-            const R sph = cpsi * sin_p - cos_p * spsi;
-            R s2, c2;
-            M<R>::sincos(R(2) * (y[4] - y[2]), &s2, &c2);
+            const R cph = cos_p * cpsi + spsi * sin_p;  // cos(phi_N - psi)
+            const R sph = cpsi * sin_p - cos_p * spsi;  // sin(phi_N - psi)
+            // sin and cos of 2 (phi_N - psi) by the double-angle identities
+            const R s2 = R(2) * sph * cph, c2 = cph * cph - sph * sph;
             r[0] = csc * sin_t * (q.adDN2 * sph - R(2) * q.d2fDN2 * (cos_t * cph + cotb * sin_t * s2));
             r[1] = q.cF2h * cotb - q.adDN2 * (cph * sin_t) +
                    q.d2fDN2 * (R(0.5) * (R(3) + cos_2t + R(2) * c2 * sin_t_2) * cotb - sin_2t * sph);
