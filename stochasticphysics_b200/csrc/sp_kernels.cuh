@@ -214,6 +214,81 @@ __global__ void __launch_bounds__(kMaxBlock) init_kernel(const EnsDev* __restric
     }
 }
 
+// ------------------------------------------------------------------ window sums
+// Kahan summation of each step's output over a window (SingleParticleSimulator.h:148-153);
+// the compensation carries over from one window to the next, the sum restarts.
+template <class R, int OUT>
+struct WindowSum {
+    R sum[OUT], comp[OUT];
+    __device__ __forceinline__ void set(int c, R s, R k) { sum[c] = s; comp[c] = k; }
+    __device__ __forceinline__ R get_sum(int c) const { return sum[c]; }
+    __device__ __forceinline__ R get_comp(int c) const { return comp[c]; }
+    __device__ __forceinline__ void clear_sum(int c) { sum[c] = R(0); }
+    __device__ __forceinline__ void add(const R* o) {
+#pragma unroll
+        for (int c = 0; c < OUT; ++c) {
+            const R yv = o[c] - comp[c];
+            const R tv = sum[c] + yv;
+            comp[c] = (tv - sum[c]) - yv;
+            sum[c] = tv;
+        }
+    }
+};
+// FP32: two outputs per 64-bit register, both updated by one paired instruction
+// (add/sub.rn.f32x2); each lane rounds exactly as the scalar form does.
+__device__ __forceinline__ unsigned long long pack2(float lo, float hi) {
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ float2 unpack2(unsigned long long v) {
+    float lo, hi;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+    return make_float2(lo, hi);
+}
+__device__ __forceinline__ unsigned long long add2(unsigned long long a, unsigned long long b) {
+    unsigned long long r;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ unsigned long long sub2(unsigned long long a, unsigned long long b) {
+    unsigned long long r;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+template <int OUT>
+struct WindowSum<float, OUT> {
+    static constexpr int NP = (OUT + 1) / 2;
+    unsigned long long sum[NP] = {}, comp[NP] = {};  // an odd OUT leaves a zero lane
+    __device__ __forceinline__ void set(int c, float s, float k) {
+        const float2 a = unpack2(sum[c / 2]), b = unpack2(comp[c / 2]);
+        sum[c / 2] = (c & 1) ? pack2(a.x, s) : pack2(s, a.y);
+        comp[c / 2] = (c & 1) ? pack2(b.x, k) : pack2(k, b.y);
+    }
+    __device__ __forceinline__ float get_sum(int c) const {
+        const float2 a = unpack2(sum[c / 2]);
+        return (c & 1) ? a.y : a.x;
+    }
+    __device__ __forceinline__ float get_comp(int c) const {
+        const float2 a = unpack2(comp[c / 2]);
+        return (c & 1) ? a.y : a.x;
+    }
+    __device__ __forceinline__ void clear_sum(int c) {
+        const float2 a = unpack2(sum[c / 2]);
+        sum[c / 2] = (c & 1) ? pack2(a.x, 0.0f) : pack2(0.0f, a.y);
+    }
+    __device__ __forceinline__ void add(const float* o) {
+#pragma unroll
+        for (int k = 0; k < NP; ++k) {
+            const unsigned long long v = pack2(o[2 * k], 2 * k + 1 < OUT ? o[2 * k + 1] : 0.0f);
+            const unsigned long long yv = sub2(v, comp[k]);
+            const unsigned long long tv = add2(sum[k], yv);
+            comp[k] = sub2(sub2(tv, sum[k]), yv);
+            sum[k] = tv;
+        }
+    }
+};
+
 // ------------------------------------------------------------------ step
 template <int PROB, class R, int A, int SOLVER, bool INJECT>
 __global__ void __launch_bounds__(kMaxBlock) step_kernel(const EnsDev* __restrict__ ensembles,
@@ -246,7 +321,8 @@ __global__ void __launch_bounds__(kMaxBlock) step_kernel(const EnsDev* __restric
         rot.min1 = static_cast<R>(e.min1); rot.max1 = static_cast<R>(e.max1);
         rot.min2 = static_cast<R>(e.min2); rot.max2 = static_cast<R>(e.max2);
 
-        R y[D], sum[OUT], comp[OUT];
+        R y[D];
+        WindowSum<R, OUT> acc;
         typename Prob::Par q;
         if (active) {
             const R* state = static_cast<const R*>(e.state);
@@ -255,13 +331,13 @@ __global__ void __launch_bounds__(kMaxBlock) step_kernel(const EnsDev* __restric
 #pragma unroll
             for (int i = 0; i < D; ++i) y[i] = state[i * Np + p];
 #pragma unroll
-            for (int c = 0; c < OUT; ++c) { sum[c] = ks[c * Np + p]; comp[c] = kc[c * Np + p]; }
+            for (int c = 0; c < OUT; ++c) acc.set(c, ks[c * Np + p], kc[c * Np + p]);
             q = Prob::load(static_cast<const R*>(e.params), Np, p);
         } else {
 #pragma unroll
             for (int i = 0; i < D; ++i) y[i] = R(0);
 #pragma unroll
-            for (int c = 0; c < OUT; ++c) { sum[c] = R(0); comp[c] = R(0); }
+            for (int c = 0; c < OUT; ++c) acc.set(c, R(0), R(0));
             q = Prob::load(static_cast<const R*>(e.params), Np, td.first);  // any valid slot; results are discarded
         }
         NewtonCount nc{0u, 0u};
@@ -306,13 +382,7 @@ __global__ void __launch_bounds__(kMaxBlock) step_kernel(const EnsDev* __restric
                     }
                     R o[OUT];
                     Prob::out_t(y, o, tr);
-#pragma unroll
-                    for (int c = 0; c < OUT; ++c) {  // Kahan summation (SingleParticleSimulator.h:148-153)
-                        const R yv = o[c] - comp[c];
-                        const R tv = sum[c] + yv;
-                        comp[c] = (tv - sum[c]) - yv;
-                        sum[c] = tv;
-                    }
+                    acc.add(o);
                 }
                 if (++wpos == W32) {  // window end: uniform across the CTA
                     wpos = 0;
@@ -323,8 +393,8 @@ __global__ void __launch_bounds__(kMaxBlock) step_kernel(const EnsDev* __restric
                     double* const partial = e.partial + ((p >> 5) * e.slots + slot) * OUT;
 #pragma unroll
                     for (int c = 0; c < OUT; ++c) {
-                        const R v = active ? sum[c] / static_cast<R>(static_cast<double>(W)) : R(0);
-                        sum[c] = R(0);
+                        const R v = active ? acc.get_sum(c) / static_cast<R>(static_cast<double>(W)) : R(0);
+                        acc.clear_sum(c);
                         const double vd = static_cast<double>(v);
                         if (traj && active) traj[(k * OUT + c) * Np + p] = vd;
                         const double ws = warp_sum(active ? weight_of<PROB>(c, mom) * vd : 0.0);
@@ -341,7 +411,7 @@ __global__ void __launch_bounds__(kMaxBlock) step_kernel(const EnsDev* __restric
 #pragma unroll
             for (int i = 0; i < D; ++i) { state[i * Np + p] = y[i]; finite = finite && M<R>::finite(y[i]); }
 #pragma unroll
-            for (int c = 0; c < OUT; ++c) { ks[c * Np + p] = sum[c]; kc[c * Np + p] = comp[c]; }
+            for (int c = 0; c < OUT; ++c) { ks[c * Np + p] = acc.get_sum(c); kc[c * Np + p] = acc.get_comp(c); }
             if (!finite) e.status[p] = 1;
         }
         if constexpr (SOLVER == kImplicitMidpoint || SOLVER == kImplicitMidpointExact) {
