@@ -34,7 +34,7 @@
 extern "C" {
 #endif
 
-#define SP_ABI_VERSION 6u
+#define SP_ABI_VERSION 7u
 
 #if defined(_WIN32)
 #define SP_API __declspec(dllexport)
@@ -372,14 +372,17 @@ SP_API sp_status sp_measure_fma_peak(sp_context* ctx, int32_t precision, double*
 /* ---- autotuner ----------------------------------------------------------
  * No counterpart in the reference (its thread pool has no launch shape).
  * Launch shape of one kernel key (problem, anisotropy, solver, precision,
- * noise): threads per CTA (one particle per thread), persistent grid (CTAs =
- * resident CTAs x SMs striding over the tiles) or one CTA per tile, and SDE
- * steps per captured chunk. */
+ * noise): particles per CTA tile, particles per thread (1, or 2 for the FP32
+ * kernels: the CTA then has block / 2 threads, each integrating two particles
+ * whose step chains interleave), persistent grid (CTAs = resident CTAs x SMs
+ * striding over the tiles) or one CTA per tile, and SDE steps per captured chunk. */
 typedef struct sp_launch_config {
     int32_t block;
     int32_t persistent;
     uint64_t chunk_steps;
     double particle_steps_per_s; /* measured rate of this shape on the probe */
+    int32_t particles_per_thread;
+    int32_t reserved0;
 } sp_launch_config;
 /* Times every candidate shape on a probe of desc (its first
  * min(n_particles, probe_particles) particles; 0 = 65536) with CUDA events and

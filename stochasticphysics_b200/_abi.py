@@ -13,7 +13,7 @@ from typing import Optional
 
 import numpy as np
 
-ABI_VERSION = 6
+ABI_VERSION = 7
 
 
 class Status(IntEnum):
@@ -223,10 +223,13 @@ class sp_launch_config(C.Structure):
         ("persistent", C.c_int32),
         ("chunk_steps", C.c_uint64),
         ("particle_steps_per_s", C.c_double),
+        ("particles_per_thread", C.c_int32),
+        ("reserved0", C.c_int32),
     ]
 
     def to_dict(self) -> dict:
         return {"block": int(self.block), "persistent": int(self.persistent), "chunk_steps": int(self.chunk_steps),
+                "particles_per_thread": int(self.particles_per_thread),
                 "particle_steps_per_s": float(self.particle_steps_per_s)}
 
 

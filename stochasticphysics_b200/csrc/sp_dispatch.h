@@ -11,10 +11,12 @@ struct KernelSet {
     bool valid = false;
     int D = 0, Mn = 0, OUT = 0, P = 0, real_bytes = 0;
     void (*init)(const EnsDev* e, const RawParticles& rp, unsigned long long Np, cudaStream_t s) = nullptr;
-    void (*step)(const EnsDev* e, const TileDesc* t, int ntiles, int grid, int block, cudaStream_t s) = nullptr;
+    // step[ppt - 1]: the step kernel with 1 or 2 particles per thread (2: FP32 only);
+    // `block` is the tile's particle count, the CTA has block / ppt threads
+    void (*step[2])(const EnsDev* e, const TileDesc* t, int ntiles, int grid, int block, cudaStream_t s) = {nullptr, nullptr};
     void (*reduce)(const EnsDev* e, int n_ens, int max_slots, int mode, cudaStream_t s) = nullptr;
     void (*field)(const EnsDev* e, int n_ens, unsigned long long chunk, int midpoint, cudaStream_t s) = nullptr;
-    const void* step_fn = nullptr;  // for cudaFuncGetAttributes / occupancy queries
+    const void* step_fn[2] = {nullptr, nullptr};  // for cudaFuncGetAttributes / occupancy queries
 };
 
 // index: problem, anisotropy, solver slot (see solver_slot),

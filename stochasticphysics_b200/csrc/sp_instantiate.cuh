@@ -6,9 +6,9 @@
 
 namespace sp {
 
-template <int PROB, class R, int A, int SOLVER, bool INJ>
+template <int PROB, class R, int A, int SOLVER, bool INJ, int PPT>
 void launch_step_t(const EnsDev* e, const TileDesc* t, int ntiles, int grid, int block, cudaStream_t s) {
-    step_kernel<PROB, R, A, SOLVER, INJ><<<grid, block, 0, s>>>(e, t, ntiles);
+    step_kernel<PROB, R, A, SOLVER, INJ, PPT><<<grid, block / PPT, 0, s>>>(e, t, ntiles);
 }
 template <int PROB, class R, int A>
 void launch_init_t(const EnsDev* e, const RawParticles& rp, unsigned long long Np, cudaStream_t s) {
@@ -38,10 +38,14 @@ KernelSet make_set() {
         k.D = Prob::D; k.Mn = Prob::Mn; k.OUT = Prob::OUT; k.P = ProblemOf<PROB, R, A>::P;
         k.real_bytes = static_cast<int>(sizeof(R));
         k.init = &launch_init_t<PROB, R, A>;
-        k.step = &launch_step_t<PROB, R, A, SOLVER, INJ>;
+        k.step[0] = &launch_step_t<PROB, R, A, SOLVER, INJ, 1>;
+        k.step_fn[0] = reinterpret_cast<const void*>(&step_kernel<PROB, R, A, SOLVER, INJ, 1>);
+        if constexpr (sizeof(R) == 4 && !INJ) {  // two particles per thread: FP32, in-kernel noise
+            k.step[1] = &launch_step_t<PROB, R, A, SOLVER, INJ, 2>;
+            k.step_fn[1] = reinterpret_cast<const void*>(&step_kernel<PROB, R, A, SOLVER, INJ, 2>);
+        }
         k.reduce = &launch_reduce_t<Prob::OUT>;
         k.field = &launch_field_chunk_t<R>;
-        k.step_fn = reinterpret_cast<const void*>(&step_kernel<PROB, R, A, SOLVER, INJ>);
         return k;
     }
 }

@@ -290,9 +290,13 @@ struct WindowSum<float, OUT> {
 };
 
 // ------------------------------------------------------------------ step
-template <int PROB, class R, int A, int SOLVER, bool INJECT>
-__global__ void __launch_bounds__(kMaxBlock) step_kernel(const EnsDev* __restrict__ ensembles,
-                                                         const TileDesc* __restrict__ tiles, int ntiles) {
+// One tile = blockDim.x * PPT particles of one ensemble; thread t integrates particles
+// first + k blockDim.x + t, k < PPT.  With PPT = 2 each thread carries two independent
+// step chains, which the scheduler interleaves (instruction-level parallelism in a
+// latency-bound loop).  Each particle's arithmetic is the same for every PPT.
+template <int PROB, class R, int A, int SOLVER, bool INJECT, int PPT>
+__global__ void __launch_bounds__(kMaxBlock / PPT) step_kernel(const EnsDev* __restrict__ ensembles,
+                                                               const TileDesc* __restrict__ tiles, int ntiles) {
     using Prob = typename ProblemOf<PROB, R, A>::type;
     using St = Stepper<Prob, R, SOLVER>;
     constexpr int D = Prob::D, Mn = Prob::Mn, OUT = Prob::OUT;
@@ -308,41 +312,49 @@ __global__ void __launch_bounds__(kMaxBlock) step_kernel(const EnsDev* __restric
         const unsigned long long nsteps = tgt > s0 ? min(e.chunk, tgt - s0) : 0ull;
         if (nsteps == 0) continue;  // uniform across the CTA
         const unsigned long long Np = e.Np, W = e.W;
-        const unsigned long long p = td.first + threadIdx.x;
-        const bool active = p < e.n;
+        unsigned long long p[PPT];
+        bool active[PPT];
+#pragma unroll
+        for (int k = 0; k < PPT; ++k) {
+            p[k] = td.first + static_cast<unsigned long long>(k) * blockDim.x + threadIdx.x;
+            active[k] = p[k] < e.n;
+        }
         const double dt_d = e.dt;
         const R dt = static_cast<R>(dt_d);
         const R sqdt = static_cast<R>(e.sqrt_dt);
         const R m2dt = static_cast<R>(-2.0 * dt_d);  // FP32 Box-Muller radius scale
-        const unsigned long long seed = e.seed, pid = e.pid_offset + p;
+        const unsigned long long seed = e.seed;
         const R* ftab = static_cast<const R*>(e.ftab);
         Rot<R> rot;
         rot.rb = e.rot_brown != 0; rot.rn = e.rot_neel != 0;
         rot.min1 = static_cast<R>(e.min1); rot.max1 = static_cast<R>(e.max1);
         rot.min2 = static_cast<R>(e.min2); rot.max2 = static_cast<R>(e.max2);
 
-        R y[D];
-        WindowSum<R, OUT> acc;
-        typename Prob::Par q;
-        if (active) {
-            const R* state = static_cast<const R*>(e.state);
-            const R* ks = static_cast<const R*>(e.ksum);
-            const R* kc = static_cast<const R*>(e.kcomp);
+        R y[PPT][D];
+        WindowSum<R, OUT> acc[PPT];
+        typename Prob::Par q[PPT];
+        typename Prob::Trig tr[PPT];  // sincos of y, carried from each step's output to the next prepare
 #pragma unroll
-            for (int i = 0; i < D; ++i) y[i] = state[i * Np + p];
+        for (int k = 0; k < PPT; ++k) {
+            if (active[k]) {
+                const R* state = static_cast<const R*>(e.state);
+                const R* ks = static_cast<const R*>(e.ksum);
+                const R* kc = static_cast<const R*>(e.kcomp);
 #pragma unroll
-            for (int c = 0; c < OUT; ++c) acc.set(c, ks[c * Np + p], kc[c * Np + p]);
-            q = Prob::load(static_cast<const R*>(e.params), Np, p);
-        } else {
+                for (int i = 0; i < D; ++i) y[k][i] = state[i * Np + p[k]];
 #pragma unroll
-            for (int i = 0; i < D; ++i) y[i] = R(0);
+                for (int c = 0; c < OUT; ++c) acc[k].set(c, ks[c * Np + p[k]], kc[c * Np + p[k]]);
+                q[k] = Prob::load(static_cast<const R*>(e.params), Np, p[k]);
+            } else {
 #pragma unroll
-            for (int c = 0; c < OUT; ++c) acc.set(c, R(0), R(0));
-            q = Prob::load(static_cast<const R*>(e.params), Np, td.first);  // any valid slot; results are discarded
+                for (int i = 0; i < D; ++i) y[k][i] = R(0);
+#pragma unroll
+                for (int c = 0; c < OUT; ++c) acc[k].set(c, R(0), R(0));
+                q[k] = Prob::load(static_cast<const R*>(e.params), Np, td.first);  // any valid slot; results are discarded
+            }
+            Prob::trig(y[k], tr[k]);
         }
         NewtonCount nc{0u, 0u};
-        typename Prob::Trig tr;  // sincos of y, carried from each step's output to the next prepare
-        Prob::trig(y, tr);
         // W < 2^31 (validated); the window position fits 32 bits.  Values used only
         // at a window end (once per W steps) are re-read there instead of being kept
         // live in registers across the step loop.
@@ -357,62 +369,71 @@ __global__ void __launch_bounds__(kMaxBlock) step_kernel(const EnsDev* __restric
             __syncwarp();
             for (int i = 0; i < len; ++i) {
                 const unsigned long long g = s0 + t0 + i;
-                if (active) {
+                const R B[3] = {sB[i][0], sB[i][1], sB[i][2]};
+#pragma unroll
+                for (int k = 0; k < PPT; ++k) {
+                    if (!active[k]) continue;
+                    const unsigned long long pid = e.pid_offset + p[k];
                     R w[Mn];
                     if constexpr (INJECT) {
 #pragma unroll
-                        for (int j = 0; j < Mn; ++j) w[j] = dwp[(g * Mn + j) * Np + p];
+                        for (int j = 0; j < Mn; ++j) w[j] = dwp[(g * Mn + j) * Np + p[k]];
                     } else {
                         philox_increments<R, Mn>(seed, pid, g, sqdt, m2dt, w);
                     }
-                    const R B[3] = {sB[i][0], sB[i][1], sB[i][2]};
                     if constexpr (SOLVER == kHeunNotConsistent) {
                         R w2[Mn];
                         philox_normals<R, Mn>(seed, pid, g, w2, 2u);
 #pragma unroll
                         for (int j = 0; j < Mn; ++j) w2[j] = w2[j] * sqdt;
-                        St::step_heun_nc(q, rot, y, B, w, w2, dt, tr);
+                        St::step_heun_nc(q[k], rot, y[k], B, w, w2, dt, tr[k]);
                     } else if constexpr (uses_double_noise(SOLVER)) {
-                        R A[Mn * (Mn - 1) / 2];
-                        double_noise_antisym<R, Mn>(seed, pid, g, e.dna, static_cast<R>(e.rho), sqdt, w, A);
-                        if constexpr (SOLVER == kWeakTest) St::step_weak(q, rot, y, B, w, A, dt, sqdt, tr);
-                        else St::step_es1(q, rot, y, B, w, A, dt, sqdt, tr);
+                        R An[Mn * (Mn - 1) / 2];
+                        double_noise_antisym<R, Mn>(seed, pid, g, e.dna, static_cast<R>(e.rho), sqdt, w, An);
+                        if constexpr (SOLVER == kWeakTest) St::step_weak(q[k], rot, y[k], B, w, An, dt, sqdt, tr[k]);
+                        else St::step_es1(q[k], rot, y[k], B, w, An, dt, sqdt, tr[k]);
                     } else {
-                        St::step(q, rot, y, B, w, dt, e.max_iter, e.tol, nc, tr);
+                        St::step(q[k], rot, y[k], B, w, dt, e.max_iter, e.tol, nc, tr[k]);
                     }
                     R o[OUT];
-                    Prob::out_t(y, o, tr);
-                    acc.add(o);
+                    Prob::out_t(y[k], o, tr[k]);
+                    acc[k].add(o);
                 }
                 if (++wpos == W32) {  // window end: uniform across the CTA
                     wpos = 0;
-                    const unsigned long long k = (g + 1) / W;
-                    const int slot = static_cast<int>(k - s0 / W - 1);
-                    const double mom = active ? e.moment[p] : 0.0;
+                    const unsigned long long kw = (g + 1) / W;
+                    const int slot = static_cast<int>(kw - s0 / W - 1);
                     double* const traj = e.traj;
-                    double* const partial = e.partial + ((p >> 5) * e.slots + slot) * OUT;
 #pragma unroll
-                    for (int c = 0; c < OUT; ++c) {
-                        const R v = active ? acc.get_sum(c) / static_cast<R>(static_cast<double>(W)) : R(0);
-                        acc.clear_sum(c);
-                        const double vd = static_cast<double>(v);
-                        if (traj && active) traj[(k * OUT + c) * Np + p] = vd;
-                        const double ws = warp_sum(active ? weight_of<PROB>(c, mom) * vd : 0.0);
-                        if ((threadIdx.x & 31) == 0) partial[c] = ws;
+                    for (int k = 0; k < PPT; ++k) {
+                        const double mom = active[k] ? e.moment[p[k]] : 0.0;
+                        double* const partial = e.partial + ((p[k] >> 5) * e.slots + slot) * OUT;
+#pragma unroll
+                        for (int c = 0; c < OUT; ++c) {
+                            const R v = active[k] ? acc[k].get_sum(c) / static_cast<R>(static_cast<double>(W)) : R(0);
+                            acc[k].clear_sum(c);
+                            const double vd = static_cast<double>(v);
+                            if (traj && active[k]) traj[(kw * OUT + c) * Np + p[k]] = vd;
+                            const double ws = warp_sum(active[k] ? weight_of<PROB>(c, mom) * vd : 0.0);
+                            if ((threadIdx.x & 31) == 0) partial[c] = ws;
+                        }
                     }
                 }
             }
         }
-        if (active) {
-            R* state = static_cast<R*>(e.state);
-            R* ks = static_cast<R*>(e.ksum);
-            R* kc = static_cast<R*>(e.kcomp);
-            bool finite = true;
 #pragma unroll
-            for (int i = 0; i < D; ++i) { state[i * Np + p] = y[i]; finite = finite && M<R>::finite(y[i]); }
+        for (int k = 0; k < PPT; ++k) {
+            if (active[k]) {
+                R* state = static_cast<R*>(e.state);
+                R* ks = static_cast<R*>(e.ksum);
+                R* kc = static_cast<R*>(e.kcomp);
+                bool finite = true;
 #pragma unroll
-            for (int c = 0; c < OUT; ++c) { ks[c * Np + p] = acc.get_sum(c); kc[c * Np + p] = acc.get_comp(c); }
-            if (!finite) e.status[p] = 1;
+                for (int i = 0; i < D; ++i) { state[i * Np + p[k]] = y[k][i]; finite = finite && M<R>::finite(y[k][i]); }
+#pragma unroll
+                for (int c = 0; c < OUT; ++c) { ks[c * Np + p[k]] = acc[k].get_sum(c); kc[c * Np + p[k]] = acc[k].get_comp(c); }
+                if (!finite) e.status[p[k]] = 1;
+            }
         }
         if constexpr (SOLVER == kImplicitMidpoint || SOLVER == kImplicitMidpointExact) {
             unsigned int it = nc.iterations, un = nc.unconverged;

@@ -171,7 +171,7 @@ extern "C" SP_API sp_status sp_simulate_noalloc(const sp_ensemble_desc* desc, co
             const unsigned long long nchunks = (L.S + L.chunk - 1) / L.chunk;
             for (unsigned long long i = 0; i < nchunks; ++i) {
                 ks.field(d_ens, 1, L.chunk, midpoint, s);
-                ks.step(d_ens, d_tiles, ntiles, ntiles, lc.block, s);
+                ks.step[0](d_ens, d_tiles, ntiles, ntiles, lc.block, s);
                 ks.reduce(d_ens, 1, L.slots, 0, s);
                 launch_commit(d_ens, 1, s);
             }

@@ -264,10 +264,11 @@ Ensemble::Ensemble(sp_context* c, const sp_ensemble_desc& d, const LaunchConfig&
     d_tiles = static_cast<TileDesc*>(dalloc(tiles.size() * sizeof(TileDesc)));
     check_cuda(cudaMemcpyAsync(d_tiles, tiles.data(), tiles.size() * sizeof(TileDesc), cudaMemcpyHostToDevice, stream),
                "upload tiles");
+    ppt = usable_ppt(*ks, launch.ppt, block);
     grid = ntiles;
     if (launch.persistent) {
         int per_sm = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ks->step_fn, block, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ks->step_fn[ppt - 1], block / ppt, 0);
         grid = std::min(ntiles, std::max(1, per_sm) * ctx->sms);
     }
 
@@ -372,7 +373,7 @@ void Ensemble::upload_and_init(const sp_ensemble_desc& d) {
 void Ensemble::enqueue_chunk(cudaStream_t s) {
     const int midpoint = desc.solver == SP_SOLVER_IMPLICIT_MIDPOINT ? 1 : 0;
     ks->field(d_ens, 1, L.chunk, midpoint, s);
-    ks->step(d_ens, d_tiles, ntiles, grid, block, s);
+    ks->step[ppt - 1](d_ens, d_tiles, ntiles, grid, block, s);
     ks->reduce(d_ens, 1, L.slots, 0, s);
     launch_commit(d_ens, 1, s);
 }

@@ -48,10 +48,16 @@ void reference_times(unsigned long long K, unsigned long long W, double dt, doub
 
 // launch shape of one kernel key: CTA size, persistent grid, steps per chunk
 struct LaunchConfig {
-    int block = 128;
+    int block = 128;       // particles per tile
     int persistent = 0;
     unsigned long long chunk = 10000;
+    int ppt = 1;           // particles per thread: the CTA has block / ppt threads
 };
+// the particles per thread a kernel set and tile size allow (2 needs the FP32 kernel and
+// at least one warp per CTA)
+inline int usable_ppt(const KernelSet& ks, int ppt, int block) {
+    return (ppt == 2 && ks.step[1] && block >= 64) ? 2 : 1;
+}
 LaunchConfig default_launch(const sp_context* ctx, const sp_ensemble_desc& d);
 // default_launch refined by the autotuner cache and SP_BLOCK / SP_CHUNK / SP_PERSISTENT
 LaunchConfig launch_config_for(const sp_context* ctx, const sp_ensemble_desc& d);
@@ -83,7 +89,7 @@ struct Ensemble {
     double device_ms = 0.0;
     unsigned long long launches = 0, particle_steps = 0, steps_done = 0;
     unsigned long long h2d_bytes = 0, d2h_bytes = 0;
-    int block = 128, grid = 1, ntiles = 0;
+    int block = 128, grid = 1, ntiles = 0, ppt = 1;
     EnsDev hdev;
     void *d_state = nullptr, *d_ksum = nullptr, *d_kcomp = nullptr, *d_params = nullptr, *d_dw = nullptr,
          *d_ftab = nullptr;

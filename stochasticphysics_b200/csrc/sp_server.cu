@@ -189,7 +189,10 @@ struct sp_server {
         check_cuda(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal), "begin capture");
         launch_bump_targets(g.d_ens, n, cs);
         g.ks->field(g.d_ens, n, g.max_chunk, midpoint, cs);
-        g.ks->step(g.d_ens, g.d_tiles, g.ntiles, g.ntiles, g.block, cs);
+        // one launch shape for the group: its largest tile, and the particles per thread
+        // the first member was configured with where that tile allows it
+        const int ppt = usable_ppt(*g.ks, g.members.front()->ens->launch.ppt, g.block);
+        g.ks->step[ppt - 1](g.d_ens, g.d_tiles, g.ntiles, g.ntiles, g.block, cs);
         g.ks->reduce(g.d_ens, n, g.max_slots, 0, cs);
         launch_commit(g.d_ens, n, cs);
         const cudaError_t ce = cudaStreamEndCapture(cs, &g.graph);

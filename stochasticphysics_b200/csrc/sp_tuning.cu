@@ -1,11 +1,12 @@
 // sp_tuning.cu — launch configuration per kernel key: defaults, the autotuner
-// and its cache, and environment overrides (SP_BLOCK, SP_CHUNK, SP_PERSISTENT).
+// and its cache, and environment overrides (SP_BLOCK, SP_CHUNK, SP_PERSISTENT, SP_PPT).
 //
 // The autotuner times candidate launch shapes on a probe ensemble (a prefix of
 // the caller's particles) with CUDA events and keeps the fastest per kernel key
-// (problem, anisotropy, solver, precision, noise).  Shapes: CTA size 64/128/256
-// (one particle per thread; the step kernel is register-bound, so CTA size moves
-// occupancy and tail effects), persistent grid or one CTA per tile, and the
+// (problem, anisotropy, solver, precision, noise).  Shapes: tile size 64/128/256
+// particles (the step kernel is register-bound, so tile size moves occupancy and
+// tail effects), one or two particles per thread (FP32: two independent step
+// chains per thread), persistent grid or one CTA per tile, and the
 // chunk length of the captured graph (per-chunk kernels: field table, window
 // reduction, commit).
 #include <algorithm>
@@ -57,6 +58,7 @@ LaunchConfig launch_config_for(const sp_context* ctx, const sp_ensemble_desc& d)
     if (lookup_tuned(d, t)) {
         c.block = t.block;
         c.persistent = t.persistent;
+        c.ppt = t.ppt;
         if (t.chunk) c.chunk = round_chunk(t.chunk, d.oversampling);
         // small ensembles keep enough CTAs to cover the SMs
         const int sms = ctx ? ctx->sms : 148;
@@ -71,6 +73,10 @@ LaunchConfig launch_config_for(const sp_context* ctx, const sp_ensemble_desc& d)
         if (v > 0) c.chunk = static_cast<unsigned long long>(v);
     }
     if (const char* s = std::getenv("SP_PERSISTENT")) c.persistent = std::atoi(s) != 0;
+    if (const char* s = std::getenv("SP_PPT")) c.ppt = std::atoi(s) == 2 ? 2 : 1;
+    const KernelSet& ks = kernel_set(d.problem, d.anisotropy, solver_slot(d.solver, d.jacobian), d.precision,
+                                     d.noise == SP_NOISE_INJECTED ? 1 : 0);
+    c.ppt = usable_ppt(ks, c.ppt, c.block);
     return c;
 }
 
@@ -94,6 +100,8 @@ void to_c(const LaunchConfig& c, double rate, sp_launch_config* o) {
     o->persistent = c.persistent;
     o->chunk_steps = c.chunk;
     o->particle_steps_per_s = rate;
+    o->particles_per_thread = c.ppt;
+    o->reserved0 = 0;
 }
 }  // namespace
 
@@ -129,16 +137,21 @@ sp_status sp_autotune(sp_context* ctx, const sp_ensemble_desc* desc, uint64_t pr
     // CTA size x grid form at the default chunk, then the chunk length for the winner
     LaunchConfig win;
     double win_rate = -1.0;
-    for (int persistent = 0; persistent <= 1; ++persistent)
-        for (int block : {64, 128, 256}) {
-            if ((probe.n_particles + block - 1) / block < static_cast<unsigned long long>(ctx->sms) && block > 64) continue;
-            LaunchConfig lc;
-            lc.block = block;
-            lc.persistent = persistent;
-            lc.chunk = c0;
-            const double r = run(lc);
-            if (r > win_rate) { win = lc; win_rate = r; }
-        }
+    const KernelSet& ks = kernel_set(desc->problem, desc->anisotropy, solver_slot(desc->solver, desc->jacobian),
+                                     desc->precision, 0);
+    const int max_ppt = ks.step[1] ? 2 : 1;
+    for (int ppt = 1; ppt <= max_ppt; ++ppt)
+        for (int persistent = 0; persistent <= 1; ++persistent)
+            for (int block : {64, 128, 256}) {
+                if ((probe.n_particles + block - 1) / block < static_cast<unsigned long long>(ctx->sms) && block > 64) continue;
+                LaunchConfig lc;
+                lc.block = block;
+                lc.persistent = persistent;
+                lc.chunk = c0;
+                lc.ppt = ppt;
+                const double r = run(lc);
+                if (r > win_rate) { win = lc; win_rate = r; }
+            }
     if (c_long != c0) {
         LaunchConfig lc = win;
         lc.chunk = c_long;
@@ -177,7 +190,8 @@ sp_status sp_launch_config_for(sp_context* ctx, const sp_ensemble_desc* desc, sp
     SP_GUARD_END
 }
 
-// "problem/anisotropy/solver/precision/noise block persistent chunk rate" per line
+// "problem/anisotropy/solver/precision/noise block persistent chunk rate ppt" per line
+// (a line without ppt reads as one particle per thread)
 sp_status sp_tuning_save(const char* path) {
     SP_GUARD_BEGIN
     if (!path) return fail(SP_ERR_INVALID_ARG, "path is NULL");
@@ -187,7 +201,7 @@ sp_status sp_tuning_save(const char* path) {
     for (const auto& kv : g_tuned) {
         auto r = g_tuned_rate.find(kv.first);
         f << kv.first << ' ' << kv.second.block << ' ' << kv.second.persistent << ' ' << kv.second.chunk << ' '
-          << (r == g_tuned_rate.end() ? 0.0 : r->second) << '\n';
+          << (r == g_tuned_rate.end() ? 0.0 : r->second) << ' ' << kv.second.ppt << '\n';
     }
     return f.good() ? SP_OK : fail(SP_ERR_INVALID_ARG, std::string("write failed: ") + path);
     SP_GUARD_END
@@ -208,10 +222,12 @@ sp_status sp_tuning_load(const char* path) {
         double rate = 0.0;
         if (!(is >> key >> c.block >> c.persistent >> c.chunk)) return fail(SP_ERR_INVALID_ARG, "malformed line: " + line);
         is >> rate;
+        if (!(is >> c.ppt)) c.ppt = 1;
         int parts[5];
         if (std::sscanf(key.c_str(), "%d/%d/%d/%d/%d", &parts[0], &parts[1], &parts[2], &parts[3], &parts[4]) != 5)
             return fail(SP_ERR_INVALID_ARG, "malformed key: " + key);
-        if (!(c.block == 32 || c.block == 64 || c.block == 128 || c.block == 256) || c.chunk == 0)
+        if (!(c.block == 32 || c.block == 64 || c.block == 128 || c.block == 256) || c.chunk == 0 ||
+            !(c.ppt == 1 || c.ppt == 2))
             return fail(SP_ERR_INVALID_ARG, "invalid launch shape: " + line);
         rows.push_back({key, {c, rate}});
     }

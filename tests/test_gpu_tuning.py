@@ -2,6 +2,8 @@
 
 The ensemble mean is reduced per warp in a fixed order, so no launch shape
 (CTA size, persistent grid, chunk length) may change a single bit of the result.
+Two particles per thread (FP32) run each particle's steps through a separately
+compiled kernel; the test states how close it is to one particle per thread.
 """
 import dataclasses
 
@@ -52,6 +54,31 @@ def test_results_do_not_depend_on_the_launch_shape(ctx, tmp_path, shape):
     assert (used["persistent"], used["chunk_steps"]) == (persistent, chunk)
     np.testing.assert_array_equal(got.mean, ref.mean)
     np.testing.assert_array_equal(got.weight, ref.weight)
+
+
+@pytest.mark.parametrize("problem,solver", [("neel", Solver.Heun_Strong), ("brown_neel", Solver.Millstein)])
+def test_two_particles_per_thread(ctx, tmp_path, problem, solver):
+    """FP32 with two particles per thread against one: each particle runs the same source
+    arithmetic in another instantiation, so trajectories agree to FP32 round-off
+    (checked within 1e-5 over 20 windows) and the autotuner may choose either."""
+    make = provider.neel_relaxation if problem == "neel" else provider.brown_neel_relaxation
+    spec = make(n=40000, steps=2100, oversampling=100, solver=solver, precision=Precision.FP32)
+    key = f"{int(spec.problem)}/{int(spec.anisotropy)}/{int(spec.solver)}/1/0"
+    f = tmp_path / "shape.txt"
+    f.write_text(f"{key} 128 0 1000 0 1\n")
+    sp.Context.tuning_load(f)
+    one = ctx.simulate(spec, trajectories=True)
+    assert ctx.launch_config(spec)["particles_per_thread"] == 1
+    f.write_text(f"{key} 128 0 1000 0 2\n")
+    sp.Context.tuning_load(f)
+    assert ctx.launch_config(spec)["particles_per_thread"] == 2
+    two = ctx.simulate(spec, trajectories=True)
+    np.testing.assert_allclose(two.trajectories, one.trajectories, rtol=0, atol=1e-5)
+    np.testing.assert_allclose(two.mean, one.mean, rtol=0, atol=1e-6)
+    np.testing.assert_array_equal(two.weight, one.weight)
+    with sp.Server(ctx) as srv:  # the server's group launch takes the same shape
+        res = srv.wait(srv.submit(spec))[0]
+    np.testing.assert_allclose(res.mean, two.mean, rtol=0, atol=1e-6)
 
 
 def test_tuned_shapes_reach_the_server(ctx, tmp_path):

@@ -29,7 +29,8 @@ def test_defaults_without_tuning():
     spec = provider.brown_neel_relaxation(n=65536, steps=20000, oversampling=1000, precision=Precision.FP32)
     s = _shape(spec)
     # CTA size halved from 256 until there are >= 2 CTAs per SM (148 SMs), down to 32
-    assert s == {"block": 128, "persistent": 0, "chunk_steps": 10000, "particle_steps_per_s": 0.0}
+    assert s == {"block": 128, "persistent": 0, "chunk_steps": 10000, "particles_per_thread": 1,
+                 "particle_steps_per_s": 0.0}
     small = provider.brown_neel_relaxation(n=4000, steps=20000, oversampling=1000)
     assert _shape(small)["block"] == 32
 
@@ -41,7 +42,8 @@ def test_loaded_shape_applies_to_its_key_only(tmp_path):
     f = tmp_path / "tune.txt"
     f.write_text(f"{key} 128 1 30000 1.5e10\n")
     assert load().sp_tuning_load(str(f).encode()) == 0
-    assert _shape(bn) == {"block": 128, "persistent": 1, "chunk_steps": 30000, "particle_steps_per_s": 1.5e10}
+    assert _shape(bn) == {"block": 128, "persistent": 1, "chunk_steps": 30000, "particles_per_thread": 1,
+                          "particle_steps_per_s": 1.5e10}
     heun = provider.brown_neel_relaxation(n=65536, steps=20000, oversampling=1000, solver=Solver.Heun_Strong,
                                           precision=Precision.FP32)
     assert _shape(heun)["persistent"] == 0 and _shape(heun)["block"] == 128
@@ -54,13 +56,35 @@ def test_loaded_shape_applies_to_its_key_only(tmp_path):
     assert _shape(tiny)["block"] == 32
 
 
+def test_particles_per_thread(tmp_path):
+    """Two particles per thread are kept for FP32 in-kernel-noise keys with tiles of at
+    least 64 particles, and fall back to one otherwise (FP64 has no such kernel)."""
+    f32 = provider.brown_neel_relaxation(n=65536, steps=20000, oversampling=1000, solver=Solver.Millstein,
+                                         precision=Precision.FP32)
+    f64 = provider.brown_neel_relaxation(n=65536, steps=20000, oversampling=1000, solver=Solver.Millstein)
+    tiny = provider.brown_neel_relaxation(n=5000, steps=20000, oversampling=1000, solver=Solver.Millstein,
+                                          precision=Precision.FP32)
+    k32 = f"{int(f32.problem)}/{int(f32.anisotropy)}/{int(f32.solver)}/1/0"
+    k64 = f"{int(f64.problem)}/{int(f64.anisotropy)}/{int(f64.solver)}/0/0"
+    f = tmp_path / "tune.txt"
+    f.write_text(f"{k32} 128 0 10000 3e10 2\n{k64} 128 0 10000 6e9 2\n")
+    assert load().sp_tuning_load(str(f).encode()) == 0
+    assert _shape(f32)["particles_per_thread"] == 2
+    assert _shape(f64)["particles_per_thread"] == 1
+    assert _shape(tiny)["block"] == 32 and _shape(tiny)["particles_per_thread"] == 1
+    g = tmp_path / "saved.txt"
+    assert load().sp_tuning_save(str(g).encode()) == 0
+    assert f"{k32} 128 0 10000 3e+10 2" in g.read_text()
+
+
 def test_save_load_roundtrip_and_reset(tmp_path):
     a = tmp_path / "a.txt"
     a.write_text("0/0/1/1/0 64 0 20000 2e10\n2/0/2/0/0 256 1 10000 4e9\n")
     assert load().sp_tuning_load(str(a).encode()) == 0
     b = tmp_path / "b.txt"
     assert load().sp_tuning_save(str(b).encode()) == 0
-    assert sorted(b.read_text().split("\n")) == sorted(["0/0/1/1/0 64 0 20000 2e+10", "2/0/2/0/0 256 1 10000 4e+09", ""])
+    assert sorted(b.read_text().split("\n")) == sorted(["0/0/1/1/0 64 0 20000 2e+10 1", "2/0/2/0/0 256 1 10000 4e+09 1",
+                                                         ""])
     load().sp_tuning_reset()
     c = tmp_path / "c.txt"
     assert load().sp_tuning_save(str(c).encode()) == 0
@@ -68,7 +92,7 @@ def test_save_load_roundtrip_and_reset(tmp_path):
 
 
 @pytest.mark.parametrize("text", ["0/0/1/1 64 0 100 1\n", "0/0/1/1/0 48 0 100 1\n", "0/0/1/1/0 64 0\n",
-                                  "0/0/1/1/0 64 0 0 1\n"])
+                                  "0/0/1/1/0 64 0 0 1\n", "0/0/1/1/0 64 0 100 1 3\n"])
 def test_malformed_tuning_files_are_refused(tmp_path, text):
     f = tmp_path / "bad.txt"
     f.write_text(text)
