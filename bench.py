@@ -250,6 +250,7 @@ def batched_leg(ctx, count, step_scale, seed=0x5EED0004, serial_sample=32):
     serial_s = time.perf_counter() - t
     return {"sets": count, "value": ps / wall, "unit": UNIT, "wall_s": wall, "particle_steps": ps,
             "max_latency_ms": max(lat),
+            "launch_shapes": {s.solver.name: ctx.launch_config(s) for s in specs[:2]},
             "one_at_a_time": {"value": sum(s.n * s.integrated_steps for s in sample) / serial_s, "sets": len(sample)},
             "workload": f"Neel, N ~ logU[1e3, 6.4e4], S ~ logU[1e5, 1e7] x {step_scale}, |B| ~ U[1, 25] mT, "
                         "f ~ logU[1e4, 1e6] Hz, K ~ U[5e3, 3e4] J/m^3, alpha ~ U[0.02, 0.3], Heun / Millstein "

@@ -379,7 +379,7 @@ __global__ void __launch_bounds__(kMaxBlock / PPT) step_kernel(const EnsDev* __r
 #pragma unroll
                         for (int j = 0; j < Mn; ++j) w[j] = dwp[(g * Mn + j) * Np + p[k]];
                     } else {
-                        philox_increments<R, Mn>(seed, pid, g, sqdt, m2dt, w);
+                        philox_increments<R, Mn, Prob::kCalledMath>(seed, pid, g, sqdt, m2dt, w);
                     }
                     if constexpr (SOLVER == kHeunNotConsistent) {
                         R w2[Mn];

@@ -139,6 +139,21 @@ __device__ __forceinline__ uint4 philox_block(unsigned long long seed, unsigned 
 }
 
 // Box-Muller on u = (w + 1/2) 2^-32.  npairs = 1 or 2 pairs of normals.
+// inlined form, for kernels whose step loop is small enough for the instruction cache
+__device__ __forceinline__ void box_muller_inline(uint4 w, int npairs, double* z) {
+    const double inv = 2.3283064365386963e-10, half = 1.1641532182693481e-10;  // 2^-32, 2^-33
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        if (k >= npairs) break;
+        const uint32_t a = k ? w.z : w.x, b = k ? w.w : w.y;
+        const double u0 = fma(static_cast<double>(a), inv, half), u1 = fma(static_cast<double>(b), inv, half);
+        const double r = ::sqrt(-2.0 * ::log(u0));
+        double s, c;
+        ::sincospi(2.0 * u1, &s, &c);
+        z[2 * k] = r * c;
+        z[2 * k + 1] = r * s;
+    }
+}
 __device__ __forceinline__ void box_muller(uint4 w, int npairs, double* z) {
     const SinCosD p = box_muller_pair_d(w.x, w.y);
     z[0] = p.c;
@@ -199,13 +214,26 @@ __device__ __forceinline__ void philox_normals(unsigned long long seed, unsigned
 }
 
 // Wiener increments dW = sqrt(dt) z of one step (m = 3 or 6, calls 0-1).  FP64 scales
-// the unit normals; FP32 folds dt into the Box-Muller radius, sqrt(-2 dt ln u), which
-// saves the m multiplications.
-template <class R, int Mdim>
+// the unit normals (CALLED: through the shared Box-Muller routine, for kernels whose
+// physics already fills the instruction cache; else inlined, which keeps a small
+// latency-bound step loop free of calls); FP32 folds dt into the Box-Muller radius,
+// sqrt(-2 dt ln u), which saves the m multiplications.
+template <class R, int Mdim, bool CALLED = true>
 __device__ __forceinline__ void philox_increments(unsigned long long seed, unsigned long long pid,
                                                   unsigned long long step, R sqdt, R m2dt, R* w) {
     if constexpr (sizeof(R) == 8) {
-        philox_normals<R, Mdim>(seed, pid, step, w);
+        if constexpr (CALLED) {
+            philox_normals<R, Mdim>(seed, pid, step, w);
+        } else {
+            double t[4];
+            box_muller_inline(philox_block(seed, pid, step, 0u), 2, t);
+            w[0] = t[0]; w[1] = t[1]; w[2] = t[2];
+            if (Mdim > 3) {
+                w[3] = t[3];
+                box_muller_inline(philox_block(seed, pid, step, 1u), 1, t);
+                w[4] = t[0]; w[5] = t[1];
+            }
+        }
 #pragma unroll
         for (int j = 0; j < Mdim; ++j) w[j] = w[j] * sqdt;
     } else {

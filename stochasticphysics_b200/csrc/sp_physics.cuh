@@ -152,6 +152,7 @@ template <class R, int A>
 struct NeelCart {
     static constexpr int D = 3, Mn = 3, OUT = 3;
     static constexpr bool kHasJacobian = true;
+    static constexpr bool kCalledMath = false;  // FP64 Box-Muller through the shared routine
     struct Par {
         R NF1, NF2, Dp, pre1, pre2, pF, twoalpha;
         V3<R> z, x, y;
@@ -291,6 +292,7 @@ template <class R, int A>
 struct NeelSph {
     static constexpr int D = 2, Mn = 3, OUT = 3;
     static constexpr bool kHasJacobian = true;
+    static constexpr bool kCalledMath = true;  // FP64 Box-Muller through the shared routine
     static constexpr bool kHasExactJacobian = false;
     struct Par {
         R NF1, NF2, Dp, DN, pF, twoalpha;
@@ -521,6 +523,7 @@ template <class R, int A>
 struct BrownNeelEuler {
     static constexpr int D = 5, Mn = 6, OUT = 9;
     static constexpr bool kHasJacobian = false;  // assert(false) in the reference (:605-626)
+    static constexpr bool kCalledMath = true;  // FP64 Box-Muller through the shared routine
     static constexpr bool kHasExactJacobian = false;
     struct Par {
         R a, bpd, d, cT, pF, cF, dDN, bpdDN, aDN, adDN2, d2fDN2, cF2h, nd;
@@ -705,9 +708,10 @@ struct BrownNeelEuler {
     static __device__ __forceinline__ void bdw(const Par& q, const R*, const Cache& c, const R* w, R* r) {
         const V3<R> wA = v3(w[0], w[1], w[2]), wB = v3(w[3], w[4], w[5]);
         const V3<R> cwA = q.cF * wA;
-        const V3<R> b = eproj(c, cwA + cross(q.dDN * c.md, wB));
+        const V3<R> mxw = cross(c.md, wB);  // shared by both rows
+        const V3<R> b = eproj(c, cwA + q.dDN * mxw);
         r[0] = b.x; r[1] = b.y; r[2] = b.z;
-        sproj(c, cwA + q.bpdDN * cross(c.md, wB) - q.aDN * wB, r + 3);
+        sproj(c, cwA + q.bpdDN * mxw - q.aDN * wB, r + 3);
     }
     // :499-601 with the prefactors grouped: adDN2 = a d DN^2, d2fDN2 = d^2 DN^2 / 4, cF2h = (c DB)^2 / 2
     static __device__ __forceinline__ void drift(const Par& q, const R* y, const Cache& c, R* r) {
@@ -765,6 +769,7 @@ template <class R, int A>
 struct BrownNeelCart {
     static constexpr int D = 6, Mn = 6, OUT = 6;
     static constexpr bool kHasJacobian = true;  // both Jacobians are zero in the reference (.h:119-128)
+    static constexpr bool kCalledMath = false;  // FP64 Box-Muller through the shared routine
     static constexpr bool kHasExactJacobian = false;
     struct Par {
         R a, bpd, d, cT, pF, cF, dDN, bpdDN, aDN, cF2, adDN2, hd2DN2, ndrift, cFe;
