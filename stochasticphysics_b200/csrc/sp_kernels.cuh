@@ -361,13 +361,30 @@ __global__ void __launch_bounds__(kMaxBlock / PPT) step_kernel(const EnsDev* __r
         unsigned int wpos = static_cast<unsigned int>(s0 % W);
         const unsigned int W32 = static_cast<unsigned int>(W);
         const R* dwp = static_cast<const R*>(e.dw);
+        static_assert(kFieldTile % 4 == 0, "the increment ring assumes tiles of whole ring turns");
+
+        // injected increments stream from HBM: a ring of the next PF steps' increments keeps
+        // PF steps of loads in flight per thread (the loads of one step alone cannot hide
+        // the memory latency); slot j of the ring holds the steps j, j + PF, ...
+        constexpr int PF = INJECT ? (Mn > 3 ? 2 : 4) : 1;
+        R ring[PPT][PF][Mn];
+        if constexpr (INJECT) {
+#pragma unroll
+            for (int k = 0; k < PPT; ++k)
+#pragma unroll
+                for (int j = 0; j < PF; ++j)
+                    if (active[k] && static_cast<unsigned long long>(j) < nsteps)
+#pragma unroll
+                        for (int m = 0; m < Mn; ++m) ring[k][j][m] = dwp[((s0 + j) * Mn + m) * Np + p[k]];
+        }
 
         for (unsigned long long t0 = 0; t0 < nsteps; t0 += kFieldTile) {
             const int len = static_cast<int>(min(static_cast<unsigned long long>(kFieldTile), nsteps - t0));
             __syncwarp();
             for (int i = threadIdx.x & 31; i < 3 * len; i += 32) (&sB[0][0])[i] = ftab[3 * t0 + i];
             __syncwarp();
-            for (int i = 0; i < len; ++i) {
+            // one step of every particle of the thread; winj: the injected increments
+            auto one_step = [&](int i, const R (*winj)[Mn]) {
                 const unsigned long long g = s0 + t0 + i;
                 const R B[3] = {sB[i][0], sB[i][1], sB[i][2]};
 #pragma unroll
@@ -377,7 +394,7 @@ __global__ void __launch_bounds__(kMaxBlock / PPT) step_kernel(const EnsDev* __r
                     R w[Mn];
                     if constexpr (INJECT) {
 #pragma unroll
-                        for (int j = 0; j < Mn; ++j) w[j] = dwp[(g * Mn + j) * Np + p[k]];
+                        for (int j = 0; j < Mn; ++j) w[j] = winj[k][j];
                     } else {
                         philox_increments<R, Mn, Prob::kCalledMath>(seed, pid, g, sqdt, m2dt, w);
                     }
@@ -419,6 +436,30 @@ __global__ void __launch_bounds__(kMaxBlock / PPT) step_kernel(const EnsDev* __r
                         }
                     }
                 }
+            };
+            if constexpr (INJECT) {
+                // kFieldTile is a multiple of PF, so step s0 + t0 + i sits in ring slot i % PF
+                for (int i0 = 0; i0 < len; i0 += PF) {
+#pragma unroll
+                    for (int j = 0; j < PF; ++j) {
+                        const int i = i0 + j;
+                        if (i < len) {  // uniform
+                            R cur[PPT][Mn];
+                            const unsigned long long gn = t0 + i + PF;  // steps after s0
+#pragma unroll
+                            for (int k = 0; k < PPT; ++k) {
+#pragma unroll
+                                for (int m = 0; m < Mn; ++m) cur[k][m] = ring[k][j][m];
+                                if (active[k] && gn < nsteps)
+#pragma unroll
+                                    for (int m = 0; m < Mn; ++m) ring[k][j][m] = dwp[((s0 + gn) * Mn + m) * Np + p[k]];
+                            }
+                            one_step(i, cur);
+                        }
+                    }
+                }
+            } else {
+                for (int i = 0; i < len; ++i) one_step(i, nullptr);
             }
         }
 #pragma unroll
