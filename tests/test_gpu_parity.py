@@ -325,6 +325,34 @@ def test_fp32_form_close_to_fp64(ctx):
         assert np.nanmax(d) < bound, f"{problem.name}/{solver.name}: FP32 mean error {np.nanmax(d):.2e}"
 
 
+def test_fp32_difference_is_unbiased_path_noise(ctx):
+    """Why the FP32 and FP64 means part after the first windows.  Brown+Neel Euler Heun,
+    4096 particles x 1e5 steps, same Philox stream.  Each particle's FP32 path drifts from
+    its FP64 path by accumulated rounding (median of the largest window difference about
+    2e-3), with random sign across particles, so the drift averages out of the ensemble
+    mean; and a small fraction of particles take a different path altogether (a barrier
+    crossing in one run and not the other), as an FP64 run started from Euler angles
+    perturbed by 1e-7 rad, FP32 rounding size, also shows.  The mean difference is
+    therefore Monte-Carlo, bounded by the two-sample standard error, not an FP32 bias."""
+    n = 4096
+    spec = small_spec(Problem.BrownAndNeelEulerSpherical, Solver.Heun_Strong, n=n, steps=100000, W=1000)
+    rng = np.random.default_rng(5)
+    pert = dataclasses.replace(spec, orientation=spec.orientation + 1e-7 * rng.standard_normal(spec.orientation.shape))
+    r64 = ctx.simulate(spec, trajectories=True)
+    r64p = ctx.simulate(pert, trajectories=True)
+    r32 = ctx.simulate(dataclasses.replace(spec, precision=Precision.FP32), trajectories=True)
+    diff32 = r32.trajectories[:, :, 6:9] - r64.trajectories[:, :, 6:9]
+    d32 = np.abs(diff32).max(axis=(1, 2))
+    dp = np.abs(r64p.trajectories[:, :, 6:9] - r64.trajectories[:, :, 6:9]).max(axis=(1, 2))
+    assert np.median(d32) < 1e-2 and np.median(dp) < 1e-5
+    divp = (dp > 0.1).mean()
+    assert 0 < divp < 0.02, f"perturbed FP64 diverged fraction {divp:.4f}"
+    last = diff32[:, -1, :]  # signed per-particle difference in the last window
+    assert np.all(np.abs(last.mean(axis=0)) < 4 * last.std(axis=0) / math.sqrt(n))
+    se = math.sqrt(2.0 / (3.0 * n))
+    assert np.abs(r32.mean[:, 6:9] - r64.mean[:, 6:9]).max() < 4 * se
+
+
 LANGEVIN = [(p, prec) for p in (Problem.Neel, Problem.NeelSpherical, Problem.BrownAndNeelEulerSpherical)
             for prec in (Precision.FP64, Precision.FP32)]
 
