@@ -293,7 +293,8 @@ struct WindowSum<float, OUT> {
 // One tile = blockDim.x * PPT particles of one ensemble; thread t integrates particles
 // first + k blockDim.x + t, k < PPT.  With PPT = 2 each thread carries two independent
 // step chains, which the scheduler interleaves (instruction-level parallelism in a
-// latency-bound loop).  Each particle's arithmetic is the same for every PPT.
+// latency-bound loop).  Each particle runs the same source arithmetic for every PPT; the
+// instantiations are compiled separately, so results agree to rounding.
 template <int PROB, class R, int A, int SOLVER, bool INJECT, int PPT>
 __global__ void __launch_bounds__(kMaxBlock / PPT) step_kernel(const EnsDev* __restrict__ ensembles,
                                                                const TileDesc* __restrict__ tiles, int ntiles) {
