@@ -267,6 +267,7 @@ def plain_neel_leg(ctx, torch, cpu_steps=20000):
     host cores for comparison."""
     import oracle
     from stochasticphysics_b200 import provider
+    from stochasticphysics_b200._abi import Precision
 
     spec = provider.neel_relaxation()
     st = torch.cuda.Stream()
@@ -282,12 +283,20 @@ def plain_neel_leg(ctx, torch, cpu_steps=20000):
     ctx.simulate(spec)
     e2e_s = time.perf_counter() - t
     ps = spec.n * spec.integrated_steps
+    with ctx.ensemble(dataclasses.replace(spec, precision=Precision.FP32)) as e:
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        e.advance(spec.integrated_steps, st.cuda_stream)
+        b.record(st)
+        torch.cuda.synchronize()
+        fp32_s = a.elapsed_time(b) / 1e3
     cpu = dataclasses.replace(spec, number_of_steps=cpu_steps + 100)
     t = time.perf_counter()
     oracle.simulate(cpu, threads=os.cpu_count() or 1)
     cpu_s = time.perf_counter() - t
     cpu_rate = spec.n * cpu_steps / cpu_s
     return {"value": ps / dev_s, "unit": UNIT, "run_s": dev_s, "e2e_run_s": e2e_s,
+            "fp32": {"value": ps / fp32_s, "run_s": fp32_s},
             "nonfinite_particles": res.stats["nonfinite_particles"],
             "note": "the Cartesian Heun step does not renormalise |m| (the reference's own norm handling); "
                     "at dt = 1e-11 s the precession step omega dt is ~0.09, |m| drifts and some particles "

@@ -53,6 +53,24 @@ def test_ini_run_matches_api_and_oracle(tmp_path, main, n, particles):
     assert np.max(np.abs(mean - ref["mean"])) <= ABS_MEAN
 
 
+@pytest.mark.parametrize("solver", ["ExplicitStrong_1.0", "WeakTest", "Heun_NotConsistent"])
+def test_reference_disabled_solvers_run_from_ini(tmp_path, solver):
+    """The solvers the reference's manager switches off, selected by name in an .ini
+    (with Approximation_of_double_noise_integral where it is read): the driver's run
+    equals the API run of the same description and the oracle's mean."""
+    path = _copy(tmp_path, "legacy_neel_spherical.ini", 10, ("legacy_particle_small.ini", "legacy_particle_large.ini"))
+    path.write_text(path.read_text().replace("'Heun_Strong'", f"'{solver}'\nApproximation_of_double_noise_integral = 2"))
+    rec = settings.run_ini(path, seed=5)["Mean_Results"]
+    spec = settings.load_ini(path, seed=5)
+    with sp.Context(0) as ctx:
+        api = ctx.simulate(spec)
+    mean = np.array(rec["Results"], dtype=float)
+    np.testing.assert_array_equal(mean, api.mean)
+    ref = oracle.simulate(spec)
+    ok = np.isfinite(ref["mean"]).all(axis=1)
+    assert np.max(np.abs(mean[ok] - ref["mean"][ok])) <= 1e-9
+
+
 def test_system_matrix_sweep_equals_per_voxel_runs(tmp_path):
     """Every voxel of the batched sweep equals a separate run of the same voxel
     description (same offset field, same Philox key) bit for bit."""
