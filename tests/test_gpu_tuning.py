@@ -56,8 +56,10 @@ def test_results_do_not_depend_on_the_launch_shape(ctx, tmp_path, shape):
     np.testing.assert_array_equal(got.weight, ref.weight)
 
 
-@pytest.mark.parametrize("problem,solver", [("neel", Solver.Heun_Strong), ("brown_neel", Solver.Millstein)])
-def test_two_particles_per_thread(ctx, tmp_path, problem, solver):
+@pytest.mark.parametrize("problem,solver,persistent", [("neel", Solver.Heun_Strong, 0), ("brown_neel", Solver.Millstein, 0),
+                                                      ("brown_neel", Solver.Heun_Strong, 1),
+                                                      ("neel", Solver.Implicit_Midpoint, 1)])
+def test_two_particles_per_thread(ctx, tmp_path, problem, solver, persistent):
     """FP32 with two particles per thread against one: each particle runs the same source
     arithmetic in another instantiation, so trajectories agree to FP32 round-off
     (checked within 1e-5 over 20 windows) and the autotuner may choose either."""
@@ -65,11 +67,11 @@ def test_two_particles_per_thread(ctx, tmp_path, problem, solver):
     spec = make(n=40000, steps=2100, oversampling=100, solver=solver, precision=Precision.FP32)
     key = f"{int(spec.problem)}/{int(spec.anisotropy)}/{int(spec.solver)}/1/0"
     f = tmp_path / "shape.txt"
-    f.write_text(f"{key} 128 0 1000 0 1\n")
+    f.write_text(f"{key} 128 {persistent} 1000 0 1\n")
     sp.Context.tuning_load(f)
     one = ctx.simulate(spec, trajectories=True)
     assert ctx.launch_config(spec)["particles_per_thread"] == 1
-    f.write_text(f"{key} 128 0 1000 0 2\n")
+    f.write_text(f"{key} 128 {persistent} 1000 0 2\n")
     sp.Context.tuning_load(f)
     assert ctx.launch_config(spec)["particles_per_thread"] == 2
     two = ctx.simulate(spec, trajectories=True)
