@@ -50,7 +50,9 @@ def test_ctypes_layout_matches_c(tmp_path):
     fields = {
         "sp_ensemble_desc": _abi.sp_ensemble_desc, "sp_particles": _abi.sp_particles, "sp_field_desc": _abi.sp_field_desc,
         "sp_problem_settings": _abi.sp_problem_settings, "sp_result": _abi.sp_result, "sp_stats": _abi.sp_stats,
-        "sp_server_config": _abi.sp_server_config,
+        "sp_server_config": _abi.sp_server_config, "sp_launch_config": _abi.sp_launch_config,
+        "sp_dist": _abi.sp_dist, "sp_particle_template": _abi.sp_particle_template,
+        "sp_provider_desc": _abi.sp_provider_desc,
     }
     lines = []
     for cname, cls in fields.items():
