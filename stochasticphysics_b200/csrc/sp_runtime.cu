@@ -334,24 +334,41 @@ void Ensemble::upload_and_init(const sp_ensemble_desc& d) {
     const sp_particles& q = d.particles;
     const bool brown = d.problem == SP_PROBLEM_BROWN_AND_NEEL || d.problem == SP_PROBLEM_BROWN_AND_NEEL_EULER_SPHERICAL;
     // one staging buffer: 7 scalars + 6 vector components per particle (+ K_cubic and the
-    // uniaxial rotation for the uniaxial+cubic anisotropy)
+    // uniaxial rotation for the uniaxial+cubic anisotropy), in the context's pinned buffer
+    // (a pageable vector if pinned memory cannot be had)
     const bool uc = d.anisotropy == SP_ANISOTROPY_UNIAXIAL_CUBIC;
-    std::vector<double> host(n * (uc ? 17 : 13), 0.0);
+    const size_t need = n * (uc ? 17 : 13);
+    std::lock_guard<std::mutex> lk(ctx->stage_mu);
+    if (ctx->stage_doubles < need) {
+        if (ctx->stage) cudaFreeHost(ctx->stage);
+        ctx->stage = nullptr;
+        ctx->stage_doubles = 0;
+        if (cudaMallocHost(reinterpret_cast<void**>(&ctx->stage), need * 8) == cudaSuccess) ctx->stage_doubles = need;
+        else { ctx->stage = nullptr; cudaGetLastError(); }
+    }
+    std::vector<double> pageable;
+    double* host = ctx->stage;
+    if (!host) {
+        pageable.resize(need);
+        host = pageable.data();
+    }
     const double* src[7] = {q.magnetic_radius, q.saturation_magnetisation, q.damping_constant, q.gyromagnetic_ratio,
                             q.anisotropy_constant, brown ? q.hydrodynamic_radius : nullptr, brown ? q.viscosity : nullptr};
-    for (int k = 0; k < 7; ++k)
-        if (src[k]) std::memcpy(host.data() + k * n, src[k], n * 8);
-    std::memcpy(host.data() + 7 * n, q.orientation, n * 24);
-    std::memcpy(host.data() + 10 * n, q.magnetisation, n * 24);
+    for (int k = 0; k < 7; ++k) {
+        if (src[k]) std::memcpy(host + k * n, src[k], n * 8);
+        else std::memset(host + k * n, 0, n * 8);
+    }
+    std::memcpy(host + 7 * n, q.orientation, n * 24);
+    std::memcpy(host + 10 * n, q.magnetisation, n * 24);
     if (uc) {
-        std::memcpy(host.data() + 13 * n, q.cubic_constant, n * 8);
-        std::memcpy(host.data() + 14 * n, q.uniaxial_rotation, n * 24);
+        std::memcpy(host + 13 * n, q.cubic_constant, n * 8);
+        std::memcpy(host + 14 * n, q.uniaxial_rotation, n * 24);
     }
     double* dev = nullptr;
-    check_cuda(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&dev), host.size() * 8, ctx->pool, stream),
+    check_cuda(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&dev), need * 8, ctx->pool, stream),
                "cudaMallocFromPoolAsync");
-    check_cuda(cudaMemcpyAsync(dev, host.data(), host.size() * 8, cudaMemcpyHostToDevice, stream), "upload particles");
-    h2d_bytes += host.size() * 8;
+    check_cuda(cudaMemcpyAsync(dev, host, need * 8, cudaMemcpyHostToDevice, stream), "upload particles");
+    h2d_bytes += need * 8;
     RawParticles rp;
     rp.radius = dev; rp.Ms = dev + n; rp.alpha = dev + 2 * n; rp.gamma = dev + 3 * n; rp.K = dev + 4 * n;
     rp.rh = dev + 5 * n; rp.viscosity = dev + 6 * n; rp.euler = dev + 7 * n; rp.mag = dev + 10 * n;
@@ -366,7 +383,7 @@ void Ensemble::upload_and_init(const sp_ensemble_desc& d) {
     launches += 3;
     g_launch_count += 3;
     check_cuda(cudaFreeAsync(dev, stream), "cudaFreeAsync");
-    // the host staging buffer must outlive the asynchronous copy
+    // the staging buffer must outlive the asynchronous copy (and stays locked until then)
     check_cuda(cudaStreamSynchronize(stream), "init");
 }
 
@@ -567,6 +584,7 @@ sp_status sp_destroy(sp_context* ctx) {
         cudaDeviceSynchronize();  // frees issued on ensemble streams have reached the pool
         cudaMemPoolDestroy(ctx->pool);
     }
+    if (ctx->stage) cudaFreeHost(ctx->stage);
     delete ctx;
     return SP_OK;
     SP_GUARD_END

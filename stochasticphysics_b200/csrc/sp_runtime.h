@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -22,6 +23,12 @@ struct sp_context {
     // (release threshold = max), so repeated runs and server requests reuse it
     // instead of paying for cudaMalloc / cudaFree each time
     cudaMemPool_t pool = nullptr;
+    // pinned host staging for particle uploads, grown on demand and reused across calls
+    // (pageable copies go through the driver's own bounce buffers at a fraction of the
+    // bandwidth); callers uploading at the same time take turns on the mutex
+    std::mutex stage_mu;
+    double* stage = nullptr;
+    size_t stage_doubles = 0;
 };
 
 namespace sp {
