@@ -134,17 +134,17 @@ def profiled_traffic_per_particle():
     return (float(m.group(1)), path.name) if m else (None, None)
 
 
-def profiled_instructions():
-    """Thread-instructions per particle-step of the FP32 step kernels (Millstein, Heun),
-    from the committed ncu summary."""
+def profiled_instructions(prefix=""):
+    """Thread-instructions per particle-step of the step kernels (Millstein, Heun), from the
+    committed ncu summary: FP32 (prefix "") or FP64 (prefix "fp64_")."""
     import re
     path = ROOT / "profiles" / "step_kernel_instruction_counts_65536.md"
     try:
         text = path.read_text()
     except OSError:
         return None, None
-    m = re.search(r"thread_instructions_per_particle_step_millstein:\s*([0-9.]+)", text)
-    h = re.search(r"thread_instructions_per_particle_step_heun:\s*([0-9.]+)", text)
+    m = re.search(rf"thread_instructions_per_particle_step_{prefix}millstein:\s*([0-9.]+)", text)
+    h = re.search(rf"thread_instructions_per_particle_step_{prefix}heun:\s*([0-9.]+)", text)
     return ((float(m.group(1)), float(h.group(1))) if m and h else None), path.name
 
 
@@ -629,6 +629,13 @@ def main():
                      "instructions_per_particle_step": {"Millstein": ipp[0], "Heun": ipp[1]},
                      "source": f"profiles/{isrc}: ncu smsp__inst_executed per particle-step x measured FP32 rate; "
                                "peak = SMs x 4 schedulers x 32 lanes x median SM clock"}
+            ipp64, _ = profiled_instructions("fp64_")
+            if ipp64 is not None:
+                clk64 = results["FP64"]["clocks"].get("sm_mhz") or 1965.0
+                peak64_ti = sms * 4 * 32 * clk64 * 1e6 / 1e12
+                ach64_ti = v64 / world * (ipp64[0] + ipp64[1]) / 2 / 1e12
+                issue["fp64"] = {"achieved": ach64_ti, "peak": peak64_ti, "frac": ach64_ti / peak64_ti,
+                                 "instructions_per_particle_step": {"Millstein": ipp64[0], "Heun": ipp64[1]}}
         cpu = None if args.no_cpu_baseline else cpu_baseline()
         c32 = results["FP32"]["clocks"]
         line = {
