@@ -1,0 +1,34 @@
+"""bench.py on the CPU: the CPU-baseline sample and the reference arm.
+
+Only whole windows are integrated (sample 0 is the initial state), so a CPU sample
+must be sized in windows; a sample shorter than the workload's window would time set-up
+alone.  The reference arm must print one JSON line with the driver's keys.
+"""
+import json
+import subprocess
+import sys
+from pathlib import Path
+
+import bench
+
+ROOT = Path(__file__).resolve().parents[1]
+
+
+def test_cpu_sample_integrates_the_steps_it_reports():
+    for steps in (300, 2000):
+        r = bench.cpu_baseline(steps_sample=steps, n=64)
+        assert r["value"] > 0 and f"x {steps} integrated steps" in r["sample"]
+
+
+def test_reference_arm_prints_one_json_line():
+    p = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--impl", "reference", "--steps", "1", "--warmup", "3",
+                        "--n-particles", "512"], capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert p.returncode == 0, p.stderr
+    lines = [ln for ln in p.stdout.splitlines() if ln.strip()]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    for key in ("impl", "metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step", "higher_is_better",
+                "scaling", "vs_baseline", "dtype", "data", "config", "cpu_baseline", "e2e"):
+        assert key in d, key
+    assert d["impl"] == "reference" and d["value"] > 0
+    assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["value"] == d["value"]
