@@ -353,6 +353,23 @@ def test_fp32_difference_is_unbiased_path_noise(ctx):
     assert np.abs(r32.mean[:, 6:9] - r64.mean[:, 6:9]).max() < 4 * se
 
 
+@pytest.mark.parametrize("problem,solver", [(Problem.Neel, Solver.Heun_Strong),
+                                            (Problem.BrownAndNeelEulerSpherical, Solver.EulerMaruyama)])
+def test_philox_mean_within_three_standard_errors_of_independent_noise(ctx, problem, solver):
+    """The in-kernel RNG against independent noise, as the reference's own generator would
+    be: the FP64 GPU run with Philox increments and the oracle run with independently drawn
+    (injected) increments of the same particles agree window by window within 3 standard
+    errors of the paired difference (per particle: GPU window mean minus oracle window
+    mean); at most 2 % of the (window, component) pairs may exceed 3 and none 5."""
+    n = 4096
+    spec = small_spec(problem, solver, n=n, steps=5000, W=250)
+    gpu = ctx.simulate(spec, trajectories=True)
+    ref = oracle.simulate(provider.with_injected_noise(spec, seed=77), trajectories=True)
+    d = gpu.trajectories[:, 1:, -3:] - ref["trajectories"][:, 1:, -3:]
+    z = np.abs(d.mean(axis=0)) / (d.std(axis=0) / math.sqrt(n))
+    assert (z > 3).mean() <= 0.02 and z.max() < 5, f"max z {z.max():.2f}, share above 3 {(z > 3).mean():.3f}"
+
+
 LANGEVIN = [(p, prec) for p in (Problem.Neel, Problem.NeelSpherical, Problem.BrownAndNeelEulerSpherical)
             for prec in (Precision.FP64, Precision.FP32)]
 
