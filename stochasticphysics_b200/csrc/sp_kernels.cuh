@@ -426,6 +426,10 @@ __global__ void __launch_bounds__(kMaxBlock / PPT) step_kernel(const EnsDev* __r
                     for (int k = 0; k < PPT; ++k) {
                         const double mom = active[k] ? e.moment[p[k]] : 0.0;
                         double* const partial = e.partial + ((p[k] >> 5) * e.slots + slot) * OUT;
+                        // the butterfly leaves every lane with the same sums; lane c keeps
+                        // component c, and the warp writes its OUT sums in one coalesced store
+                        const int lane = threadIdx.x & 31;
+                        double mine = 0.0;
 #pragma unroll
                         for (int c = 0; c < OUT; ++c) {
                             const R v = active[k] ? acc[k].get_sum(c) / static_cast<R>(static_cast<double>(W)) : R(0);
@@ -433,8 +437,9 @@ __global__ void __launch_bounds__(kMaxBlock / PPT) step_kernel(const EnsDev* __r
                             const double vd = static_cast<double>(v);
                             if (traj && active[k]) traj[(kw * OUT + c) * Np + p[k]] = vd;
                             const double ws = warp_sum(active[k] ? weight_of<PROB>(c, mom) * vd : 0.0);
-                            if ((threadIdx.x & 31) == 0) partial[c] = ws;
+                            if (lane == c) mine = ws;
                         }
+                        if (lane < OUT) partial[lane] = mine;
                     }
                 }
             };
