@@ -14,8 +14,8 @@ Heun) on the device-resident state, i.e. 2 x 65536 x 10000 particle-steps.
                sums), device-resident, CUDA-event timed, max over ranks
   fp64_plain   the same steps with the plain FP64 kernel
   e2e          the same metric through the public C ABI with host buffers: per step
-               sp_simulate of both ensembles (upload, 10000 steps, results back); the
-               two submitted together to the server is reported beside it
+               both ensembles submitted together to the server (upload, 10000 steps,
+               results back); sp_simulate one after the other is reported beside it
   cpu_baseline the CPU oracle (restatement of the reference formulas) on all host
                cores, rank 0 only, on a bounded sample of the same workload
   serving      continuous-batching leg (N=1): Poisson arrivals of mixed Neel /
@@ -148,7 +148,7 @@ def profiled_instructions(prefix=""):
     return ((float(m.group(1)), float(h.group(1))) if m and h else None), path.name
 
 
-def serving_leg(ctx, seconds, rate, step_scale, seed=0x5EED0005, serial_sample=48):
+def serving_leg(ctx, seconds, rate, step_scale, seed=0x5EED0005, serial_sample=48, chunk_steps=0):
     """Poisson arrivals of mixed Neel / BrownAndNeelEulerSpherical requests with the
     batched-set distributions and the 2D Lissajous field, served by the continuous-
     batching server in FP32; latency = submit -> result ready (server clock).  The
@@ -173,7 +173,7 @@ def serving_leg(ctx, seconds, rate, step_scale, seed=0x5EED0005, serial_sample=4
     free, _ = __import__("torch").cuda.mem_get_info()
     budget = int(min(150e9, 0.8 * free))
     ids = [None] * len(specs)
-    with sp.Server(ctx, memory_budget_bytes=budget) as srv:
+    with sp.Server(ctx, memory_budget_bytes=budget, chunk_steps=chunk_steps) as srv:
         def submitter():
             t0 = time.perf_counter()
             for i, (ta, spec) in enumerate(zip(arrivals, specs)):
@@ -580,9 +580,9 @@ def main():
         diffs = [np.abs(a[1:kdone + 1, 6:9] - b[1:kdone + 1, 6:9]) for a, b in zip(m32, m64)]
         se_indep = math.sqrt(2.0 / (3.0 * N_PER_GPU))
 
-        # e2e through the public C ABI with host buffers: per bench step, sp_simulate of the
-        # two ensembles one after the other (host arrays in, results out); the same two
-        # submitted together to the server and waited for is reported beside it
+        # e2e through the public C ABI with host buffers: per bench step, the two ensembles
+        # submitted together to the server (host arrays in) and waited for (results out);
+        # sp_simulate of the two one after the other is reported beside it
         e2e_specs = workload_specs(N_PER_GPU, CHUNK + 1000, Precision.FP32, rank)
         for s in e2e_specs:
             ctx.simulate(s)  # warm the path
@@ -605,8 +605,8 @@ def main():
             for s in e2e_specs:
                 ctx.simulate(s)
             seq_times.append(time.perf_counter() - t)
-        e2e_server_value = world * ps_per_step * args.steps / barrier_max(sum(e2e_times))
-        e2e_value = world * ps_per_step * args.steps / barrier_max(sum(seq_times))
+        e2e_value = world * ps_per_step * args.steps / barrier_max(sum(e2e_times))
+        e2e_simulate_value = world * ps_per_step * args.steps / barrier_max(sum(seq_times))
         h2d = sum(s.n * 13 * 8 for s in e2e_specs)
         d2h = sum(o.mean.nbytes + o.weight.nbytes + o.time.nbytes + o.field.nbytes for o in outs)
         serving = batched = None
@@ -669,8 +669,8 @@ def main():
                          "fp64": {"achieved": sum(ach64) / 2, "peak": peak64, "frac": (sum(ach64) / 2) / peak64},
                          "issue": issue},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "api": "sp_simulate, the two ensembles one after the other",
-                    "sp_server_both_in_flight": e2e_server_value},
+                    "api": "sp_server_submit / sp_server_wait, the two ensembles in flight together",
+                    "sp_simulate_one_after_the_other": e2e_simulate_value},
             "gpu_launches": results["FP32"]["launches"],
             "clocks": c32,
             "cpu_baseline": cpu,

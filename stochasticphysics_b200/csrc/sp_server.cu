@@ -95,9 +95,19 @@ struct sp_server {
                (d.noise == SP_NOISE_INJECTED);
     }
 
+    // Requests join and leave a group only at chunk boundaries, so the chunk bounds how long
+    // a new request waits behind a running group.  Without a configured chunk the tuned
+    // (throughput) chunk is capped at kServeChunk steps, in whole windows.
+    static constexpr unsigned long long kServeChunk = 4000;
     LaunchConfig launch_for(const sp_ensemble_desc& d) const {
         LaunchConfig c = launch_config_for(ctx, d);
-        if (cfg.chunk_steps) c.chunk = std::max<unsigned long long>(cfg.chunk_steps, 1);
+        if (cfg.chunk_steps) {
+            c.chunk = std::max<unsigned long long>(cfg.chunk_steps, 1);
+        } else {
+            const unsigned long long W = d.oversampling;
+            const unsigned long long cap = W >= kServeChunk ? W : (kServeChunk / W) * W;
+            c.chunk = std::min(c.chunk, cap);
+        }
         return c;
     }
 
