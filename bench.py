@@ -640,7 +640,7 @@ def main():
                 ach64_ti = v64 / world * (ipp64[0] + ipp64[1]) / 2 / 1e12
                 issue["fp64"] = {"achieved": ach64_ti, "peak": peak64_ti, "frac": ach64_ti / peak64_ti,
                                  "instructions_per_particle_step": {"Millstein": ipp64[0], "Heun": ipp64[1]}}
-        cpu = None if args.no_cpu_baseline else cpu_baseline()
+        cpu = None if (args.no_cpu_baseline or world > 1) else cpu_baseline()  # rank 0 at N = 1 only
         c32 = results["FP32"]["clocks"]
         line = {
             "metric": METRIC, "value": v32, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
