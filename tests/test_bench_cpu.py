@@ -32,3 +32,17 @@ def test_reference_arm_prints_one_json_line():
         assert key in d, key
     assert d["impl"] == "reference" and d["value"] > 0
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["value"] == d["value"]
+
+
+def test_bench_workloads_integrate_whole_windows():
+    """Every workload the bench times integrates a positive number of whole windows, the
+    count its rates are computed from."""
+    from stochasticphysics_b200 import provider
+    from stochasticphysics_b200._abi import Precision, Problem
+    specs = bench.workload_specs(256, 2 * 4 * 10000 + 2000, Precision.FP32, 0)
+    specs += provider.batched_sets(count=64, step_scale=0.02)
+    specs += provider.batched_sets(count=64, step_scale=0.006, lissajous=True,
+                                   problems=(Problem.Neel, Problem.BrownAndNeelEulerSpherical))
+    for s in specs:
+        assert s.integrated_steps > 0 and s.integrated_steps % s.oversampling == 0
+        assert s.number_of_steps >= 2 * s.oversampling
