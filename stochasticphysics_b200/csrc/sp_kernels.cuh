@@ -4,11 +4,14 @@
 //                   Problems/Helpers/ParameterCalculator{Neel,Brown}.h), the
 //                   initial state (getStart of each problem), sample 0 and the
 //                   weights (getWeighting), reduced per warp
-//  step_kernel      one chunk of steps for a list of particle tiles: the state
-//                   lives in registers, B(t) is computed once per step per CTA
-//                   into shared memory, the Wiener increments come from
-//                   in-kernel Philox (or from HBM in injection mode), each
-//                   window's Kahan mean is reduced per warp in FP64
+//  step_kernel      one chunk of steps for a list of particle tiles, one or two
+//                   particles per thread: the state lives in registers, each warp
+//                   stages the chunk's B(t) table (computed once per step in FP64 by
+//                   field_chunk_kernel) in shared memory, the Wiener increments come
+//                   from in-kernel Philox (or from HBM in injection mode, a few steps
+//                   ahead through a register ring), each step's output sines and
+//                   cosines carry to the next step's prepare, and each window's Kahan
+//                   mean is reduced per warp in FP64 and stored in one coalesced store
 //                   (SingleParticleSimulator.h:129-159, MeanSimulationResult.h:87-119)
 //  reduce_kernel    per-warp window partials -> ensemble sums, fixed order
 //  commit_kernel    advances the device step counter (graph replay)
