@@ -31,6 +31,8 @@ Heun) on the device-resident state, i.e. 2 x 65536 x 10000 particle-steps.
                FP64 with the reference's Newton matrix, FP64 and FP32 with the exact one
   injected     injection mode (caller-supplied dW read from HBM every step), Neel Heun,
                65536 particles, FP64 and FP32: particle-steps/s and dW GB/s vs HBM peak
+  ensemble_sizes  the workload one ensemble at a time at 16k to 1M particles, FP32 and
+               FP64 (a 65536-particle ensemble alone does not fill the GPU)
   --impl reference  runs that CPU restatement as the reference arm
 
 Launch shapes come from the autotuner (sp_autotune) unless --no-autotune.
@@ -388,6 +390,37 @@ def injected_leg(ctx, torch, n=65536, timed_steps=1000, warm_steps=100):
     return out
 
 
+def sizes_leg(ctx, torch, sizes=(16384, 65536, 262144, 1048576)):
+    """The Brown+Neel workload one ensemble at a time at several sizes, FP32 and FP64,
+    Millstein and Heun, with the launch shapes tuned for the bench workload: a 65536-
+    particle ensemble (2048 warps) does not fill the GPU's resident warps by itself, so
+    larger ensembles show the kernels' own rate.  Device-resident, CUDA-event timed after
+    a warm-up window."""
+    from stochasticphysics_b200 import provider
+    from stochasticphysics_b200._abi import Precision, Solver
+
+    st = torch.cuda.Stream()
+    rows = []
+    for n in sizes:
+        for solver in (Solver.Millstein, Solver.Heun_Strong):
+            row = {"particles": n, "solver": solver.name}
+            for prec, steps in ((Precision.FP32, 4000), (Precision.FP64, 2000)):
+                spec = provider.brown_neel_relaxation(n=n, steps=steps + 2000, oversampling=1000, solver=solver,
+                                                      precision=prec)
+                with ctx.ensemble(spec) as e:
+                    e.advance(1000, st.cuda_stream)
+                    torch.cuda.synchronize()
+                    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    a.record(st)
+                    e.advance(steps, st.cuda_stream)
+                    b.record(st)
+                    torch.cuda.synchronize()
+                row[prec.name.lower()] = n * steps / (a.elapsed_time(b) / 1e3)
+            row["fp32_over_fp64"] = row["fp32"] / row["fp64"]
+            rows.append(row)
+    return {"unit": UNIT, "rows": rows}
+
+
 def cpu_baseline(steps_sample=2000, n=None):
     """The CPU oracle on all host cores for a bounded sample of the workload."""
     import oracle
@@ -504,6 +537,7 @@ def main():
     ap.add_argument("--batched-sets", type=int, default=256, help="parameter sets of the batched leg (0: skip)")
     ap.add_argument("--no-stiff", action="store_true", help="skip the stiff ImplicitMidpoint leg")
     ap.add_argument("--no-injected", action="store_true", help="skip the injected-noise (HBM) leg")
+    ap.add_argument("--no-sizes", action="store_true", help="skip the ensemble-size sweep")
     ap.add_argument("--batched-step-scale", type=float, default=0.02,
                     help="scale of the batched sets' step counts (S ~ logU[1e5, 1e7] x scale)")
     args = ap.parse_args()
@@ -616,6 +650,7 @@ def main():
             batched = batched_leg(ctx, args.batched_sets, args.batched_step_scale)
         stiff = None if (world > 1 or args.no_stiff) else stiff_leg(ctx, torch)
         injected = None if (world > 1 or args.no_injected) else injected_leg(ctx, torch)
+        sizes = None if (world > 1 or args.no_sizes) else sizes_leg(ctx, torch)
         plain_neel = None if (world > 1 or args.no_cpu_baseline) else plain_neel_leg(ctx, torch)
 
     if rank == 0:
@@ -679,6 +714,7 @@ def main():
             "batched": batched,
             "stiff": stiff,
             "injected": injected,
+            "ensemble_sizes": sizes,
             "plain_neel_1024": plain_neel,
         }
         print(json.dumps(line), flush=True)
