@@ -68,6 +68,8 @@ inline int usable_ppt(const KernelSet& ks, int ppt, int block) {
 LaunchConfig default_launch(const sp_context* ctx, const sp_ensemble_desc& d);
 // default_launch refined by the autotuner cache and SP_BLOCK / SP_CHUNK / SP_PERSISTENT
 LaunchConfig launch_config_for(const sp_context* ctx, const sp_ensemble_desc& d);
+// particle-steps/s the autotuner measured for d's kernel key (0 when untuned)
+double tuned_rate(const sp_ensemble_desc& d);
 
 struct EnsembleLayout {
     int D = 0, Mn = 0, OUT = 0, P = 0, real = 8, slots = 2;

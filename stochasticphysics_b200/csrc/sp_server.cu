@@ -225,10 +225,27 @@ struct sp_server {
                 }
             }
             try {
-                // one chunk for every group
+                // one chunk for every group, the longest first: the groups' CTAs then fill
+                // the SMs the longest leaves free instead of it running alone at the end.
+                // Length = particle-steps of the chunk over the key's tuned rate (the
+                // particle-steps alone while any key is untuned).
+                std::vector<std::pair<double, Group*>> order;
+                bool all_tuned = true;
+                for (auto& kv : groups)
+                    if (!kv.second.members.empty() && tuned_rate(kv.second.members.front()->desc) <= 0.0) all_tuned = false;
                 for (auto& kv : groups) {
                     Group& g = kv.second;
                     if (g.members.empty()) continue;
+                    double work = 0.0;
+                    for (Request* r : g.members) {
+                        const Ensemble* e = r->ens.get();
+                        work += static_cast<double>(e->L.n) * static_cast<double>(std::min(e->L.chunk, e->L.S - e->steps_done));
+                    }
+                    order.emplace_back(all_tuned ? work / tuned_rate(g.members.front()->desc) : work, &g);
+                }
+                std::stable_sort(order.begin(), order.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+                for (auto& og : order) {
+                    Group& g = *og.second;
                     if (g.dirty) rebuild(g);
                     check_cuda(cudaGraphLaunch(g.gexec, g.stream), "graph launch");
                     g_launch_count += 5;

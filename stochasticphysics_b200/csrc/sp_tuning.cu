@@ -52,6 +52,12 @@ bool lookup_tuned(const sp_ensemble_desc& d, LaunchConfig& c) {
     return true;
 }
 
+double tuned_rate(const sp_ensemble_desc& d) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tuned_rate.find(key_of(d));
+    return it == g_tuned_rate.end() ? 0.0 : it->second;
+}
+
 LaunchConfig launch_config_for(const sp_context* ctx, const sp_ensemble_desc& d) {
     LaunchConfig c = default_launch(ctx, d);
     LaunchConfig t;
