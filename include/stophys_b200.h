@@ -398,6 +398,17 @@ SP_API sp_status sp_autotune(sp_context* ctx, const sp_ensemble_desc* desc, uint
                              int32_t* n_candidates);
 /* Launch shape the library uses for desc now (tuned or default). */
 SP_API sp_status sp_launch_config_for(sp_context* ctx, const sp_ensemble_desc* desc, sp_launch_config* out);
+/* sp_ensemble_create with the caller's launch shape (shape NULL = the tuned or default
+ * one): block 32, 64, 128 or 256; persistent 0 or 1; chunk_steps >= 1, rounded down to
+ * whole windows (at least one); particles_per_thread 1 or 2 (2 falls back to 1 where the
+ * kernel key has no two-particle form or the block is under 64); particle_steps_per_s
+ * and reserved0 are ignored.  Results do not depend on the shape.  Ensembles advanced
+ * side by side on separate streams run faster with short chunks (about 1000 steps): a
+ * chunk launch ends with its CTAs draining, and the SMs they free go to the other
+ * ensembles' CTAs only when those have launches in flight, where a lone ensemble is
+ * fastest with the longer chunk the autotuner picks. */
+SP_API sp_status sp_ensemble_create_shaped(sp_context* ctx, const sp_ensemble_desc* desc, const sp_launch_config* shape,
+                                           sp_ensemble** ens);
 /* Write / read (merge) the tuned shapes of this process as text, one key per
  * line; reset forgets them all (defaults apply again). */
 SP_API sp_status sp_tuning_save(const char* path);

@@ -612,6 +612,32 @@ sp_status sp_ensemble_create(sp_context* ctx, const sp_ensemble_desc* desc, sp_e
     SP_GUARD_END
 }
 
+sp_status sp_ensemble_create_shaped(sp_context* ctx, const sp_ensemble_desc* desc, const sp_launch_config* shape,
+                                    sp_ensemble** ens) {
+    SP_GUARD_BEGIN
+    if (!shape) return sp_ensemble_create(ctx, desc, ens);
+    if (!ctx || !ens) return fail(SP_ERR_INVALID_ARG, "NULL argument");
+    std::string why;
+    const sp_status s = validate_desc(desc, why);
+    if (s != SP_OK) return fail(s, why);
+    const int b = shape->block;
+    if (b != 32 && b != 64 && b != 128 && b != 256) return fail(SP_ERR_INVALID_ARG, "shape.block must be 32, 64, 128 or 256");
+    if (shape->persistent != 0 && shape->persistent != 1) return fail(SP_ERR_INVALID_ARG, "shape.persistent must be 0 or 1");
+    if (shape->chunk_steps < 1) return fail(SP_ERR_INVALID_ARG, "shape.chunk_steps must be at least 1");
+    if (shape->particles_per_thread != 1 && shape->particles_per_thread != 2)
+        return fail(SP_ERR_INVALID_ARG, "shape.particles_per_thread must be 1 or 2");
+    LaunchConfig lc;
+    lc.block = b;
+    lc.persistent = shape->persistent;
+    const unsigned long long W = desc->oversampling;
+    lc.chunk = shape->chunk_steps <= W ? W : shape->chunk_steps / W * W;
+    lc.ppt = shape->particles_per_thread;
+    auto* e = new Ensemble(ctx, *desc, lc);
+    *ens = reinterpret_cast<sp_ensemble*>(e);
+    return SP_OK;
+    SP_GUARD_END
+}
+
 sp_status sp_ensemble_advance(sp_ensemble* ens, uint64_t n_steps, void* cuda_stream) {
     SP_GUARD_BEGIN
     if (!ens) return fail(SP_ERR_INVALID_ARG, "NULL ensemble");

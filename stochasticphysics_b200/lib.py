@@ -21,7 +21,7 @@ SYMBOLS = [
     "sp_server_create", "sp_server_submit", "sp_server_poll", "sp_server_wait", "sp_server_cancel",
     "sp_server_destroy", "sp_debug_philox_normals", "sp_measure_fma_peak", "sp_simulate_noalloc",
     "sp_autotune", "sp_launch_config_for", "sp_tuning_save", "sp_tuning_load", "sp_tuning_reset",
-    "sp_provide_particles",
+    "sp_provide_particles", "sp_ensemble_create_shaped",
 ]
 
 _lib = None
@@ -56,6 +56,7 @@ def load():
     L.sp_destroy.argtypes = [vp]
     L.sp_simulate.argtypes = [vp, C.POINTER(sp_ensemble_desc), C.POINTER(sp_result), C.POINTER(sp_stats)]
     L.sp_ensemble_create.argtypes = [vp, C.POINTER(sp_ensemble_desc), C.POINTER(vp)]
+    L.sp_ensemble_create_shaped.argtypes = [vp, C.POINTER(sp_ensemble_desc), C.POINTER(sp_launch_config), C.POINTER(vp)]
     L.sp_ensemble_advance.argtypes = [vp, u64, vp]
     L.sp_ensemble_steps_done.argtypes = [vp, C.POINTER(u64), C.POINTER(u64)]
     L.sp_ensemble_read.argtypes = [vp, C.POINTER(sp_result), C.POINTER(sp_stats)]

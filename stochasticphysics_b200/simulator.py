@@ -77,8 +77,11 @@ class Context:
         check(self._lib.sp_simulate(self.handle, h.byref(), C.byref(buf.c), C.byref(st)))
         return _result(buf, st)
 
-    def ensemble(self, spec: EnsembleSpec) -> "DeviceEnsemble":
-        return DeviceEnsemble(self, spec)
+    def ensemble(self, spec: EnsembleSpec, shape: Optional[dict] = None) -> "DeviceEnsemble":
+        """A device-resident ensemble; `shape` (keys block, persistent, chunk_steps,
+        particles_per_thread, as :meth:`launch_config` returns them) replaces the tuned
+        launch shape (sp_ensemble_create_shaped)."""
+        return DeviceEnsemble(self, spec, shape)
 
     def server(self, memory_budget_bytes: int = 0, chunk_steps: int = 0, max_active: int = 0) -> "Server":
         return Server(self, memory_budget_bytes, chunk_steps, max_active)
@@ -145,12 +148,18 @@ class Context:
 class DeviceEnsemble:
     """A device-resident ensemble: inputs uploaded once, advanced chunk by chunk."""
 
-    def __init__(self, ctx: Context, spec: EnsembleSpec):
+    def __init__(self, ctx: Context, spec: EnsembleSpec, shape: Optional[dict] = None):
         self.ctx, self.spec = ctx, spec
         self._lib = ctx._lib
         self._holder = DescHolder(spec)
         h = C.c_void_p()
-        check(self._lib.sp_ensemble_create(ctx.handle, self._holder.byref(), C.byref(h)))
+        if shape is None:
+            check(self._lib.sp_ensemble_create(ctx.handle, self._holder.byref(), C.byref(h)))
+        else:
+            lc = sp_launch_config(block=int(shape["block"]), persistent=int(shape["persistent"]),
+                                  chunk_steps=int(shape["chunk_steps"]),
+                                  particles_per_thread=int(shape.get("particles_per_thread", 1)))
+            check(self._lib.sp_ensemble_create_shaped(ctx.handle, self._holder.byref(), C.byref(lc), C.byref(h)))
         self.handle = h
 
     def advance(self, n_steps: int, stream: Optional[int] = None) -> None:

@@ -13,6 +13,7 @@ import pytest
 import stochasticphysics_b200 as sp
 from stochasticphysics_b200 import provider
 from stochasticphysics_b200._abi import Precision, Solver
+from stochasticphysics_b200.lib import SPError
 
 pytestmark = pytest.mark.gpu
 
@@ -33,7 +34,13 @@ def test_autotune_picks_the_fastest_candidate(ctx):
     best, cands = out["best"], out["candidates"]
     assert len(cands) >= 4
     assert all(c["particle_steps_per_s"] > 0 for c in cands)
-    assert best["particle_steps_per_s"] == max(c["particle_steps_per_s"] for c in cands)
+    top = max(c["particle_steps_per_s"] for c in cands)
+    assert best["particle_steps_per_s"] >= 0.98 * top
+    # the winning shape keeps the shortest chunk within 2 % of the best rate
+    shape = ("block", "persistent", "particles_per_thread")
+    same = [c for c in cands if all(c[k] == best[k] for k in shape)]
+    assert {c["chunk_steps"] for c in same} >= {1000, 2000, 10000, 40000}
+    assert best["chunk_steps"] == min(c["chunk_steps"] for c in same if c["particle_steps_per_s"] >= 0.98 * top)
     used = ctx.launch_config(spec)
     assert (used["block"], used["persistent"], used["chunk_steps"]) == (best["block"], best["persistent"],
                                                                          best["chunk_steps"])
@@ -95,3 +102,21 @@ def test_tuned_shapes_reach_the_server(ctx, tmp_path):
         res = [srv.wait(i)[0] for i in ids]
     np.testing.assert_array_equal(res[0].mean, ref.mean)
     assert not np.array_equal(res[1].mean, ref.mean)
+
+
+def test_shaped_ensemble_equals_the_tuned_one(ctx):
+    """sp_ensemble_create_shaped: the caller's CTA size, grid form and chunk (rounded down
+    to whole windows) change no bit of the result; invalid shapes are refused."""
+    spec = provider.brown_neel_relaxation(n=5000, steps=8000, oversampling=1000, solver=Solver.Heun_Strong,
+                                          precision=Precision.FP32)
+    shape = {"block": 64, "persistent": 1, "chunk_steps": 1500, "particles_per_thread": 1}
+    with ctx.ensemble(spec) as a, ctx.ensemble(spec, shape=shape) as b:
+        for e in (a, b):
+            e.advance(3000)
+            e.advance(3000)
+        ra, rb = a.read(), b.read()
+    np.testing.assert_array_equal(rb.mean, ra.mean)
+    np.testing.assert_array_equal(rb.weight, ra.weight)
+    for bad in ({"block": 96}, {"persistent": 2}, {"chunk_steps": 0}, {"particles_per_thread": 3}):
+        with pytest.raises(SPError, match="shape"):
+            ctx.ensemble(spec, shape=dict(shape, **bad))
