@@ -331,10 +331,12 @@ SP_API sp_status sp_ensemble_footprint(const sp_ensemble_desc* desc, uint64_t* b
 /* ---- continuous-batching server ----------------------------------------- */
 typedef struct sp_server_config {
     uint64_t memory_budget_bytes; /* admission limit on device bytes of admitted requests */
-    uint64_t chunk_steps;         /* steps per scheduling chunk; 0 = the tuned chunk
+    uint64_t chunk_steps;         /* steps per scheduling round; 0 = the tuned chunk
                                      capped at 4000 steps (whole windows): requests join
-                                     and leave only between chunks, so the chunk bounds
-                                     how long a new request waits behind running ones   */
+                                     and leave only between rounds, so the round bounds
+                                     how long a new request waits behind running ones.
+                                     A round runs as chunk launches of at most 1000
+                                     steps (whole windows where a window fits)           */
     int32_t max_active;           /* cap on concurrently admitted requests (0 = none)     */
     int32_t reserved;
 } sp_server_config;

@@ -9,8 +9,10 @@
 // group runs ONE batched launch per chunk over a shared work list of particle
 // tiles (step_kernel reads the tile -> ensemble map), captured once per group
 // membership as a CUDA graph.  Groups run on separate streams so different
-// kernels overlap on the device.  Finished ensembles are read back and freed
-// at the next chunk boundary, which makes room for queued requests.
+// kernels overlap on the device; a round replays each group's chunk graph a few
+// times, so one group's next chunk fills the SMs another's draining chunk frees.
+// Finished ensembles are read back and freed at the next round boundary, which
+// makes room for queued requests.
 //
 // Every particle's arithmetic, noise stream and per-warp reduction order are
 // independent of which other ensembles share the launch, so a request's
@@ -46,6 +48,8 @@ struct Request {
     sp_status error = SP_OK;
     std::string message;
     uint64_t bytes = 0;
+    unsigned long long chunks_per_round = 1;
+    bool in_round = false;  // launched in the current round (not admitted during it)
     Clock::time_point t_submit, t_done;
     std::vector<double> mean, weight, time, field;
     sp_stats stats{};
@@ -58,6 +62,7 @@ struct Group {
     TileDesc* d_tiles = nullptr;
     int ntiles = 0, max_slots = 2, block = 128;
     unsigned long long max_chunk = 1;
+    unsigned long long chunks_per_round = 1;  // the largest of its members'
     cudaStream_t stream = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
@@ -95,19 +100,25 @@ struct sp_server {
                (d.noise == SP_NOISE_INJECTED);
     }
 
-    // Requests join and leave a group only at chunk boundaries, so the chunk bounds how long
-    // a new request waits behind a running group.  Without a configured chunk the tuned
-    // (throughput) chunk is capped at kServeChunk steps, in whole windows.
+    // Requests join and leave a group only between rounds, so the round bounds how long a
+    // new request waits behind a running group: cfg.chunk_steps steps, or else the tuned
+    // (throughput) chunk capped at kServeChunk steps, in whole windows.  A round runs as
+    // chunk launches of at most kSliceSteps (whole windows where a window fits): each
+    // launch ends with its CTAs draining, and with several groups in flight the others'
+    // next launches fill the SMs so freed (two 65536-particle Brown+Neel ensembles run
+    // 15 % faster in 1000-step launches than in 10000-step ones).
     static constexpr unsigned long long kServeChunk = 4000;
-    LaunchConfig launch_for(const sp_ensemble_desc& d) const {
+    static constexpr unsigned long long kSliceSteps = 1000;
+    static unsigned long long whole_windows(unsigned long long steps, unsigned long long W) {
+        return steps <= W ? W : steps / W * W;
+    }
+    LaunchConfig launch_for(const sp_ensemble_desc& d, unsigned long long* chunks_per_round = nullptr) const {
         LaunchConfig c = launch_config_for(ctx, d);
-        if (cfg.chunk_steps) {
-            c.chunk = std::max<unsigned long long>(cfg.chunk_steps, 1);
-        } else {
-            const unsigned long long W = d.oversampling;
-            const unsigned long long cap = W >= kServeChunk ? W : (kServeChunk / W) * W;
-            c.chunk = std::min(c.chunk, cap);
-        }
+        const unsigned long long W = d.oversampling;
+        const unsigned long long round = cfg.chunk_steps ? std::max<unsigned long long>(cfg.chunk_steps, 1)
+                                                         : std::min(c.chunk, whole_windows(kServeChunk, W));
+        c.chunk = round <= kSliceSteps ? round : std::min(round, whole_windows(kSliceSteps, W));
+        if (chunks_per_round) *chunks_per_round = std::max<unsigned long long>(1, round / c.chunk);
         return c;
     }
 
@@ -147,7 +158,7 @@ struct sp_server {
             if (used_bytes + r->bytes > budget) break;
             queue.pop_front();
             try {
-                r->ens = std::make_unique<Ensemble>(ctx, r->desc, launch_for(r->desc));
+                r->ens = std::make_unique<Ensemble>(ctx, r->desc, launch_for(r->desc, &r->chunks_per_round));
                 r->ens->last_stream = nullptr;
                 // the ensemble holds its inputs on the device now: drop the host copies
                 std::vector<double>().swap(r->arrays);
@@ -175,6 +186,7 @@ struct sp_server {
         std::vector<TileDesc> tiles;
         g.max_slots = 2;
         g.max_chunk = 1;
+        g.chunks_per_round = 1;
         g.block = 32;
         for (Request* r : g.members) g.block = std::max(g.block, r->ens->block);
         for (size_t i = 0; i < g.members.size(); ++i) {
@@ -182,6 +194,7 @@ struct sp_server {
             ens.push_back(e->hdev);
             g.max_slots = std::max(g.max_slots, e->L.slots);
             g.max_chunk = std::max(g.max_chunk, e->L.chunk);
+            g.chunks_per_round = std::max(g.chunks_per_round, g.members[i]->chunks_per_round);
             for (unsigned long long f = 0; f < e->L.n; f += g.block) tiles.push_back(TileDesc{static_cast<unsigned>(i), static_cast<unsigned>(f)});
         }
         g.ntiles = static_cast<int>(tiles.size());
@@ -225,33 +238,46 @@ struct sp_server {
                 }
             }
             try {
-                // one chunk for every group, the longest first: the groups' CTAs then fill
-                // the SMs the longest leaves free instead of it running alone at the end.
-                // Length = particle-steps of the chunk over the key's tuned rate (the
+                // one round for every group: its chunk graph chunks_per_round times, the
+                // groups' launches interleaved and the longest group first, so the others'
+                // CTAs fill the SMs it leaves free instead of it running alone at the end.
+                // Length = particle-steps of the round over the key's tuned rate (the
                 // particle-steps alone while any key is untuned).
                 std::vector<std::pair<double, Group*>> order;
                 bool all_tuned = true;
                 for (auto& kv : groups)
                     if (!kv.second.members.empty() && tuned_rate(kv.second.members.front()->desc) <= 0.0) all_tuned = false;
+                unsigned long long launches = 0;
                 for (auto& kv : groups) {
                     Group& g = kv.second;
                     if (g.members.empty()) continue;
+                    if (g.dirty) rebuild(g);
+                    launches = std::max(launches, g.chunks_per_round);
                     double work = 0.0;
                     for (Request* r : g.members) {
                         const Ensemble* e = r->ens.get();
-                        work += static_cast<double>(e->L.n) * static_cast<double>(std::min(e->L.chunk, e->L.S - e->steps_done));
+                        work += static_cast<double>(e->L.n) *
+                                static_cast<double>(std::min(g.chunks_per_round * e->L.chunk, e->L.S - e->steps_done));
                     }
                     order.emplace_back(all_tuned ? work / tuned_rate(g.members.front()->desc) : work, &g);
                 }
                 std::stable_sort(order.begin(), order.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
-                for (auto& og : order) {
-                    Group& g = *og.second;
-                    if (g.dirty) rebuild(g);
-                    check_cuda(cudaGraphLaunch(g.gexec, g.stream), "graph launch");
-                    g_launch_count += 5;
+                for (auto& og : order)
+                    for (Request* r : og.second->members) r->in_round = true;
+                for (unsigned long long j = 0; j < launches; ++j)
+                    for (auto& og : order) {
+                        Group& g = *og.second;
+                        if (j >= g.chunks_per_round) continue;
+                        check_cuda(cudaGraphLaunch(g.gexec, g.stream), "graph launch");
+                        g_launch_count += 5;
+                    }
+                {
+                    // requests that arrived meanwhile are uploaded while the round runs and
+                    // join at the next one
+                    std::lock_guard<std::mutex> lk(mu);
+                    admit_locked();
                 }
-                for (auto& kv : groups)
-                    if (!kv.second.members.empty()) check_cuda(cudaStreamSynchronize(kv.second.stream), "chunk");
+                for (auto& og : order) check_cuda(cudaStreamSynchronize(og.second->stream), "chunk");
             } catch (const Error& e) {
                 std::lock_guard<std::mutex> lk(mu);
                 for (Request* r : active) { r->ens.reset(); finish(r, SP_REQUEST_FAILED, e.status, e.what()); }
@@ -265,11 +291,18 @@ struct sp_server {
             std::lock_guard<std::mutex> lk(mu);
             std::vector<Request*> still;
             for (Request* r : active) {
+                if (!r->in_round) {
+                    still.push_back(r);
+                    continue;
+                }
+                r->in_round = false;
                 Ensemble* e = r->ens.get();
-                const unsigned long long step = std::min(e->L.chunk, e->L.S - e->steps_done);
+                // each launch advances the ensemble by min(chunk, steps left) (bump, commit)
+                const unsigned long long nl = groups[key_of(r->desc)].chunks_per_round;
+                const unsigned long long step = std::min(nl * e->L.chunk, e->L.S - e->steps_done);
                 e->steps_done += step;
                 e->particle_steps += step * e->L.n;
-                e->launches += 5;
+                e->launches += 5 * nl;
                 const bool done = e->steps_done >= e->L.S;
                 if (done || r->cancel) {
                     try {
