@@ -616,16 +616,18 @@ sp_status sp_ensemble_create_shaped(sp_context* ctx, const sp_ensemble_desc* des
                                     sp_ensemble** ens) {
     SP_GUARD_BEGIN
     if (!shape) return sp_ensemble_create(ctx, desc, ens);
-    if (!ctx || !ens) return fail(SP_ERR_INVALID_ARG, "NULL argument");
+    if (!ens) return fail(SP_ERR_INVALID_ARG, "ens is NULL");
     std::string why;
     const sp_status s = validate_desc(desc, why);
     if (s != SP_OK) return fail(s, why);
+    // the shape is checked before the context, so hosts can check it without a device
     const int b = shape->block;
     if (b != 32 && b != 64 && b != 128 && b != 256) return fail(SP_ERR_INVALID_ARG, "shape.block must be 32, 64, 128 or 256");
     if (shape->persistent != 0 && shape->persistent != 1) return fail(SP_ERR_INVALID_ARG, "shape.persistent must be 0 or 1");
     if (shape->chunk_steps < 1) return fail(SP_ERR_INVALID_ARG, "shape.chunk_steps must be at least 1");
     if (shape->particles_per_thread != 1 && shape->particles_per_thread != 2)
         return fail(SP_ERR_INVALID_ARG, "shape.particles_per_thread must be 1 or 2");
+    if (!ctx) return fail(SP_ERR_INVALID_ARG, "ctx is NULL");
     LaunchConfig lc;
     lc.block = b;
     lc.persistent = shape->persistent;

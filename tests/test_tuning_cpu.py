@@ -98,3 +98,21 @@ def test_malformed_tuning_files_are_refused(tmp_path, text):
     f.write_text(text)
     assert load().sp_tuning_load(str(f).encode()) == 1
     assert load().sp_tuning_load(str(tmp_path / "missing.txt").encode()) == 1
+
+
+def test_shaped_create_checks_the_shape_before_the_device():
+    """sp_ensemble_create_shaped refuses malformed shapes before it needs a context, so
+    the checks run here without a GPU; a well-formed shape then needs the context."""
+    spec = provider.brown_neel_relaxation(n=4096, steps=20000, oversampling=1000, precision=Precision.FP32)
+    good = dict(block=64, persistent=1, chunk_steps=1500, particles_per_thread=2)
+    h = C.c_void_p()
+    lib = load()
+    cases = [({}, "ctx is NULL"), ({"block": 96}, "shape.block"), ({"persistent": 2}, "shape.persistent"),
+             ({"chunk_steps": 0}, "shape.chunk_steps"), ({"particles_per_thread": 0}, "shape.particles_per_thread")]
+    for change, message in cases:
+        lc = sp_launch_config(**dict(good, **change))
+        assert lib.sp_ensemble_create_shaped(None, DescHolder(spec).byref(), C.byref(lc), C.byref(h)) == 1
+        assert message in lib.sp_last_error().decode()
+    lc = sp_launch_config(**good)
+    assert lib.sp_ensemble_create_shaped(None, DescHolder(spec).byref(), C.byref(lc), None) == 1
+    assert "ens is NULL" in lib.sp_last_error().decode()
