@@ -34,6 +34,17 @@ def test_reference_arm_prints_one_json_line():
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["value"] == d["value"]
 
 
+def test_reference_arm_other_ranks_exit_without_work():
+    """Under torchrun the reference arm runs on rank 0 alone; the other ranks exit 0 silently."""
+    import os
+    env = dict(os.environ, RANK="1", LOCAL_RANK="1", WORLD_SIZE="2")
+    p = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--impl", "reference", "--gpus", "2", "--steps", "1",
+                        "--warmup", "3", "--n-particles", "512"], capture_output=True, text=True, timeout=600, cwd=ROOT,
+                       env=env)
+    assert p.returncode == 0, p.stderr
+    assert p.stdout.strip() == ""
+
+
 def test_bench_workloads_integrate_whole_windows():
     """Every workload the bench times integrates a positive number of whole windows, the
     count its rates are computed from."""
