@@ -629,8 +629,8 @@ def main():
         se_indep = math.sqrt(2.0 / (3.0 * N_PER_GPU))
 
         # e2e through the public C ABI with host buffers: per bench step, the two ensembles
-        # submitted together to the server (host arrays in) and waited for (results out);
-        # sp_simulate of the two one after the other is reported beside it
+        # submitted together to the server (sp_server_submit_many: host arrays in) and
+        # waited for (results out); sp_simulate of the two one after the other beside it
         e2e_specs = workload_specs(N_PER_GPU, CHUNK + 1000, Precision.FP32, rank)
         # submitted longest first (the lower tuned rate), as the co-scheduled leg launches
         e2e_specs.sort(key=lambda s: ctx.launch_config(s)["particle_steps_per_s"])
@@ -638,14 +638,14 @@ def main():
             ctx.simulate(s)  # warm the path
         e2e_times, seq_times = [], []
         with sp.Server(ctx) as srv:
-            ids = [srv.submit(s) for s in e2e_specs]
+            ids = srv.submit_many(e2e_specs)
             for i in ids:
                 srv.wait(i)
             for _ in range(args.steps):
                 if world > 1:
                     dist.barrier()
                 t = time.perf_counter()
-                ids = [srv.submit(s) for s in e2e_specs]
+                ids = srv.submit_many(e2e_specs)
                 outs = [srv.wait(i)[0] for i in ids]
                 e2e_times.append(time.perf_counter() - t)
         for _ in range(args.steps):
@@ -720,7 +720,7 @@ def main():
                          "fp64": {"achieved": sum(ach64) / 2, "peak": peak64, "frac": (sum(ach64) / 2) / peak64},
                          "issue": issue},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "api": "sp_server_submit / sp_server_wait, the two ensembles in flight together",
+                    "api": "sp_server_submit_many / sp_server_wait, the two ensembles in flight together",
                     "sp_simulate_one_after_the_other": e2e_simulate_value},
             "gpu_launches": results["FP32"]["launches"],
             "clocks": c32,

@@ -352,6 +352,12 @@ typedef enum sp_request_state {
 SP_API sp_status sp_server_create(sp_context* ctx, const sp_server_config* cfg, sp_server** srv);
 /* The description (and every array it points to) is copied at submit. */
 SP_API sp_status sp_server_submit(sp_server* srv, const sp_ensemble_desc* desc, uint64_t* request_id);
+/* Submits descs[0..n) at once: each is checked and copied as by sp_server_submit, then all
+ * are queued under one lock, so an idle server admits them together and their first
+ * rounds overlap (submitted one by one, the first can start alone before the next is
+ * queued).  All or nothing: if any is refused, none is queued and the error text names
+ * its index.  request_ids[i] receives the id of descs[i]. */
+SP_API sp_status sp_server_submit_many(sp_server* srv, const sp_ensemble_desc* descs, int32_t n, uint64_t* request_ids);
 SP_API sp_status sp_server_poll(sp_server* srv, uint64_t request_id, int32_t* state);
 /* Blocks up to timeout_ms (<0: forever) and copies results of a finished request.
  * A finished, failed or cancelled request is reported once: afterwards its id is

@@ -401,24 +401,61 @@ sp_status sp_server_create(sp_context* ctx, const sp_server_config* cfg, sp_serv
     SP_GUARD_END
 }
 
-sp_status sp_server_submit(sp_server* s, const sp_ensemble_desc* desc, uint64_t* id) {
-    SP_GUARD_BEGIN
-    if (!s || !id) return fail(SP_ERR_INVALID_ARG, "NULL argument");
-    std::string why;
+namespace {
+// Validated deep copy of one description with its device footprint, or the refusal.
+sp_status make_request(sp_server* s, const sp_ensemble_desc* desc, std::unique_ptr<Request>& out, std::string& why) {
     const sp_status st = validate_desc(desc, why);
-    if (st != SP_OK) return fail(st, why);
+    if (st != SP_OK) return st;
     auto r = std::make_unique<Request>();
     copy_desc_arrays(*desc, *r);
     r->bytes = layout_of(r->desc, s->launch_for(r->desc)).bytes;
-    if (r->bytes > s->budget)
-        return fail(SP_ERR_ADMISSION_REFUSED, "request needs " + std::to_string(r->bytes) + " bytes; budget is " +
-                                                   std::to_string(s->budget));
+    if (r->bytes > s->budget) {
+        why = "request needs " + std::to_string(r->bytes) + " bytes; budget is " + std::to_string(s->budget);
+        return SP_ERR_ADMISSION_REFUSED;
+    }
+    out = std::move(r);
+    return SP_OK;
+}
+}  // namespace
+
+sp_status sp_server_submit(sp_server* s, const sp_ensemble_desc* desc, uint64_t* id) {
+    SP_GUARD_BEGIN
+    if (!s || !id) return fail(SP_ERR_INVALID_ARG, "NULL argument");
+    std::unique_ptr<Request> r;
+    std::string why;
+    const sp_status st = make_request(s, desc, r, why);
+    if (st != SP_OK) return fail(st, why);
     r->t_submit = Clock::now();
     std::lock_guard<std::mutex> lk(s->mu);
     r->id = s->next_id++;
     *id = r->id;
     s->queue.push_back(r.get());
     s->all[r->id] = std::move(r);
+    s->cv_work.notify_one();
+    return SP_OK;
+    SP_GUARD_END
+}
+
+sp_status sp_server_submit_many(sp_server* s, const sp_ensemble_desc* descs, int32_t n, uint64_t* ids) {
+    SP_GUARD_BEGIN
+    if (!s || !descs || !ids) return fail(SP_ERR_INVALID_ARG, "NULL argument");
+    if (n < 1) return fail(SP_ERR_INVALID_ARG, "n must be >= 1");
+    std::vector<std::unique_ptr<Request>> rs(static_cast<size_t>(n));
+    for (int32_t i = 0; i < n; ++i) {
+        std::string why;
+        const sp_status st = make_request(s, &descs[i], rs[static_cast<size_t>(i)], why);
+        if (st != SP_OK) return fail(st, "request " + std::to_string(i) + ": " + why);
+    }
+    const auto now = Clock::now();
+    std::lock_guard<std::mutex> lk(s->mu);
+    for (int32_t i = 0; i < n; ++i) {
+        std::unique_ptr<Request>& r = rs[static_cast<size_t>(i)];
+        r->t_submit = now;
+        r->id = s->next_id++;
+        ids[i] = r->id;
+        s->queue.push_back(r.get());
+        s->all[r->id] = std::move(r);
+    }
     s->cv_work.notify_one();
     return SP_OK;
     SP_GUARD_END

@@ -21,7 +21,7 @@ SYMBOLS = [
     "sp_server_create", "sp_server_submit", "sp_server_poll", "sp_server_wait", "sp_server_cancel",
     "sp_server_destroy", "sp_debug_philox_normals", "sp_measure_fma_peak", "sp_simulate_noalloc",
     "sp_autotune", "sp_launch_config_for", "sp_tuning_save", "sp_tuning_load", "sp_tuning_reset",
-    "sp_provide_particles", "sp_ensemble_create_shaped",
+    "sp_provide_particles", "sp_ensemble_create_shaped", "sp_server_submit_many",
 ]
 
 _lib = None
@@ -64,6 +64,7 @@ def load():
     L.sp_ensemble_footprint.argtypes = [C.POINTER(sp_ensemble_desc), C.POINTER(u64)]
     L.sp_server_create.argtypes = [vp, C.POINTER(sp_server_config), C.POINTER(vp)]
     L.sp_server_submit.argtypes = [vp, C.POINTER(sp_ensemble_desc), C.POINTER(u64)]
+    L.sp_server_submit_many.argtypes = [vp, C.POINTER(sp_ensemble_desc), i32, C.POINTER(u64)]
     L.sp_server_poll.argtypes = [vp, u64, C.POINTER(i32)]
     L.sp_server_wait.argtypes = [vp, u64, C.c_double, C.POINTER(sp_result), C.POINTER(sp_stats), dp]
     L.sp_server_cancel.argtypes = [vp, u64]

@@ -15,8 +15,8 @@ from typing import Optional
 
 import numpy as np
 
-from ._abi import (DescHolder, EnsembleSpec, ResultBuffers, sp_launch_config, sp_result, sp_server_config, sp_stats,
-                   RequestState)
+from ._abi import (DescHolder, EnsembleSpec, RequestState, ResultBuffers, sp_ensemble_desc, sp_launch_config, sp_result,
+                   sp_server_config, sp_stats)
 from .lib import check, load
 
 
@@ -215,6 +215,18 @@ class Server:
         check(self._lib.sp_server_submit(self.handle, holder.byref(), C.byref(rid)))
         self._specs[int(rid.value)] = spec
         return int(rid.value)
+
+    def submit_many(self, specs) -> list:
+        """Queues all specs at once (sp_server_submit_many): an idle server admits them
+        together.  All or nothing."""
+        holders = [DescHolder(sp_) for sp_ in specs]
+        arr = (sp_ensemble_desc * len(holders))(*[h.desc for h in holders])
+        rids = (C.c_uint64 * len(holders))()
+        check(self._lib.sp_server_submit_many(self.handle, arr, len(holders), rids))
+        out = [int(r) for r in rids]
+        for rid, spec in zip(out, specs):
+            self._specs[rid] = spec
+        return out
 
     def poll(self, rid: int) -> RequestState:
         s = C.c_int32()

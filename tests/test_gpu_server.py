@@ -77,3 +77,19 @@ def test_many_requests_release_their_memory(ctx):
             for i in ids:
                 with pytest.raises(sp.SPError):
                     srv.poll(i)
+
+
+def test_submit_many_queues_all_or_nothing(ctx):
+    """sp_server_submit_many: every result equals its own sp_simulate; a refused
+    description (here over the budget) queues none and names its index."""
+    specs = [small(n=3000, steps=6000, seed=21), small(n=5000, steps=3000, seed=22),
+             provider.brown_neel_relaxation(n=2000, steps=5000, oversampling=1000, solver=Solver.Millstein, seed=23)]
+    with sp.Server(ctx) as srv:
+        ids = srv.submit_many(specs)
+        assert len(set(ids)) == 3
+        for rid, spec in zip(ids, specs):
+            np.testing.assert_array_equal(srv.wait(rid)[0].mean, ctx.simulate(spec).mean)
+    with sp.Server(ctx, memory_budget_bytes=1 << 20) as srv:
+        with pytest.raises(sp.SPError, match="request 1") as e:
+            srv.submit_many([small(n=100), small(n=200000)])
+        assert e.value.status == Status.ADMISSION_REFUSED
