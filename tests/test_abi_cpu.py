@@ -144,3 +144,13 @@ def test_create_without_device_fails_loudly():
     with pytest.raises(sp.SPError) as ei:
         sp.Context(0)
     assert ei.value.status in (int(sp.Status.NO_DEVICE), int(sp.Status.CUDA))
+
+
+def test_server_entry_points_refuse_null_arguments():
+    """The server calls check their arguments before touching a device."""
+    lib = load()
+    ids = (C.c_uint64 * 2)()
+    assert lib.sp_server_submit_many(None, None, 2, ids) == int(sp.Status.INVALID_ARG)
+    assert "NULL" in lib.sp_last_error().decode()
+    assert lib.sp_server_submit(None, None, None) == int(sp.Status.INVALID_ARG)
+    assert lib.sp_server_poll(None, 1, None) == int(sp.Status.INVALID_ARG)
