@@ -15,8 +15,9 @@ Heun) on the device-resident state, i.e. 2 x 65536 x 10000 particle-steps.
                1000-step chunk launches, CUDA-event timed, max over ranks
   fp64_plain   the same steps with the plain FP64 kernel
   e2e          the same metric through the public C ABI with host buffers: per step
-               both ensembles submitted together to the server (upload, 10000 steps,
-               results back); sp_simulate one after the other is reported beside it
+               both ensembles submitted together to the server (sp_server_submit_many;
+               upload, 10000 steps, results back); sp_simulate one after the other is
+               reported beside it
   cpu_baseline the CPU oracle (restatement of the reference formulas) on all host
                cores, rank 0 only, on a bounded sample of the same workload
   serving      continuous-batching leg (N=1): Poisson arrivals of mixed Neel /
