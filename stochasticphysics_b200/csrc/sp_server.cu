@@ -115,8 +115,12 @@ struct sp_server {
     LaunchConfig launch_for(const sp_ensemble_desc& d, unsigned long long* chunks_per_round = nullptr) const {
         LaunchConfig c = launch_config_for(ctx, d);
         const unsigned long long W = d.oversampling;
-        const unsigned long long round = cfg.chunk_steps ? std::max<unsigned long long>(cfg.chunk_steps, 1)
-                                                         : std::min(c.chunk, whole_windows(kServeChunk, W));
+        // no longer than the run itself, (K - 1) W steps: a configured round of 1e9 steps
+        // would otherwise become 1e6 launches of which all but the first few do nothing
+        const unsigned long long S = (d.number_of_steps / W - 1) * W;
+        const unsigned long long round =
+            std::min(cfg.chunk_steps ? cfg.chunk_steps : std::min(c.chunk, whole_windows(kServeChunk, W)),
+                     std::max<unsigned long long>(S, 1));
         c.chunk = round <= kSliceSteps ? round : std::min(round, whole_windows(kSliceSteps, W));
         if (chunks_per_round) *chunks_per_round = std::max<unsigned long long>(1, round / c.chunk);
         return c;
