@@ -57,3 +57,22 @@ def test_bench_workloads_integrate_whole_windows():
     for s in specs:
         assert s.integrated_steps > 0 and s.integrated_steps % s.oversampling == 0
         assert s.number_of_steps >= 2 * s.oversampling
+
+
+def test_co_scheduled_shape_passes_the_shape_checks():
+    """The bench's side-by-side ensembles take the tuned (here: default) shape with
+    CO_CHUNK-step chunks; sp_ensemble_create_shaped accepts it (it stops only at the
+    missing context)."""
+    import ctypes as C
+    from stochasticphysics_b200._abi import DescHolder, Precision, sp_launch_config
+    from stochasticphysics_b200.lib import load
+    lib = load()
+    for spec in bench.workload_specs(bench.N_PER_GPU, 4 * bench.CHUNK, Precision.FP32, 0):
+        out = sp_launch_config()
+        assert lib.sp_launch_config_for(None, DescHolder(spec).byref(), C.byref(out)) == 0
+        shape = dict(out.to_dict(), chunk_steps=bench.CO_CHUNK)
+        lc = sp_launch_config(block=shape["block"], persistent=shape["persistent"], chunk_steps=shape["chunk_steps"],
+                              particles_per_thread=shape["particles_per_thread"])
+        h = C.c_void_p()
+        assert lib.sp_ensemble_create_shaped(None, DescHolder(spec).byref(), C.byref(lc), C.byref(h)) == 1
+        assert "ctx is NULL" in lib.sp_last_error().decode()
