@@ -13,11 +13,15 @@
 //
 // Set-up: the first call on each device resolves the array's device address
 // with cudaGetSymbolAddress (with that device current) and caches it; make that
-// first call before any stream capture begins.  All calls share the array and
-// each call re-initialises what it uses, so calls whose work overlaps on the
-// GPU (different streams or threads at once) race; serialise them.
+// first call before any stream capture begins.  The cached address belongs to the
+// device's current context: after cudaDeviceReset (or any teardown of the primary
+// context) the library must be reloaded before this entry point is used again.
+// All calls share the array and each call re-initialises what it uses, so calls
+// whose work overlaps on the GPU (different streams or threads at once) race;
+// serialise them.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -36,8 +40,12 @@ namespace {
 std::mutex g_noalloc_mu;
 void* g_noalloc_addr[64] = {};
 
-__global__ void noalloc_tiles_kernel(TileDesc* tiles, int ntiles, int block) {
+// the ensemble descriptor and the tile list: the descriptor travels as a kernel
+// argument (copied when the launch is issued), so nothing is read from host memory
+// after the call returns
+__global__ void noalloc_setup_kernel(EnsDev* dst, EnsDev e, TileDesc* tiles, int ntiles, int block) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) *dst = e;
     if (i < ntiles) tiles[i] = TileDesc{0u, static_cast<unsigned>(i * block)};
 }
 
@@ -142,6 +150,7 @@ extern "C" SP_API sp_status sp_simulate_noalloc(const sp_ensemble_desc* desc, co
         e.moment = reinterpret_cast<double*>(base + o_moment); e.status = base + o_status;
         e.partial = reinterpret_cast<double*>(base + o_partial); e.ftab = base + o_ftab;
         e.msum = device_mean; e.wsum = device_weight; e.traj = nullptr; e.dw = nullptr;
+        e.traj_stride = 1; e.traj_n = 0;
         e.ctl = reinterpret_cast<EnsCtl*>(base + o_ctl);
         EnsDev* d_ens = reinterpret_cast<EnsDev*>(base + o_ens);
         TileDesc* d_tiles = reinterpret_cast<TileDesc*>(base + o_tiles);
@@ -149,9 +158,7 @@ extern "C" SP_API sp_status sp_simulate_noalloc(const sp_ensemble_desc* desc, co
         // the array keeps the previous call's contents: clear the control block and the outputs
         check_cuda(cudaMemsetAsync(e.ctl, 0, sizeof(EnsCtl), s), "clear control block");
         check_cuda(cudaMemsetAsync(device_mean, 0, L.K * L.OUT * 8, s), "clear mean");
-        // from pageable host memory the copy has taken `e` before cudaMemcpyAsync returns
-        check_cuda(cudaMemcpyAsync(d_ens, &e, sizeof(EnsDev), cudaMemcpyHostToDevice, s), "upload descriptor");
-        noalloc_tiles_kernel<<<(ntiles + 127) / 128, 128, 0, s>>>(d_tiles, ntiles, lc.block);
+        noalloc_setup_kernel<<<(std::max(ntiles, 1) + 127) / 128, 128, 0, s>>>(d_ens, e, d_tiles, ntiles, lc.block);
 
         RawParticles rp;
         rp.radius = dp.magnetic_radius; rp.Ms = dp.saturation_magnetisation; rp.alpha = dp.damping_constant;
@@ -164,7 +171,7 @@ extern "C" SP_API sp_status sp_simulate_noalloc(const sp_ensemble_desc* desc, co
         rp.simple_model = desc->problem_settings.use_simple_model;
         ks.init(d_ens, rp, L.Np, s);
         ks.reduce(d_ens, 1, 2, 1, s);
-        launches_add(3);  // tiles, init, reduce
+        launches_add(3);  // descriptor and tiles, init, reduce
         if (L.S > 0) {
             launch_set_target(e.ctl, L.S, s);
             const int midpoint = desc->solver == SP_SOLVER_IMPLICIT_MIDPOINT ? 1 : 0;

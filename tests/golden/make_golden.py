@@ -248,4 +248,6 @@ def main(ref_root: Path) -> None:
 
 
 if __name__ == "__main__":
-    main(Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference"))
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <root of the StochasticPhysics source tree>")
+    main(Path(sys.argv[1]))
