@@ -34,7 +34,7 @@
 extern "C" {
 #endif
 
-#define SP_ABI_VERSION 7u
+#define SP_ABI_VERSION 8u
 
 #if defined(_WIN32)
 #define SP_API __declspec(dllexport)
@@ -241,8 +241,10 @@ typedef struct sp_ensemble_desc {
     int32_t noise;        /* sp_noise       */
     sp_problem_settings problem_settings;
     int32_t max_iteration;       /* Solver_Settings Max_Iterations (ImplicitMidpoint) */
-    int32_t record_trajectories; /* keep per-particle window means on the device (parity
-                                    runs; the reference's per-particle result vectors) */
+    int32_t record_trajectories; /* 0: none; s >= 1: keep the window means of every s-th
+                                    particle (ensemble indices s-1, 2s-1, ...: the reference's
+                                    Save_intervall rule, SimulationResultManager.h:117-118), 1 =
+                                    every particle (parity runs); read as sp_result.trajectories */
     int32_t jacobian;            /* sp_jacobian (ImplicitMidpoint only)               */
     int32_t double_noise_approx; /* Solver_Settings Approximation_of_double_noise_integral
                                     (WeakTest, ExplicitStrong_1.0): order p of the double
@@ -275,8 +277,13 @@ typedef struct sp_result {
     double* weight;       /* [out_dim] summed weights (Ms*V per component)                */
     double* time;         /* [n_samples] window-centre times (SingleParticleSimulator.h:236-273) */
     double* field;        /* [n_samples][3] window-mean field                             */
-    double* trajectories; /* [n_particles][n_samples][out_dim] per-particle window means  */
+    double* trajectories; /* [n_particles / s][n_samples][out_dim] window means of the
+                             particles record_trajectories = s selects (all when s = 1)  */
     double* final_state;  /* [n_particles][state_dim] state after the last step           */
+    double* weighted_sum; /* [n_samples][out_dim] the un-normalised sums sum_p w_p r_p[k] that
+                             MeanSimulationResult accumulates before normalize divides them by
+                             the weight (Results/MeanSimulationResult.h:87-119); what shards of
+                             one ensemble exchange to be merged (sp_merge_shards)              */
 } sp_result;
 
 typedef struct sp_stats {
@@ -303,6 +310,20 @@ SP_API sp_status sp_query_dims(int32_t problem, int32_t* state_dim, int32_t* noi
 SP_API sp_status sp_validate(const sp_ensemble_desc* desc);
 /* Total kernels this process launched through the library. */
 SP_API uint64_t sp_kernel_launch_count(void);
+
+/* ---- shards -------------------------------------------------------------
+ * Merges the results of shards of one ensemble (the same description split by
+ * particle_id_offset, e.g. one shard per GPU) into the result of the whole: the
+ * reference folds every particle into MeanSimulationResult::operator+= (weighted
+ * result and weight added, Results/MeanSimulationResult.h:87-119) and normalize()
+ * divides by the summed weight unless it is all zero (:63-75).  Inputs are each
+ * shard's weighted_sum [n_samples][out_dim] and weight [out_dim] (sp_result);
+ * they are added in FP64 in shard order.  Outputs (any may be NULL): mean_out
+ * [n_samples][out_dim], weighted_sum_out [n_samples][out_dim], weight_out
+ * [out_dim].  Host memory only; needs no device. */
+SP_API sp_status sp_merge_shards(int32_t n_shards, uint64_t n_samples, int32_t out_dim,
+                                 const double* const* weighted_sums, const double* const* weights,
+                                 double* mean_out, double* weighted_sum_out, double* weight_out);
 
 /* ---- context ----------------------------------------------------------- */
 SP_API sp_status sp_create(sp_context** ctx, int32_t device);
@@ -444,8 +465,10 @@ SP_API sp_status sp_provide_particles(sp_context* ctx, const sp_ensemble_desc* d
  * static device array of 32 MiB that each GPU loading the library holds until
  * exit; ensembles needing more are refused with SP_ERR_INVALID_ARG.  Philox noise
  * only, no trajectories.  The first call on a device resolves the array's
- * address (make it before any stream capture); calls overlapping on the GPU
- * share the array and race. */
+ * address (make it before any stream capture) and keeps it for the life of the
+ * device's context: after cudaDeviceReset the library must be reloaded before
+ * this entry point is used again.  Calls overlapping on the GPU share the array
+ * and race. */
 SP_API sp_status sp_simulate_noalloc(const sp_ensemble_desc* desc, const sp_particles* device_particles,
                                      double* device_mean, double* device_weight, void* cuda_stream);
 

@@ -10,8 +10,8 @@ from ._abi import (Anisotropy, DistSpec, Distribution, EnsembleSpec, FieldSpec, 
                    Noise, ParticleTemplateSpec, Precision, ProviderSpec,
                    Problem, RequestState, Solver, Status, DIMS)
 from .lib import SPError, load  # noqa: F401
-from .simulator import Context, DeviceEnsemble, Server, SimulationResult, kernel_launch_count  # noqa: F401
+from .simulator import Context, DeviceEnsemble, Server, SimulationResult, kernel_launch_count, merge_shards  # noqa: F401
 
 __all__ = ["Anisotropy", "DistSpec", "Distribution", "ParticleTemplateSpec", "ProviderSpec", "EnsembleSpec", "FieldSpec", "FieldType", "Jacobian", "Noise", "Precision", "Problem", "RequestState",
            "Solver", "Status", "DIMS", "SPError", "load", "Context", "DeviceEnsemble", "Server", "SimulationResult",
-           "kernel_launch_count"]
+           "kernel_launch_count", "merge_shards"]

@@ -13,7 +13,7 @@ from typing import Optional
 
 import numpy as np
 
-ABI_VERSION = 7
+ABI_VERSION = 8
 
 
 class Status(IntEnum):
@@ -203,6 +203,7 @@ class sp_result(C.Structure):
         ("field", _dp),
         ("trajectories", _dp),
         ("final_state", _dp),
+        ("weighted_sum", _dp),
     ]
 
 
@@ -414,7 +415,7 @@ class EnsembleSpec:
     neel_min_angle_before_transformation: float = 0.0
     use_simple_model: bool = False
     injected_dw: Optional[np.ndarray] = None
-    record_trajectories: bool = False
+    record_trajectories: int = 0  # 0/False: none; s (True = 1): every s-th particle's window means
     jacobian: Jacobian = Jacobian.Reference
     double_noise_approx: int = -1                    # WeakTest / ExplicitStrong_1: order p, -1..10
     cubic_constant: Optional[np.ndarray] = None      # UniaxialCubic: K_cubic (n)
@@ -487,7 +488,7 @@ class DescHolder:
         ps.brown_min_angle_before_transformation = float(spec.brown_min_angle_before_transformation)
         ps.neel_min_angle_before_transformation = float(spec.neel_min_angle_before_transformation)
         d.max_iteration = int(spec.max_iteration)
-        d.record_trajectories = int(bool(spec.record_trajectories))
+        d.record_trajectories = int(spec.record_trajectories)
         d.jacobian = int(spec.jacobian)
         d.double_noise_approx = int(spec.double_noise_approx)
         d.accuracy_goal = float(spec.accuracy_goal)
@@ -526,19 +527,23 @@ class ResultBuffers:
         self.weight = np.zeros(od)
         self.time = np.zeros(k)
         self.field = np.zeros((k, 3))
-        self.trajectories = np.zeros((spec.n, k, od)) if trajectories else None
+        self.weighted_sum = np.zeros((k, od))
+        stride = max(1, int(spec.record_trajectories))  # the recorded particles: every stride-th
+        self.trajectories = np.zeros((spec.n // stride, k, od)) if trajectories else None
         self.final_state = np.zeros((spec.n, sd)) if final_state else None
         r = sp_result()
         r.mean = _ptr(self.mean)
         r.weight = _ptr(self.weight)
         r.time = _ptr(self.time)
         r.field = _ptr(self.field)
+        r.weighted_sum = _ptr(self.weighted_sum)
         r.trajectories = _ptr(self.trajectories)
         r.final_state = _ptr(self.final_state)
         self.c = r
 
     def as_dict(self):
-        d = {"mean": self.mean, "weight": self.weight, "time": self.time, "field": self.field}
+        d = {"mean": self.mean, "weight": self.weight, "time": self.time, "field": self.field,
+             "weighted_sum": self.weighted_sum}
         if self.trajectories is not None:
             d["trajectories"] = self.trajectories
         if self.final_state is not None:

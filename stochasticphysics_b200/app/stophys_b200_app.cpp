@@ -6,7 +6,8 @@
 // build every particle through the provider (Provider/ParticleProvider.h:194-217,
 // Settings/ParticleSimulationSettings.h:51-152), run the ensemble on the GPU and
 // write the mean result {Time, Field, Results, Weight, Mean_Properties}
-// (Results/MeanSimulationResult.h:131-141) as JSON.
+// (Results/MeanSimulationResult.h:131-141) as JSON, and with Save_single_simulations
+// every Save_intervall-th particle's own result (Results/SimulationResultManager.h:115-149).
 //
 // Accepted keys are the names the reference's serialize() functions use, plus the
 // older field layout of its example files (Amplitude_1 = offset, Amplitude_2 =
@@ -343,6 +344,10 @@ struct Run {
     std::vector<ParticleTemplate> templates;
     std::vector<uint64_t> used;
     std::string savefile;
+    // Result_Settings single-simulation keys (ResultSettings.h:90-118)
+    bool save_single = false, extra_single_files = false;
+    unsigned long long save_interval = 1;
+    std::string single_prefix = "Simulation", single_savefile = "ResultsSingle.json";
     bool discrete = false;
     // -device-provider: the templates as an sp_provider_desc (particles drawn on the GPU)
     std::vector<sp_particle_template> dev_templates;
@@ -560,7 +565,49 @@ Run build(const std::string& path, unsigned long long seed, int precision) {
                    run.rh.data(), run.eta.data(), run.euler.data(), run.mag.data(),
                    uc ? run.K2.data() : nullptr, uc ? run.urot.data() : nullptr};
     if (auto v = opt("Result_Settings", "Savefile")) run.savefile = Ini::str(*v);
+    if (auto v = opt("Result_Settings", "Save_single_simulations")) run.save_single = Ini::boolean(*v);
+    if (auto v = opt("Result_Settings", "Use_extra_file_for_single_simulations")) run.extra_single_files = Ini::boolean(*v);
+    if (auto v = opt("Result_Settings", "Save_single_name_prefix")) run.single_prefix = Ini::str(*v);
+    if (auto v = opt("Result_Settings", "Single_simulations_savefile")) run.single_savefile = Ini::str(*v);
+    if (auto v = opt("Result_Settings", "Save_intervall")) {
+        const double iv = Ini::num(*v);
+        if (!(iv >= 1) || iv != std::floor(iv)) throw std::runtime_error("Save_intervall must be a positive integer");
+        run.save_interval = static_cast<unsigned long long>(iv);
+    }
     return run;
+}
+
+// ------------------------------------------------------------------ single-simulation results
+// SimulationResultManager::addSingleResult (Results/SimulationResultManager.h:115-149):
+// result counter c = 1, 2, ... (particle order here; completion order in the reference's
+// thread pool); every Save_intervall-th is written as the named value <prefix>_<c>, either
+// all into Single_simulations_savefile or, with Use_extra_file_for_single_simulations, each
+// into its own file named <prefix>_<c> beside it with its extension.  The reference refuses
+// a single-results file equal to Savefile.  Files are JSON (the reference's SerAr MATLAB/HDF5
+// archives are not available), so a configured extension other than .json becomes .json.
+std::string json_path(const std::string& path) {
+    const auto slash = path.find_last_of('/');
+    const auto dot = path.find_last_of('.');
+    const bool has_ext = dot != std::string::npos && (slash == std::string::npos || dot > slash);
+    return (has_ext ? path.substr(0, dot) : path) + ".json";
+}
+std::string single_name(const Run& run, unsigned long long counter) {
+    return run.single_prefix + "_" + std::to_string(counter);
+}
+std::string single_file(const Run& run, unsigned long long counter) {
+    const std::string base = json_path(run.single_savefile);
+    if (!run.extra_single_files) return base;
+    const auto slash = base.find_last_of('/');
+    const std::string dir = slash == std::string::npos ? "" : base.substr(0, slash + 1);
+    return dir + single_name(run, counter) + ".json";
+}
+// number of particles the single-result settings select (counter % interval == 0)
+unsigned long long single_count(const Run& run) {
+    return run.save_single ? run.d.n_particles / run.save_interval : 0;
+}
+void check_single_settings(const Run& run) {
+    if (single_count(run) > 0 && run.single_savefile == run.savefile)
+        throw std::runtime_error("Writing SingleResults and MeanResult to same file currently not supported!");
 }
 
 // ------------------------------------------------------------------ system matrix
@@ -729,7 +776,13 @@ void write_description(std::ostream& o, const Run& run) {
         o << ",\"uniaxial_rotation\":";
         jrows(o, run.urot.data(), n, 3);
     }
-    o << "},\"savefile\":" << jstr(run.savefile) << "}\n";
+    o << "},\"single_results\":[";
+    for (unsigned long long i = 0; i < single_count(run); ++i) {
+        const unsigned long long c = (i + 1) * run.save_interval;
+        o << (i ? "," : "") << "{\"particle\":" << c - 1 << ",\"name\":" << jstr(single_name(run, c))
+          << ",\"file\":" << jstr(single_file(run, c)) << "}";
+    }
+    o << "],\"savefile\":" << jstr(run.savefile) << "}\n";
 }
 
 void write_mean_results(std::ostream& os, const std::vector<double>& time, const std::vector<double>& field,
@@ -749,6 +802,53 @@ void write_mean_results(std::ostream& os, const std::vector<double>& time, const
        << ",\"Damping_constant\":" << jnum(mean_of(run.alpha)) << ",\"Gyromagnetic_ratio\":" << jnum(mean_of(run.gamma))
        << ",\"Anisotropy_constant\":" << jnum(mean_of(run.K)) << ",\"Hydrodynamic_Radius\":" << jnum(mean_of(run.rh))
        << ",\"Viscosity\":" << jnum(mean_of(run.eta)) << "}}";
+}
+
+// The recorded window means of the selected particles, one named value each
+// (SingleSimulationResult::save, Results/SingleSimulationResult.h:96-104: UsedProperties,
+// Time, Weight, Field, Results).  traj is [count][K][od] as sp_result returns it.
+void write_single_results(const Run& run, const std::vector<double>& traj, const std::vector<double>& time,
+                          const std::vector<double>& field, size_t K, size_t od) {
+    const sp_ensemble_desc& d = run.d;
+    const unsigned long long count = single_count(run);
+    std::ofstream shared;
+    for (unsigned long long i = 0; i < count; ++i) {
+        const unsigned long long c = (i + 1) * run.save_interval, p = c - 1;
+        std::ofstream own;
+        std::ofstream& f = run.extra_single_files ? own : shared;
+        if (run.extra_single_files || i == 0) {
+            f.open(single_file(run, c));
+            if (!f) throw std::runtime_error("cannot write " + single_file(run, c));
+            f << "{";
+        } else {
+            f << ",";
+        }
+        // getWeighting: Ms V for every output, 1 for the axis of the coupled Cartesian problem
+        // (NeelRelaxation.h:287-291, BrownAndNeelRelaxation.h:152-159)
+        const double kPi = 3.14159265358979323846;
+        const double moment = run.Ms[p] * 4.0 / 3.0 * kPi * run.r[p] * run.r[p] * run.r[p];
+        std::vector<double> w(od, moment);
+        if (d.problem == SP_PROBLEM_BROWN_AND_NEEL)
+            for (size_t k = 0; k < 3; ++k) w[k] = 1.0;
+        f << jstr(single_name(run, c)) << ":{\"UsedProperties\":{\"Temperature\":" << jnum(d.temperature)
+          << ",\"Magnetic_radius\":" << jnum(run.r[p]) << ",\"Saturation_magnetisation\":" << jnum(run.Ms[p])
+          << ",\"Damping_constant\":" << jnum(run.alpha[p]) << ",\"Gyromagnetic_ratio\":" << jnum(run.gamma[p])
+          << ",\"Anisotropy_constant\":" << jnum(run.K[p]) << ",\"Hydrodynamic_Radius\":" << jnum(run.rh[p])
+          << ",\"Viscosity\":" << jnum(run.eta[p]) << "},\"Time\":";
+        jarr(f, time.data(), K);
+        f << ",\"Weight\":";
+        jarr(f, w.data(), od);
+        f << ",\"Field\":";
+        jrows(f, field.data(), K, 3);
+        f << ",\"Results\":";
+        jrows(f, traj.data() + i * K * od, K, od);
+        f << "}";
+        if (run.extra_single_files || i + 1 == count) {
+            f << "}\n";
+            f.close();
+            if (!f) throw std::runtime_error("writing " + single_file(run, c) + " failed");
+        }
+    }
 }
 
 // File name of one voxel's result: Savefile stem + "_Vox_x_y_z" + extension
@@ -819,7 +919,7 @@ int run_sysmatrix(const Run& run, const SysMat& sm, std::ostream& os, int device
     double max_latency = 0.0;
     for (size_t i = 0; i < descs.size() && err.empty(); ++i) {
         std::vector<double> mean(K * od), weight(od), time(K), field(3 * K);
-        sp_result res{mean.data(), weight.data(), time.data(), field.data(), nullptr, nullptr};
+        sp_result res{mean.data(), weight.data(), time.data(), field.data(), nullptr, nullptr, nullptr};
         sp_stats st{};
         double lat = 0.0;
         if (sp_server_wait(srv, ids[i], -1.0, &res, &st, &lat) != SP_OK) {
@@ -882,7 +982,13 @@ int main(int argc, char** argv) {
             if (!fo) throw std::runtime_error("cannot write " + out);
         }
         std::ostream& os = out.empty() ? std::cout : fo;
-        if (!sysmatrix.empty()) return run_sysmatrix(run, SysMat::load(sysmatrix), os, device, print_only);
+        check_single_settings(run);
+        if (!sysmatrix.empty()) {
+            if (single_count(run) > 0)
+                std::fprintf(stderr, "stophys_b200: Save_single_simulations applies to plain runs; the system-matrix "
+                                     "sweep writes mean results only\n");
+            return run_sysmatrix(run, SysMat::load(sysmatrix), os, device, print_only);
+        }
         if (print_only) {
             write_description(os, run);
             return 0;
@@ -891,7 +997,16 @@ int main(int argc, char** argv) {
         if (sp_query_dims(d.problem, &sd, &nd, &od) != SP_OK) throw std::runtime_error(sp_last_error());
         const size_t K = d.number_of_steps / d.oversampling;
         std::vector<double> mean(K * od), weight(od), time(K), field(3 * K);
-        sp_result res{mean.data(), weight.data(), time.data(), field.data(), nullptr, nullptr};
+        sp_result res{mean.data(), weight.data(), time.data(), field.data(), nullptr, nullptr, nullptr};
+        // single-simulation results: the device records every Save_intervall-th particle only
+        const unsigned long long nsingle = single_count(run);
+        std::vector<double> traj;
+        if (nsingle > 0) {
+            if (run.save_interval > 0x7fffffffull) throw std::runtime_error("Save_intervall exceeds 2^31 - 1");
+            run.d.record_trajectories = static_cast<int32_t>(run.save_interval);
+            traj.assign(nsingle * K * od, 0.0);
+            res.trajectories = traj.data();
+        }
         sp_stats st{};
         sp_context* ctx = nullptr;
         if (sp_create(&ctx, device) != SP_OK) throw std::runtime_error(sp_last_error());
@@ -911,6 +1026,7 @@ int main(int argc, char** argv) {
         }
         sp_destroy(ctx);
         if (s != SP_OK) throw std::runtime_error(sp_last_error());
+        if (nsingle > 0) write_single_results(run, traj, time, field, K, static_cast<size_t>(od));
         os << "{\"Mean_Results\":";
         write_mean_results(os, time, field, mean, weight, K, static_cast<size_t>(od), run);
         os << ",\"Stats\":{\"particle_steps\":" << st.particle_steps

@@ -208,7 +208,8 @@ __global__ void __launch_bounds__(kMaxBlock) init_kernel(const EnsDev* __restric
     for (int c = 0; c < OUT; ++c) {
         const double w = active ? weight_of<PROB>(c, moment) : 0.0;
         const double vo = active ? static_cast<double>(o[c]) : 0.0;
-        if (e.traj && active) e.traj[static_cast<unsigned long long>(c) * Np + p] = vo;
+        if (e.traj && active && (p + 1) % e.traj_stride == 0)
+            e.traj[static_cast<unsigned long long>(c) * e.traj_n + (p + 1) / e.traj_stride - 1] = vo;
         const double s0 = warp_sum(w * vo), s1 = warp_sum(w);
         if (lane == 0) {
             e.partial[(warp * e.slots + 0) * OUT + c] = s0;
@@ -429,6 +430,9 @@ __global__ void __launch_bounds__(kMaxBlock / PPT) step_kernel(const EnsDev* __r
                     for (int k = 0; k < PPT; ++k) {
                         const double mom = active[k] ? e.moment[p[k]] : 0.0;
                         double* const partial = e.partial + ((p[k] >> 5) * e.slots + slot) * OUT;
+                        // recorded particles: every traj_stride-th (the reference's Save_intervall)
+                        const bool rec = traj && active[k] && (p[k] + 1) % e.traj_stride == 0;
+                        const unsigned long long ti = rec ? (p[k] + 1) / e.traj_stride - 1 : 0;
                         // the butterfly leaves every lane with the same sums; lane c keeps
                         // component c, and the warp writes its OUT sums in one coalesced store
                         const int lane = threadIdx.x & 31;
@@ -438,7 +442,7 @@ __global__ void __launch_bounds__(kMaxBlock / PPT) step_kernel(const EnsDev* __r
                             const R v = active[k] ? acc[k].get_sum(c) / static_cast<R>(static_cast<double>(W)) : R(0);
                             acc[k].clear_sum(c);
                             const double vd = static_cast<double>(v);
-                            if (traj && active[k]) traj[(kw * OUT + c) * Np + p[k]] = vd;
+                            if (rec) traj[(kw * OUT + c) * e.traj_n + ti] = vd;
                             const double ws = warp_sum(active[k] ? weight_of<PROB>(c, mom) * vd : 0.0);
                             if (lane == c) mine = ws;
                         }

@@ -68,6 +68,7 @@ sp_status validate_desc(const sp_ensemble_desc* d, std::string& why) {
     if (d->n_particles == 0) return bad("n_particles must be > 0");
     if (d->n_particles > (1ull << 31)) return bad("n_particles exceeds 2^31");
     if (d->oversampling == 0) return bad("oversampling must be > 0");
+    if (d->record_trajectories < 0) return bad("record_trajectories must be >= 0 (0 = none, s = every s-th particle)");
     if (d->oversampling >= (1ull << 31)) return bad("oversampling must be < 2^31");
     if (d->number_of_steps < d->oversampling) return bad("number_of_steps must be >= oversampling");
     if (!(d->timestep > 0.0) || !std::isfinite(d->timestep)) return bad("timestep must be finite and > 0");
@@ -168,7 +169,7 @@ EnsembleLayout layout_of(const sp_ensemble_desc& d, const LaunchConfig& lc) {
     L.bytes = L.Np * (L.D + 2ull * L.OUT + L.P) * L.real + L.Np * 8 + L.Np + nw * L.slots * L.OUT * 8 +
               L.K * L.OUT * 8 + L.OUT * 8 + L.K * 3 * 8 + L.chunk * 3 * L.real + sizeof(EnsCtl) + sizeof(EnsDev) +
               ((L.Np + 31) / 32 + 1) * sizeof(TileDesc);
-    if (d.record_trajectories) L.bytes += L.K * L.OUT * L.Np * 8;
+    if (d.record_trajectories > 0) L.bytes += L.K * L.OUT * (L.n / d.record_trajectories) * 8;
     if (d.noise == SP_NOISE_INJECTED) L.bytes += L.S * L.Mn * L.Np * L.real;
     return L;
 }
@@ -206,7 +207,9 @@ Ensemble::Ensemble(sp_context* c, const sp_ensemble_desc& d, const LaunchConfig&
     d_ftab = dalloc(L.chunk * 3 * R);
     d_ctl = static_cast<EnsCtl*>(dalloc(sizeof(EnsCtl)));
     d_ens = static_cast<EnsDev*>(dalloc(sizeof(EnsDev)));
-    if (d.record_trajectories) d_traj = static_cast<double*>(dalloc(L.K * L.OUT * L.Np * 8));
+    traj_stride = d.record_trajectories > 0 ? static_cast<unsigned long long>(d.record_trajectories) : 0;
+    traj_n = traj_stride ? L.n / traj_stride : 0;
+    if (traj_n) d_traj = static_cast<double*>(dalloc(L.K * L.OUT * traj_n * 8));
     check_cuda(cudaMemsetAsync(d_msum, 0, L.K * L.OUT * 8, stream), "memset");
     check_cuda(cudaMemsetAsync(d_ctl, 0, sizeof(EnsCtl), stream), "memset");
 
@@ -253,6 +256,7 @@ Ensemble::Ensemble(sp_context* c, const sp_ensemble_desc& d, const LaunchConfig&
     e.slots = L.slots;
     e.state = d_state; e.ksum = d_ksum; e.kcomp = d_kcomp; e.params = d_params; e.moment = d_moment;
     e.dw = d_dw; e.partial = d_partial; e.msum = d_msum; e.wsum = d_wsum; e.traj = d_traj; e.ftab = d_ftab;
+    e.traj_stride = traj_stride ? traj_stride : 1; e.traj_n = traj_n;
     e.status = d_status; e.ctl = d_ctl;
     check_cuda(cudaMemcpyAsync(d_ens, &e, sizeof(EnsDev), cudaMemcpyHostToDevice, stream), "upload EnsDev");
 
@@ -467,19 +471,21 @@ void Ensemble::read(sp_result* out, sp_stats* st) {
                 for (int c = 0; c < OUT; ++c) out->mean[k * OUT + c] = allzero ? msum[k * OUT + c] : msum[k * OUT + c] / wsum[c];
         }
         if (out->weight) std::memcpy(out->weight, wsum.data(), OUT * 8);
+        if (out->weighted_sum) std::memcpy(out->weighted_sum, msum.data(), msum.size() * 8);
         if (out->time) reference_times(L.K, L.W, desc.timestep, out->time);
         if (out->field) {
             check_cuda(cudaMemcpy(out->field, d_field, L.K * 3 * 8, cudaMemcpyDeviceToHost), "read field");
             d2h_bytes += L.K * 3 * 8;
         }
         if (out->trajectories) {
-            if (!d_traj) throw Error(SP_ERR_INVALID_ARG, "trajectories were not recorded (record_trajectories = 0)");
-            std::vector<double> t(L.K * OUT * L.Np);
-            check_cuda(cudaMemcpy(t.data(), d_traj, t.size() * 8, cudaMemcpyDeviceToHost), "read traj");
+            if (!traj_stride)
+                throw Error(SP_ERR_INVALID_ARG, "trajectories were not recorded (record_trajectories = 0)");
+            std::vector<double> t(L.K * OUT * traj_n);
+            if (traj_n) check_cuda(cudaMemcpy(t.data(), d_traj, t.size() * 8, cudaMemcpyDeviceToHost), "read traj");
             d2h_bytes += t.size() * 8;
-            for (size_t p = 0; p < L.n; ++p)
+            for (size_t p = 0; p < traj_n; ++p)
                 for (size_t k = 0; k < L.K; ++k)
-                    for (int c = 0; c < OUT; ++c) out->trajectories[(p * L.K + k) * OUT + c] = t[(k * OUT + c) * L.Np + p];
+                    for (int c = 0; c < OUT; ++c) out->trajectories[(p * L.K + k) * OUT + c] = t[(k * OUT + c) * traj_n + p];
         }
         if (out->final_state) {
             std::vector<unsigned char> s(L.D * L.Np * L.real);
@@ -543,6 +549,36 @@ sp_status sp_validate(const sp_ensemble_desc* desc) {
     std::string why;
     const sp_status s = validate_desc(desc, why);
     return s == SP_OK ? SP_OK : fail(s, why);
+}
+
+// MeanSimulationResult::operator+= over shards (Results/MeanSimulationResult.h:87-119):
+// sums and weights added in shard order, then normalize() (:63-75), which leaves the
+// sums as they are when every weight is zero.
+sp_status sp_merge_shards(int32_t n_shards, uint64_t n_samples, int32_t out_dim, const double* const* weighted_sums,
+                          const double* const* weights, double* mean_out, double* weighted_sum_out,
+                          double* weight_out) {
+    SP_GUARD_BEGIN
+    if (n_shards < 1) return fail(SP_ERR_INVALID_ARG, "n_shards must be at least 1");
+    if (out_dim < 1 || out_dim > 9) return fail(SP_ERR_INVALID_ARG, "out_dim must be 1..9");
+    if (!weighted_sums || !weights) return fail(SP_ERR_INVALID_ARG, "weighted_sums and weights are required");
+    for (int32_t s = 0; s < n_shards; ++s)
+        if (!weighted_sums[s] || !weights[s])
+            return fail(SP_ERR_INVALID_ARG, "shard " + std::to_string(s) + " has a NULL weighted_sum or weight");
+    const size_t cells = static_cast<size_t>(n_samples) * static_cast<size_t>(out_dim);
+    std::vector<double> sum(cells, 0.0), w(out_dim, 0.0);
+    for (int32_t s = 0; s < n_shards; ++s) {
+        for (int32_t c = 0; c < out_dim; ++c) w[c] += weights[s][c];
+        const double* src = weighted_sums[s];
+        for (size_t i = 0; i < cells; ++i) sum[i] += src[i];
+    }
+    bool allzero = true;
+    for (int32_t c = 0; c < out_dim; ++c) allzero = allzero && w[c] == 0.0;
+    if (mean_out)
+        for (size_t i = 0; i < cells; ++i) mean_out[i] = allzero ? sum[i] : sum[i] / w[i % out_dim];
+    if (weighted_sum_out) std::memcpy(weighted_sum_out, sum.data(), cells * 8);
+    if (weight_out) std::memcpy(weight_out, w.data(), static_cast<size_t>(out_dim) * 8);
+    return SP_OK;
+    SP_GUARD_END
 }
 
 sp_status sp_create(sp_context** out, int32_t device) {
@@ -686,7 +722,7 @@ sp_status sp_simulate(sp_context* ctx, const sp_ensemble_desc* desc, sp_result* 
     const sp_status s = validate_desc(desc, why);
     if (s != SP_OK) return fail(s, why);
     sp_ensemble_desc d = *desc;
-    if (out && out->trajectories) d.record_trajectories = 1;
+    if (out && out->trajectories && d.record_trajectories == 0) d.record_trajectories = 1;
     Ensemble e(ctx, d, launch_config_for(ctx, d));
     e.advance(e.L.S, nullptr);
     e.read(out, stats);

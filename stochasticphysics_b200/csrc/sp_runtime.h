@@ -99,6 +99,7 @@ struct Ensemble {
     unsigned long long launches = 0, particle_steps = 0, steps_done = 0;
     unsigned long long h2d_bytes = 0, d2h_bytes = 0;
     int block = 128, grid = 1, ntiles = 0, ppt = 1;
+    unsigned long long traj_stride = 0, traj_n = 0;  // recorded particles: every traj_stride-th, traj_n of them
     EnsDev hdev;
     void *d_state = nullptr, *d_ksum = nullptr, *d_kcomp = nullptr, *d_params = nullptr, *d_dw = nullptr,
          *d_ftab = nullptr;

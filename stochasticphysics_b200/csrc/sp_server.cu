@@ -51,7 +51,7 @@ struct Request {
     unsigned long long chunks_per_round = 1;
     bool in_round = false;  // launched in the current round (not admitted during it)
     Clock::time_point t_submit, t_done;
-    std::vector<double> mean, weight, time, field;
+    std::vector<double> mean, weight, time, field, weighted_sum;
     sp_stats stats{};
 };
 
@@ -114,10 +114,11 @@ struct sp_server {
     }
     LaunchConfig launch_for(const sp_ensemble_desc& d, unsigned long long* chunks_per_round = nullptr) const {
         LaunchConfig c = launch_config_for(ctx, d);
-        const unsigned long long W = d.oversampling;
+        const unsigned long long W = std::max<unsigned long long>(d.oversampling, 1);
         // no longer than the run itself, (K - 1) W steps: a configured round of 1e9 steps
         // would otherwise become 1e6 launches of which all but the first few do nothing
-        const unsigned long long S = (d.number_of_steps / W - 1) * W;
+        // (K >= 1 is clamped here so an unvalidated description cannot underflow K - 1)
+        const unsigned long long S = (std::max<unsigned long long>(d.number_of_steps / W, 1) - 1) * W;
         const unsigned long long round =
             std::min(cfg.chunk_steps ? cfg.chunk_steps : std::min(c.chunk, whole_windows(kServeChunk, W)),
                      std::max<unsigned long long>(S, 1));
@@ -140,6 +141,8 @@ struct sp_server {
             r->weight.assign(r->ens->L.OUT, 0.0);
             r->time.assign(r->ens->L.K, 0.0);
             r->field.assign(r->ens->L.K * 3, 0.0);
+            r->weighted_sum.assign(r->ens->L.K * r->ens->L.OUT, 0.0);
+            out.weighted_sum = r->weighted_sum.data();
             out.mean = r->mean.data();
             out.weight = r->weight.data();
             out.time = r->time.data();
@@ -497,6 +500,7 @@ sp_status sp_server_wait(sp_server* s, uint64_t id, double timeout_ms, sp_result
         if (out->weight) std::memcpy(out->weight, r->weight.data(), r->weight.size() * 8);
         if (out->time) std::memcpy(out->time, r->time.data(), r->time.size() * 8);
         if (out->field) std::memcpy(out->field, r->field.data(), r->field.size() * 8);
+        if (out->weighted_sum) std::memcpy(out->weighted_sum, r->weighted_sum.data(), r->weighted_sum.size() * 8);
         if (out->trajectories || out->final_state)
             return fail(SP_ERR_INVALID_ARG, "the server returns ensemble results only");
     }

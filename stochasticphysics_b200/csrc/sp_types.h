@@ -9,7 +9,7 @@
 //   moment  [Np]         double Ms*V, the reference's getWeighting
 //   partial [warps][slots][OUT] double  per-warp weighted window means of one chunk
 //   msum    [K][OUT]     double weighted ensemble sums of every sample
-//   traj    [K][OUT][Np] double optional per-particle window means
+//   traj    [K][OUT][Nt] double optional window means of every s-th particle (Nt = n / s)
 //   dw      [S][M][Np]   Real   optional injected Wiener increments
 //   ftab    [chunk][3]   Real   B(t) of each step of the current chunk (FP64 phase, once per ensemble)
 #pragma once
@@ -100,7 +100,8 @@ struct EnsDev {
     double* partial;
     double* msum;   // [K][OUT] weighted ensemble sums
     double* wsum;   // [OUT] summed weights
-    double* traj;
+    double* traj;   // [K][OUT][traj_n] window means of particles traj_stride-1, 2 traj_stride-1, ...
+    unsigned long long traj_stride, traj_n;
     void* ftab;     // [chunk][3] Real: B(t) of every step of the current chunk
     unsigned char* status;
     EnsCtl* ctl;

@@ -21,7 +21,7 @@ SYMBOLS = [
     "sp_server_create", "sp_server_submit", "sp_server_poll", "sp_server_wait", "sp_server_cancel",
     "sp_server_destroy", "sp_debug_philox_normals", "sp_measure_fma_peak", "sp_simulate_noalloc",
     "sp_autotune", "sp_launch_config_for", "sp_tuning_save", "sp_tuning_load", "sp_tuning_reset",
-    "sp_provide_particles", "sp_ensemble_create_shaped", "sp_server_submit_many",
+    "sp_provide_particles", "sp_ensemble_create_shaped", "sp_server_submit_many", "sp_merge_shards",
 ]
 
 _lib = None
@@ -79,6 +79,7 @@ def load():
     L.sp_tuning_load.argtypes = [C.c_char_p]
     L.sp_tuning_reset.argtypes = []
     L.sp_provide_particles.argtypes = [vp, C.POINTER(sp_ensemble_desc), dp]
+    L.sp_merge_shards.argtypes = [i32, u64, i32, C.POINTER(dp), C.POINTER(dp), dp, dp, dp]
     for name in SYMBOLS:
         if name not in ("sp_last_error", "sp_abi_version", "sp_kernel_launch_count"):
             getattr(L, name).restype = C.c_int

@@ -32,8 +32,8 @@ def _driver() -> Path:
     return APP
 
 
-def _call(args, timeout):
-    p = subprocess.run([str(_driver()), *args], capture_output=True, text=True, timeout=timeout)
+def _call(args, timeout, cwd=None):
+    p = subprocess.run([str(_driver()), *args], capture_output=True, text=True, timeout=timeout, cwd=cwd)
     if p.returncode != 0:
         raise SettingsError(p.stderr.strip() or f"stophys_b200 exited with {p.returncode}")
     return p.stdout
@@ -45,7 +45,8 @@ def _flags(path, seed, precision):
 
 
 def describe_ini(path, seed: int = 0x5EED, precision: Precision = Precision.FP64, timeout: float = 120.0) -> dict:
-    """The parsed description and every provided particle, as the driver prints it."""
+    """The parsed description and every provided particle, as the driver prints it, with
+    the single-simulation results the Result_Settings select (particle, name, file)."""
     return json.loads(_call(_flags(path, seed, precision) + ["-print"], timeout))
 
 
@@ -96,15 +97,16 @@ def load_ini(path, seed: int = 0x5EED, precision: Precision = Precision.FP64) ->
 
 
 def run_ini(path, seed: int = 0x5EED, precision: Precision = Precision.FP64, device: int = 0,
-            timeout: float = 3600.0, sysmatrix=None, device_provider: bool = False) -> dict:
+            timeout: float = 3600.0, sysmatrix=None, device_provider: bool = False, cwd=None) -> dict:
     """Runs the .ini on `device` through the driver; returns its JSON record.  With
     `sysmatrix` (a System_Matrix_Settings .ini) it runs the voxel sweep: one
     ensemble per voxel, offset field moved to the voxel's field, Philox key
-    seed + voxel number, all batched through the server."""
+    seed + voxel number, all batched through the server.  Single-simulation result
+    files (Save_single_simulations) are written relative to `cwd`."""
     extra = [f"-sysmatrix:{sysmatrix}"] if sysmatrix else []
     if device_provider:  # particles drawn on the GPU from the same templates
         extra.append("-device-provider")
-    return json.loads(_call(_flags(path, seed, precision) + extra + [f"-device:{int(device)}"], timeout))
+    return json.loads(_call(_flags(path, seed, precision) + extra + [f"-device:{int(device)}"], timeout, cwd=cwd))
 
 
 def describe_sysmatrix(path, sysmatrix, seed: int = 0x5EED, timeout: float = 120.0) -> dict:

@@ -29,6 +29,8 @@ class SimulationResult:
     trajectories: Optional[np.ndarray] = None
     final_state: Optional[np.ndarray] = None
     stats: dict = field(default_factory=dict)
+    # un-normalised sum_p w_p r_p[k]: what shards of one ensemble exchange (merge_shards)
+    weighted_sum: Optional[np.ndarray] = None
 
 
 def _stats_dict(st: sp_stats) -> dict:
@@ -39,7 +41,29 @@ def _stats_dict(st: sp_stats) -> dict:
 
 def _result(buf: ResultBuffers, st: sp_stats) -> SimulationResult:
     return SimulationResult(time=buf.time, field=buf.field, mean=buf.mean, weight=buf.weight,
-                            trajectories=buf.trajectories, final_state=buf.final_state, stats=_stats_dict(st))
+                            trajectories=buf.trajectories, final_state=buf.final_state, stats=_stats_dict(st),
+                            weighted_sum=buf.weighted_sum)
+
+
+def merge_shards(weighted_sums, weights):
+    """Ensemble mean, weighted sums and weights of the union of shards of one description
+    (sp_merge_shards: MeanSimulationResult::operator+= over the shards in order, then
+    normalize; Particle_Simulation/Results/MeanSimulationResult.h:63-119).  Inputs are each
+    shard's ``weighted_sum`` [n_samples][out_dim] and ``weight`` [out_dim]."""
+    sums = [np.ascontiguousarray(s, dtype=np.float64) for s in weighted_sums]
+    ws = [np.ascontiguousarray(w, dtype=np.float64) for w in weights]
+    if not sums or len(sums) != len(ws):
+        raise ValueError("one weight vector per shard is needed")
+    k, od = sums[0].shape
+    if any(s.shape != (k, od) for s in sums) or any(w.shape != (od,) for w in ws):
+        raise ValueError("every shard needs weighted_sum [n_samples][out_dim] and weight [out_dim] of one shape")
+    dp = C.POINTER(C.c_double)
+    sp_arr = (dp * len(sums))(*[s.ctypes.data_as(dp) for s in sums])
+    w_arr = (dp * len(ws))(*[w.ctypes.data_as(dp) for w in ws])
+    mean, tot, wt = np.zeros((k, od)), np.zeros((k, od)), np.zeros(od)
+    check(load().sp_merge_shards(len(sums), k, od, sp_arr, w_arr, mean.ctypes.data_as(dp), tot.ctypes.data_as(dp),
+                                 wt.ctypes.data_as(dp)))
+    return mean, tot, wt
 
 
 class Context:

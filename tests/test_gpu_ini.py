@@ -105,3 +105,49 @@ def test_device_provider_run_agrees_statistically(tmp_path):
     # templates 1e-8 and 1.4e-8 m at weights 3:1, lognormal 10 %: mean 1.1e-8 m
     assert abs(mp["Magnetic_radius"] / 1.1e-8 - 1) < 0.02
     assert dev["Stats"]["particle_steps"] == host["Stats"]["particle_steps"]
+
+
+@pytest.mark.parametrize("extra_files", [False, True])
+def test_single_simulation_results_match_the_oracle(tmp_path, extra_files):
+    """Save_single_simulations: every 3rd particle's window means, written by the driver
+    (Results/SimulationResultManager.h:115-149), equal the oracle's trajectories of those
+    particles within the Philox-mode parity bar, with the particle's own weight Ms V."""
+    import json
+    import math
+
+    main = _copy(tmp_path, "legacy_neel_spherical.ini", 10, ("legacy_particle_small.ini", "legacy_particle_large.ini"))
+    text = main.read_text().replace(
+        "[Result_Settings]\nSavefile='legacy_result.mat'",
+        "[Result_Settings]\nSavefile='legacy_result.mat'\nSave_single_simulations = TRUE\nSave_intervall = 3\n"
+        "Single_simulations_savefile = 'singles/one.mat'\n"
+        f"Use_extra_file_for_single_simulations = {'TRUE' if extra_files else 'FALSE'}")
+    main.write_text(text)
+    (tmp_path / "singles").mkdir()
+    rec = settings.run_ini(main, seed=21, cwd=tmp_path)
+    spec = settings.load_ini(main, seed=21)
+    ref = oracle.simulate(spec, trajectories=True)
+    for c in (3, 6, 9):
+        name = f"Simulation_{c}"
+        f = tmp_path / "singles" / (f"{name}.json" if extra_files else "one.json")
+        single = json.loads(f.read_text())[name]
+        res = np.array(single["Results"], dtype=float)
+        assert np.max(np.abs(res - ref["trajectories"][c - 1])) < 1e-9
+        moment = spec.saturation_magnetisation[c - 1] * 4.0 / 3.0 * math.pi * spec.magnetic_radius[c - 1] ** 3
+        np.testing.assert_allclose(single["Weight"], [moment] * 3, rtol=1e-14)
+        np.testing.assert_array_equal(np.array(single["Time"], dtype=float), np.array(rec["Mean_Results"]["Time"]))
+        assert single["UsedProperties"]["Magnetic_radius"] == spec.magnetic_radius[c - 1]
+    if extra_files:
+        assert sorted(p.name for p in (tmp_path / "singles").iterdir()) == [
+            "Simulation_3.json", "Simulation_6.json", "Simulation_9.json"]
+
+
+def test_strided_trajectories_equal_the_selected_particles(tmp_path):
+    """record_trajectories = s keeps every s-th particle's window means only."""
+    from stochasticphysics_b200 import provider
+    spec = dataclasses.replace(provider.neel_relaxation(n=100, steps=2000, oversampling=100), record_trajectories=7)
+    with sp.Context(0) as ctx:
+        strided = ctx.simulate(spec, trajectories=True)
+        full = ctx.simulate(dataclasses.replace(spec, record_trajectories=1), trajectories=True)
+    assert strided.trajectories.shape == (14, spec.n_samples, 3)
+    np.testing.assert_array_equal(strided.trajectories, full.trajectories[6::7])
+    np.testing.assert_array_equal(strided.mean, full.mean)

@@ -4,9 +4,12 @@ Bars (stated per test):
   injection mode (same Wiener increments on both sides), FP64:
       per-trajectory window means within 1e-9 relative (floor 1e-3 absolute scale),
       ensemble mean within 1e-10 absolute (the mean magnetisation is O(1)).
-      Where the dynamics amplify round-off (particles crossing saddles, e.g. cubic
-      anisotropy at ~1 kT barriers) the FP64 oracle itself drifts from its own
-      long-double run; there the bar is 20x that double-vs-long-double spread.
+      Strict: every (problem, solver, anisotropy) over 1000 integrated steps on the
+      particles whose oracle agrees with its own long-double run to 1e-11.
+      Whole ensembles: where the dynamics amplify round-off (particles crossing saddles,
+      e.g. cubic anisotropy at ~1 kT barriers) the FP64 oracle itself drifts from its
+      long-double run; there the bar is 20x that spread, over the longest horizon on
+      which it stays at or below 1e-7 (asserted; the bar and horizon are printed).
   in-kernel Philox, FP64: the same 32-bit Philox words as the oracle; normals
       within 1e-14 relative, trajectories within 1e-9
   FP32 form: ensemble mean within 1e-3 of the FP64 kernel on the same noise
@@ -81,14 +84,63 @@ def compare(gpu, ref, rel=REL_TRAJ, mean_abs=ABS_MEAN):
     return t_err, m_err
 
 
-def conditioned_bars(spec, ref):
-    """1e-9 / 1e-10, or 20x the oracle's own double-vs-long-double spread when that is larger."""
+RELAX_CAP = 1e-7    # the largest relaxed per-trajectory bar any whole-ensemble test may apply
+LD_STRICT = 1e-11   # oracle double-vs-long-double spread of the particles of the strict tests
+MIN_WINDOWS = 5     # a relaxed comparison covers at least the initial state and 4 windows
+
+
+def ld_spread(spec, ref):
+    """Per-particle, per-window relative spread of the oracle's double run against its own
+    long-double run (inf where either is non-finite), shape [n][windows]."""
     ld = oracle.simulate(spec, trajectories=True, long_double=True)
-    ok = np.isfinite(ref["trajectories"]).all(axis=(1, 2)) & np.isfinite(ld["trajectories"]).all(axis=(1, 2))
-    e_ld = np.max(np.abs(ref["trajectories"][ok] - ld["trajectories"][ok]) /
-                  np.maximum(np.abs(ld["trajectories"][ok]), 1e-3)) if ok.any() else 0.0
-    m_ld = np.max(np.abs(ref["mean"] - ld["mean"])) if ok.all() else 0.0
-    return max(REL_TRAJ, 20 * e_ld), max(ABS_MEAN, 20 * m_ld)
+    t, tl = ref["trajectories"], ld["trajectories"]
+    with np.errstate(invalid="ignore"):
+        e = np.max(np.abs(t - tl) / np.maximum(np.abs(tl), 1e-3), axis=2)
+    e[~(np.isfinite(t).all(axis=2) & np.isfinite(tl).all(axis=2))] = np.inf
+    return e, ld
+
+
+def conditioned_bars(spec, ref, label=""):
+    """Bars and horizon of a whole-ensemble comparison: the strict 1e-9 / 1e-10, or 20x the
+    oracle's own double-vs-long-double spread when that is larger, over the longest run of
+    windows on which the relaxed per-trajectory bar stays at or below RELAX_CAP.  Returns
+    (trajectory bar, mean bar, windows)."""
+    e, ld = ld_spread(spec, ref)
+    per_window = np.max(e, axis=0)
+    cum = np.maximum.accumulate(per_window)
+    k = int(np.searchsorted(cum, RELAX_CAP / 20, side="right"))
+    assert k >= MIN_WINDOWS, f"{label}: the oracle is ill-conditioned from window {k} on (spread {cum[k]:.1e})"
+    rel = max(REL_TRAJ, 20 * float(cum[k - 1]))
+    m_ld = float(np.max(np.abs(ref["mean"][:k] - ld["mean"][:k])))
+    mabs = max(ABS_MEAN, 20 * m_ld)
+    assert rel <= RELAX_CAP and mabs <= RELAX_CAP
+    print(f"{label}: bars {rel:.1e} / {mabs:.1e} over {k} of {len(cum)} windows")
+    return rel, mabs, k
+
+
+def first_windows(res, k):
+    """The first k windows of a GPU result or an oracle record (later windows cannot change them)."""
+    if isinstance(res, dict):
+        return {**res, "trajectories": res["trajectories"][:, :k], "mean": res["mean"][:k],
+                "time": res["time"][:k], "field": res["field"][:k]}
+    return dataclasses.replace(res, trajectories=res.trajectories[:, :k], mean=res.mean[:k], time=res.time[:k],
+                               field=res.field[:k])
+
+
+def select_particles(spec, idx):
+    """The particles idx (with their injected increments) as an ensemble of their own."""
+    idx = np.asarray(idx)
+    kw = {}
+    for name in ("magnetic_radius", "saturation_magnetisation", "damping_constant", "gyromagnetic_ratio",
+                 "anisotropy_constant", "hydrodynamic_radius", "viscosity", "cubic_constant"):
+        v = getattr(spec, name)
+        kw[name] = None if v is None else np.asarray(v)[idx]
+    for name in ("orientation", "magnetisation", "uniaxial_rotation"):
+        v = getattr(spec, name)
+        kw[name] = None if v is None else np.asarray(v).reshape(-1, 3)[idx]
+    m = spec.dims[1]
+    kw["injected_dw"] = np.ascontiguousarray(np.asarray(spec.injected_dw).reshape(-1, m, spec.n)[:, :, idx])
+    return dataclasses.replace(spec, n=len(idx), **kw)
 
 
 @pytest.mark.parametrize("problem,solver", [(Problem.Neel, Solver.Heun_Strong), (Problem.Neel, Solver.EulerMaruyama),
@@ -113,9 +165,9 @@ CASES += [(Problem.Neel, Solver.Implicit_Midpoint, Anisotropy.Uniaxial),
           (Problem.BrownAndNeel, Solver.Implicit_Midpoint, Anisotropy.Uniaxial)]
 
 
-@pytest.mark.parametrize("problem,solver,aniso", CASES,
-                         ids=[f"{p.name}-{s.name}-{a.name}" for p, s, a in CASES])
-def test_injection_parity_fp64(ctx, problem, solver, aniso):
+def injection_case(problem, solver, aniso, steps=1050, W=50):
+    """The injection-mode ensemble of one (problem, solver, anisotropy): 67 particles,
+    (steps / W - 1) W integrated steps (1000 by default)."""
     kw = {}
     if problem == Problem.BrownAndNeel and solver == Solver.EulerMaruyama:
         # EM without renormalisation amplifies the precession by sqrt(1 + (w dt)^2) per step;
@@ -125,13 +177,50 @@ def test_injection_parity_fp64(ctx, problem, solver, aniso):
         # with the coordinate rotation on, finish() returns phi in (-pi, pi] and the Newton
         # residual jumps by 2 pi: the reference formulation is only usable without rotation
         kw["use_coordinate_transformation"] = False
-    spec = provider.with_injected_noise(small_spec(problem, solver, aniso, **kw), seed=3)
+    spec = small_spec(problem, solver, aniso, steps=steps, W=W, **kw)
+    if problem == Problem.NeelSpherical and solver == Solver.Implicit_Midpoint:
+        # without the rotation, 1/sin(theta) near a pole leaves Newton unconverged and the
+        # oracle's double and long-double runs part within the first window: keep the easy
+        # axes (and the moments along them) within 60 degrees of the equator
+        e = np.array(spec.orientation, copy=True)
+        e[:, 1] = np.arccos(np.random.default_rng(4).uniform(-0.5, 0.5, spec.n))
+        sign = np.sign(np.sum(np.asarray(spec.magnetisation) * provider.easy_axis(problem, spec.orientation), axis=1))
+        spec = dataclasses.replace(spec, orientation=e, magnetisation=provider.easy_axis(problem, e) * sign[:, None])
+    spec = provider.with_injected_noise(spec, seed=3)
     if solver == Solver.Implicit_Midpoint:
         spec = dataclasses.replace(spec, max_iteration=20, accuracy_goal=1e-10)
+    return spec
+
+
+CASE_IDS = [f"{p.name}-{s.name}-{a.name}" for p, s, a in CASES]
+
+
+@pytest.mark.parametrize("problem,solver,aniso", CASES, ids=CASE_IDS)
+def test_injection_parity_fp64_strict(ctx, problem, solver, aniso):
+    """The strict bars, 1e-9 per trajectory and 1e-10 on the ensemble mean, over 1000
+    integrated steps for every case: on the particles (at least 16) whose oracle run agrees
+    with its own long-double run to LD_STRICT in every window."""
+    spec = injection_case(problem, solver, aniso)
+    assert spec.integrated_steps >= 1000
+    e, _ = ld_spread(spec, oracle.simulate(spec, trajectories=True))
+    good = np.where(np.max(e, axis=1) <= LD_STRICT)[0]
+    assert len(good) >= 16, f"only {len(good)} well-conditioned particles"
+    sub = select_particles(spec, good)
+    gpu = ctx.simulate(sub, trajectories=True, final_state=True)
+    ref = oracle.simulate(sub, trajectories=True, final_state=True)
+    t_err, m_err = compare(gpu, ref)
+    print(f"strict on {len(good)} of {spec.n} particles: trajectory {t_err:.1e}, mean {m_err:.1e}")
+    assert gpu.stats["nonfinite_particles"] == 0
+
+
+@pytest.mark.parametrize("problem,solver,aniso", CASES, ids=CASE_IDS)
+def test_injection_parity_fp64(ctx, problem, solver, aniso):
+    """The whole ensemble of every case, with the conditioned bars (at most RELAX_CAP)."""
+    spec = injection_case(problem, solver, aniso)
     gpu = ctx.simulate(spec, trajectories=True, final_state=True)
     ref = oracle.simulate(spec, trajectories=True, final_state=True)
-    rel, mabs = conditioned_bars(spec, ref)
-    compare(gpu, ref, rel=rel, mean_abs=mabs)
+    rel, mabs, k = conditioned_bars(spec, ref, f"{problem.name}-{solver.name}-{aniso.name}")
+    compare(first_windows(gpu, k), first_windows(ref, k), rel=rel, mean_abs=mabs)
     assert gpu.stats["nonfinite_particles"] == 0
     if solver == Solver.Implicit_Midpoint:
         assert gpu.stats["newton_iterations"] > 0
@@ -147,8 +236,8 @@ def test_exact_jacobian_parity_fp64(ctx, aniso):
     spec = dataclasses.replace(spec, max_iteration=20, accuracy_goal=1e-10, jacobian=Jacobian.Exact)
     gpu = ctx.simulate(spec, trajectories=True, final_state=True)
     ref = oracle.simulate(spec, trajectories=True, final_state=True)
-    rel, mabs = conditioned_bars(spec, ref)
-    compare(gpu, ref, rel=rel, mean_abs=mabs)
+    rel, mabs, k = conditioned_bars(spec, ref, f"exact-{aniso.name}")
+    compare(first_windows(gpu, k), first_windows(ref, k), rel=rel, mean_abs=mabs)
     assert gpu.stats["newton_unconverged"] == 0 and ref["newton_unconverged"] == 0
     assert abs(gpu.stats["newton_iterations"] - ref["newton_iterations"]) <= 0.01 * ref["newton_iterations"] + 5
     assert gpu.stats["newton_iterations"] <= 4.1 * spec.n * spec.integrated_steps
@@ -189,8 +278,10 @@ def test_field_waveform_parity(ctx, name):
     spec = provider.with_injected_noise(spec, seed=4)
     gpu = ctx.simulate(spec, trajectories=True)
     ref = oracle.simulate(spec, trajectories=True)
-    rel, mabs = conditioned_bars(spec, ref)
-    compare(gpu, ref, rel=rel, mean_abs=mabs)
+    rel, mabs, k = conditioned_bars(spec, ref, name)
+    compare(first_windows(gpu, k), first_windows(ref, k), rel=rel, mean_abs=mabs)
+    # the field table is independent of the dynamics: all windows at the field bar
+    np.testing.assert_allclose(gpu.field, ref["field"], rtol=1e-12, atol=1e-16)
     assert np.ptp(ref["field"][1:], axis=0).max() > 1e-3  # the waveform actually varies
 
 
@@ -202,8 +293,8 @@ def test_euler_maruyama_normalized_parity(ctx, problem):
     spec = provider.with_injected_noise(small_spec(problem, Solver.EulerMaruyama_Normalized), seed=3)
     gpu = ctx.simulate(spec, trajectories=True, final_state=True)
     ref = oracle.simulate(spec, trajectories=True, final_state=True)
-    rel, mabs = conditioned_bars(spec, ref)
-    compare(gpu, ref, rel=rel, mean_abs=mabs)
+    rel, mabs, k = conditioned_bars(spec, ref, f"normalized-{problem.name}")
+    compare(first_windows(gpu, k), first_windows(ref, k), rel=rel, mean_abs=mabs)
     assert gpu.stats["nonfinite_particles"] == 0
     if problem != Problem.NeelSpherical:
         fs = gpu.final_state.reshape(spec.n, -1, 3)
@@ -228,11 +319,14 @@ def test_uniaxial_cubic_parity(ctx, problem, solver):
     spec = provider.with_injected_noise(spec, seed=3)
     gpu = ctx.simulate(spec, trajectories=True)
     ref = oracle.simulate(spec, trajectories=True)
-    rel, mabs = conditioned_bars(spec, ref)
-    compare(gpu, ref, rel=rel, mean_abs=mabs)
+    label = f"uniaxial-cubic-{problem.name}-{solver.name}"
+    rel, mabs, k = conditioned_bars(spec, ref, label)
+    compare(first_windows(gpu, k), first_windows(ref, k), rel=rel, mean_abs=mabs)
     if solver == Solver.Implicit_Midpoint:
         ex = dataclasses.replace(spec, jacobian=Jacobian.Exact)
-        compare(ctx.simulate(ex, trajectories=True), oracle.simulate(ex, trajectories=True), rel=rel, mean_abs=mabs)
+        rex = oracle.simulate(ex, trajectories=True)
+        rel, mabs, k = conditioned_bars(ex, rex, label + "-exact")
+        compare(first_windows(ctx.simulate(ex, trajectories=True), k), first_windows(rex, k), rel=rel, mean_abs=mabs)
 
 
 def test_runaway_particles_match(ctx):
