@@ -427,6 +427,88 @@ def sizes_leg(ctx, torch, sizes=(16384, 65536, 262144, 1048576)):
     return {"unit": UNIT, "rows": rows}
 
 
+def fp32_accuracy(ctx, shards=16, n_shard=65536, steps=101000, oversampling=1000):
+    """FP32 form against the plain FP64 kernel on the headline workload's particle model
+    (Brown+Neel Euler/spherical, Milstein and Heun, the same Philox increments), on an
+    ensemble of shards x n_shard particles large enough for the comparison's standard error
+    to sit well below 1e-3.  Each shard keeps its global particle ids; the shards of one
+    precision are submitted together to the server and merged with sp_merge_shards
+    (MeanSimulationResult::operator+=).  Relative error: |M32 - M64| of the moment-weighted
+    mean magnetisation (outputs 7-9), whose saturation value is 1 (|m| = 1 per particle), per
+    window and component.  Its standard error comes from the spread of the per-shard
+    differences (batch means over `shards` independent shards)."""
+    import numpy as np
+
+    import stochasticphysics_b200 as sp
+    from stochasticphysics_b200 import merge_shards, provider
+    from stochasticphysics_b200._abi import Precision, Solver
+
+    out = {}
+    for solver in (Solver.Millstein, Solver.Heun_Strong):
+        whole = provider.brown_neel_relaxation(n=shards * n_shard, steps=steps, oversampling=oversampling,
+                                               solver=solver)
+        parts = [whole.subset(i * n_shard, (i + 1) * n_shard) for i in range(shards)]
+        res = {}
+        for prec in (Precision.FP64, Precision.FP32):
+            specs = [dataclasses.replace(s, precision=prec) for s in parts]
+            with sp.Server(ctx) as srv:
+                ids = srv.submit_many(specs)
+                res[prec] = [srv.wait(i)[0] for i in ids]
+        merged = {prec: merge_shards([r.weighted_sum for r in rs], [r.weight for r in rs])[0]
+                  for prec, rs in res.items()}
+        d = (merged[Precision.FP32] - merged[Precision.FP64])[1:, 6:9]  # windows k >= 1, magnetisation
+        per_shard = np.stack([(a.mean - b.mean)[1:, 6:9] for a, b in zip(res[Precision.FP32], res[Precision.FP64])])
+        wts = np.array([r.weight[6] for r in res[Precision.FP64]])
+        wts = wts / wts.sum()
+        # weighted batch-means standard error of the merged difference
+        dev = per_shard - np.tensordot(wts, per_shard, axes=1)[None]
+        se = np.sqrt(np.tensordot(wts ** 2, dev ** 2, axes=1) * shards / (shards - 1))
+        bias = d.mean(axis=0)  # signed difference averaged over the windows, per component
+        bias_se = np.sqrt(np.tensordot(wts ** 2, (per_shard.mean(axis=1) - bias[None]) ** 2, axes=1)
+                          * shards / (shards - 1))
+        amp = float(np.abs(merged[Precision.FP64][1:, 6:9]).max())
+        out[solver.name] = {
+            "max_rel_error": float(np.abs(d).max()), "mean_rel_error": float(np.abs(d).mean()),
+            "first_window_rel_error": float(np.abs(d[0]).max()),
+            "max_se": float(se.max()), "mean_se": float(se.mean()), "max_z": float((np.abs(d) / se).max()),
+            "window_mean_bias": [float(x) for x in bias], "window_mean_bias_se": [float(x) for x in bias_se],
+            "max_abs_mean_m_fp64": amp, "max_error_over_response": float(np.abs(d).max()) / amp}
+    out["workload"] = (f"brown_neel_relaxation, {shards} shards x {n_shard} particles = {shards * n_shard}, "
+                       f"{(steps // oversampling - 1) * oversampling} integrated steps ({steps // oversampling - 1} "
+                       f"windows of {oversampling}), same Philox stream in both precisions")
+    out["definition"] = ("relative error = |M32 - M64| of the moment-weighted mean magnetisation per window and "
+                         "component (saturation value 1); se = batch-means standard error over the shards")
+    return out
+
+
+def merged_shards_check(ctx, torch, dist, world, rank, steps=3000):
+    """Multi-GPU: every rank runs its shard (global particle ids) of one verification
+    ensemble of world x N_PER_GPU particles, the shards' FP64 window sums and weights are
+    all-gathered over NCCL (the path's only exchange) and rank 0 merges them with
+    sp_merge_shards and compares the merged mean with its own run of the whole union."""
+    import numpy as np
+
+    from stochasticphysics_b200 import merge_shards, provider
+    from stochasticphysics_b200._abi import Precision
+
+    whole = provider.brown_neel_relaxation(n=N_PER_GPU * world, steps=steps, oversampling=1000,
+                                           precision=Precision.FP64)
+    r = ctx.simulate(whole.subset(N_PER_GPU * rank, N_PER_GPU * (rank + 1)))
+    k, od = r.weighted_sum.shape
+    mine = torch.from_numpy(np.concatenate([r.weighted_sum.ravel(), r.weight])).cuda()
+    parts = [torch.empty_like(mine) for _ in range(world)]
+    dist.all_gather(parts, mine)
+    if rank != 0:
+        return None
+    host = [q.cpu().numpy() for q in parts]
+    mean, _, weight = merge_shards([h[:k * od].reshape(k, od) for h in host], [h[k * od:] for h in host])
+    ref = ctx.simulate(whole)
+    return {"ranks": world, "particles": whole.n, "integrated_steps": whole.integrated_steps,
+            "max_abs_diff_vs_whole": float(np.abs(mean - ref.mean).max()),
+            "weight_rel_diff": float(np.abs(weight / ref.weight - 1).max()),
+            "exchange_bytes_per_rank": int(mine.numel() * 8)}
+
+
 def cpu_baseline(steps_sample=2000, n=None):
     """The CPU oracle on all host cores for a bounded sample of the workload."""
     import oracle
@@ -546,6 +628,9 @@ def main():
     ap.add_argument("--no-sizes", action="store_true", help="skip the ensemble-size sweep")
     ap.add_argument("--batched-step-scale", type=float, default=0.02,
                     help="scale of the batched sets' step counts (S ~ logU[1e5, 1e7] x scale)")
+    ap.add_argument("--accuracy-shards", type=int, default=16,
+                    help="65536-particle shards of the FP32-vs-FP64 accuracy leg (0: skip)")
+    ap.add_argument("--accuracy-steps", type=int, default=101000, help="steps of the accuracy leg")
     args = ap.parse_args()
     globals()["N_PER_GPU"], globals()["CHUNK"] = args.n_particles, args.chunk
     args.warmup = max(args.warmup, 3)
@@ -637,7 +722,7 @@ def main():
         e2e_specs.sort(key=lambda s: ctx.launch_config(s)["particle_steps_per_s"])
         for s in e2e_specs:
             ctx.simulate(s)  # warm the path
-        e2e_times, seq_times = [], []
+        e2e_times, seq_times, phases = [], [], []
         with sp.Server(ctx) as srv:
             ids = srv.submit_many(e2e_specs)
             for i in ids:
@@ -649,6 +734,7 @@ def main():
                 ids = srv.submit_many(e2e_specs)
                 outs = [srv.wait(i)[0] for i in ids]
                 e2e_times.append(time.perf_counter() - t)
+                phases.append([[o.stats[k] for k in ("queue_ms", "setup_ms", "run_ms", "readback_ms")] for o in outs])
         for _ in range(args.steps):
             if world > 1:
                 dist.barrier()
@@ -659,12 +745,22 @@ def main():
         e2e_value = world * ps_per_step * args.steps / barrier_max(sum(e2e_times))
         e2e_simulate_value = world * ps_per_step * args.steps / barrier_max(sum(seq_times))
         h2d = sum(s.n * 13 * 8 for s in e2e_specs)
+        ph = np.array(phases)  # [steps][requests][phase]
+        e2e_breakdown = {
+            "step_ms": 1e3 * statistics.mean(e2e_times),
+            "per_request_ms": {name: [float(x) for x in ph[:, :, j].mean(axis=0)]
+                               for j, name in enumerate(("queue", "setup", "run", "readback"))},
+            "note": "server host clock per request (submit -> admission -> set-up -> rounds -> read-back); "
+                    "requests in submission order"}
         d2h = sum(o.mean.nbytes + o.weight.nbytes + o.time.nbytes + o.field.nbytes for o in outs)
         serving = batched = None
         if world == 1 and args.serving_seconds > 0:
             serving = serving_leg(ctx, args.serving_seconds, args.serving_rate, args.serving_step_scale)
         if world == 1 and args.batched_sets > 0:
             batched = batched_leg(ctx, args.batched_sets, args.batched_step_scale)
+        accuracy = None if (world > 1 or args.accuracy_shards <= 0) else fp32_accuracy(
+            ctx, shards=args.accuracy_shards, steps=args.accuracy_steps)
+        merged = merged_shards_check(ctx, torch, dist, world, rank) if world > 1 else None
         stiff = None if (world > 1 or args.no_stiff) else stiff_leg(ctx, torch)
         injected = None if (world > 1 or args.no_injected) else injected_leg(ctx, torch)
         sizes = None if (world > 1 or args.no_sizes) else sizes_leg(ctx, torch)
@@ -705,11 +801,13 @@ def main():
             "sequential_ensembles": {"fp32": world * ps_per_step * args.steps / (results["FP32"]["seq_ms"] / 1e3),
                                      "fp64": world * ps_per_step * args.steps / (results["FP64"]["seq_ms"] / 1e3)},
             "fp32_vs_fp64_mean_m": {
-                "max_abs_diff": float(max(d.max() for d in diffs)),
-                "first_window_abs_diff": float(max(d[0].max() for d in diffs)),
-                "two_sample_se": se_indep,
-                "note": "same Philox noise; paths decorrelate by chaos, FP64 with float-rounded noise "
-                        "diverges from itself equally fast; max_abs_diff is bounded by the two-sample SE"},
+                "ensemble": accuracy,
+                "bench_run_65536": {"max_abs_diff": float(max(d.max() for d in diffs)),
+                                    "first_window_abs_diff": float(max(d[0].max() for d in diffs)),
+                                    "two_sample_se": se_indep,
+                                    "note": "the timed 65536-particle ensembles themselves: their difference "
+                                            "after the first windows is Monte-Carlo, of the order of the SE"}},
+            "merged_shards": merged,
             "nonfinite_particles": {"fp32": results["FP32"]["nonfinite"], "fp64": results["FP64"]["nonfinite"]},
             "roofline": {"bound": "fp32-fma", "achieved": sum(ach) / 2, "peak": peak32, "unit": "TFLOP/s",
                          "frac": (sum(ach) / 2) / peak32,
@@ -722,6 +820,7 @@ def main():
                          "issue": issue},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "api": "sp_server_submit_many / sp_server_wait, the two ensembles in flight together",
+                    "breakdown": e2e_breakdown,
                     "sp_simulate_one_after_the_other": e2e_simulate_value},
             "gpu_launches": results["FP32"]["launches"],
             "clocks": c32,

@@ -293,6 +293,10 @@ typedef struct sp_stats {
     uint64_t newton_unconverged;  /* ImplicitMidpoint: steps that hit Max_Iterations */
     uint64_t kernel_launches;     /* device kernels launched for this ensemble       */
     double device_ms;             /* device time of the stepping kernels             */
+    /* host-clock phases of the call or request, ms: waiting for admission (server only),
+       set-up (device buffers, particle upload, initial state), integration (first launch
+       to the last chunk complete) and read-back of the results */
+    double queue_ms, setup_ms, run_ms, readback_ms;
 } sp_stats;
 
 typedef struct sp_context sp_context;

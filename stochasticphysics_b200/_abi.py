@@ -215,6 +215,10 @@ class sp_stats(C.Structure):
         ("newton_unconverged", C.c_uint64),
         ("kernel_launches", C.c_uint64),
         ("device_ms", C.c_double),
+        ("queue_ms", C.c_double),
+        ("setup_ms", C.c_double),
+        ("run_ms", C.c_double),
+        ("readback_ms", C.c_double),
     ]
 
 

@@ -5,6 +5,7 @@
 // thread-local text returned by sp_last_error().
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cmath>
 #include <limits>
 #include <cstdio>
@@ -723,9 +724,22 @@ sp_status sp_simulate(sp_context* ctx, const sp_ensemble_desc* desc, sp_result* 
     if (s != SP_OK) return fail(s, why);
     sp_ensemble_desc d = *desc;
     if (out && out->trajectories && d.record_trajectories == 0) d.record_trajectories = 1;
+    using Clock = std::chrono::steady_clock;
+    const auto ms = [](Clock::time_point a, Clock::time_point b) {
+        return std::chrono::duration<double, std::milli>(b - a).count();
+    };
+    const Clock::time_point t0 = Clock::now();
     Ensemble e(ctx, d, launch_config_for(ctx, d));
+    const Clock::time_point t1 = Clock::now();
     e.advance(e.L.S, nullptr);
+    e.synchronize();
+    const Clock::time_point t2 = Clock::now();
     e.read(out, stats);
+    if (stats) {
+        stats->setup_ms = ms(t0, t1);
+        stats->run_ms = ms(t1, t2);
+        stats->readback_ms = ms(t2, Clock::now());
+    }
     return SP_OK;
     SP_GUARD_END
 }

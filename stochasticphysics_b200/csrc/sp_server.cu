@@ -50,7 +50,7 @@ struct Request {
     uint64_t bytes = 0;
     unsigned long long chunks_per_round = 1;
     bool in_round = false;  // launched in the current round (not admitted during it)
-    Clock::time_point t_submit, t_done;
+    Clock::time_point t_submit, t_admit0, t_admit1, t_run_end, t_done;
     std::vector<double> mean, weight, time, field, weighted_sum;
     sp_stats stats{};
 };
@@ -149,6 +149,14 @@ struct sp_server {
             out.field = r->field.data();
             r->ens->read(&out, &r->stats);
             r->ens.reset();
+            const auto ms = [](Clock::time_point a, Clock::time_point b) {
+                return std::chrono::duration<double, std::milli>(b - a).count();
+            };
+            const Clock::time_point now = Clock::now();
+            r->stats.queue_ms = ms(r->t_submit, r->t_admit0);
+            r->stats.setup_ms = ms(r->t_admit0, r->t_admit1);
+            r->stats.run_ms = ms(r->t_admit1, r->t_run_end);
+            r->stats.readback_ms = ms(r->t_run_end, now);
         }
     }
 
@@ -165,7 +173,9 @@ struct sp_server {
             if (used_bytes + r->bytes > budget) break;
             queue.pop_front();
             try {
+                r->t_admit0 = Clock::now();
                 r->ens = std::make_unique<Ensemble>(ctx, r->desc, launch_for(r->desc, &r->chunks_per_round));
+                r->t_admit1 = Clock::now();
                 r->ens->last_stream = nullptr;
                 // the ensemble holds its inputs on the device now: drop the host copies
                 std::vector<double>().swap(r->arrays);
@@ -312,6 +322,7 @@ struct sp_server {
                 e->launches += 5 * nl;
                 const bool done = e->steps_done >= e->L.S;
                 if (done || r->cancel) {
+                    r->t_run_end = Clock::now();
                     try {
                         if (done) retire(r);
                         else r->ens.reset();

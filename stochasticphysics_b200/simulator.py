@@ -36,7 +36,8 @@ class SimulationResult:
 def _stats_dict(st: sp_stats) -> dict:
     return {"particle_steps": st.particle_steps, "nonfinite_particles": st.nonfinite_particles,
             "newton_iterations": st.newton_iterations, "newton_unconverged": st.newton_unconverged,
-            "kernel_launches": st.kernel_launches, "device_ms": st.device_ms}
+            "kernel_launches": st.kernel_launches, "device_ms": st.device_ms, "queue_ms": st.queue_ms,
+            "setup_ms": st.setup_ms, "run_ms": st.run_ms, "readback_ms": st.readback_ms}
 
 
 def _result(buf: ResultBuffers, st: sp_stats) -> SimulationResult:
