@@ -230,6 +230,83 @@ def serving_leg(ctx, seconds, rate, step_scale, seed=0x5EED0005, serial_sample=4
     }
 
 
+def overload_leg(ctx, arrival_s=2.0, observe_s=30.0, rate=50.0, seed=0x5EED0005):
+    """The serving workload at its stated size: Poisson arrivals at `rate`/s for `arrival_s`
+    seconds of full-length requests (N ~ logU[1e3, 6.4e4], S ~ logU[1e5, 1e7], Neel or
+    BrownAndNeelEulerSpherical, Lissajous field, FP32).  The offered load, about 50 x 1.5e4 x
+    2.15e6 = 1.6e12 particle-steps/s, is some 30x what one B200 integrates, so the server
+    saturates: reported are the particle-steps it completes per second over a fixed
+    observation window, the requests in flight (admitted or queued) sampled every 0.5 s, and
+    the latencies of the requests that finish inside the window; the rest are cancelled."""
+    import numpy as np
+
+    import stochasticphysics_b200 as sp
+    from stochasticphysics_b200 import provider
+    from stochasticphysics_b200._abi import Precision, Problem, RequestState
+
+    rng = np.random.default_rng(seed)
+    arrivals, t = [], 0.0
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t > arrival_s:
+            break
+        arrivals.append(t)
+    specs = provider.batched_sets(count=len(arrivals), seed=seed, precision=Precision.FP32, step_scale=1.0,
+                                  lissajous=True, problems=(Problem.Neel, Problem.BrownAndNeelEulerSpherical))
+    work = [s.n * s.integrated_steps for s in specs]
+    free, _ = __import__("torch").cuda.mem_get_info()
+    budget = int(min(150e9, 0.8 * free))
+    ids = [None] * len(specs)
+    depth, done, lat = [], {}, []
+    with sp.Server(ctx, memory_budget_bytes=budget) as srv:
+        t0 = time.perf_counter()
+        nxt = 0
+        next_sample = 0.0
+        while True:
+            now = time.perf_counter() - t0
+            while nxt < len(specs) and arrivals[nxt] <= now:
+                ids[nxt] = srv.submit(specs[nxt])
+                nxt += 1
+            for i in range(nxt):
+                if i in done:
+                    continue
+                if srv.poll(ids[i]) == RequestState.DONE:
+                    _, ms = srv.wait(ids[i])
+                    done[i] = now
+                    lat.append(ms)
+            if now >= next_sample:
+                depth.append((round(now, 2), nxt - len(done)))
+                next_sample += 0.5
+            if now >= observe_s or (nxt == len(specs) and len(done) == len(specs)):
+                break
+            time.sleep(0.005)
+        t_end = time.perf_counter() - t0
+        # partial progress of the requests still running counts toward the throughput
+        in_flight = [i for i in range(nxt) if i not in done]
+        for i in in_flight:
+            srv.cancel(ids[i])
+        for i in in_flight:
+            try:
+                srv.wait(ids[i])
+            except sp.SPError:
+                pass
+    completed = sum(work[i] for i in done)
+    lat_s = sorted(lat)
+    return {"requests": len(specs), "arrival_rate_per_s": rate, "arrival_window_s": arrival_s,
+            "observe_window_s": observe_s, "wall_s": t_end,
+            "offered_particle_steps_per_s": sum(work) / arrival_s,
+            "completed_requests": len(done), "completed_particle_steps": completed,
+            "saturated_value": completed / t_end, "unit": UNIT,
+            "p50_ms_completed": float(np.percentile(lat_s, 50)) if lat_s else None,
+            "p99_ms_completed": float(np.percentile(lat_s, 99)) if lat_s else None,
+            "in_flight_over_time": depth, "memory_budget_bytes": budget,
+            "note": "completed_particle_steps counts finished requests only (the cancelled ones' partial "
+                    "work is not included), so saturated_value is a lower bound on the integration rate",
+            "workload": f"Poisson {rate}/s for {arrival_s} s, full-length requests (step_scale 1.0): "
+                        "N ~ logU[1e3, 6.4e4], S ~ logU[1e5, 1e7], Neel or BrownAndNeelEulerSpherical, "
+                        "Heun / Millstein, FP32, Lissajous 12 mT at 25.25 / 26.04 kHz, dt = 1e-11 s"}
+
+
 def batched_leg(ctx, count, step_scale, seed=0x5EED0004, serial_sample=32):
     """Parameter-set batch: `count` Neel ensembles with the batched-set distributions
     (N ~ logU[1e3, 6.4e4], S ~ logU[1e5, 1e7] x step_scale, Heun / Millstein
@@ -628,6 +705,8 @@ def main():
     ap.add_argument("--no-sizes", action="store_true", help="skip the ensemble-size sweep")
     ap.add_argument("--batched-step-scale", type=float, default=0.02,
                     help="scale of the batched sets' step counts (S ~ logU[1e5, 1e7] x scale)")
+    ap.add_argument("--overload-seconds", type=float, default=30.0,
+                    help="observation window of the full-size serving overload leg (0: skip)")
     ap.add_argument("--accuracy-shards", type=int, default=16,
                     help="65536-particle shards of the FP32-vs-FP64 accuracy leg (0: skip)")
     ap.add_argument("--accuracy-steps", type=int, default=101000, help="steps of the accuracy leg")
@@ -756,6 +835,9 @@ def main():
         serving = batched = None
         if world == 1 and args.serving_seconds > 0:
             serving = serving_leg(ctx, args.serving_seconds, args.serving_rate, args.serving_step_scale)
+        overload = None
+        if world == 1 and args.overload_seconds > 0:
+            overload = overload_leg(ctx, observe_s=args.overload_seconds, rate=args.serving_rate)
         if world == 1 and args.batched_sets > 0:
             batched = batched_leg(ctx, args.batched_sets, args.batched_step_scale)
         accuracy = None if (world > 1 or args.accuracy_shards <= 0) else fp32_accuracy(
@@ -828,6 +910,7 @@ def main():
             "launch_shapes": shapes,
             "co_scheduled_chunk_steps": CO_CHUNK,
             "serving": serving,
+            "serving_overload": overload,
             "batched": batched,
             "stiff": stiff,
             "injected": injected,

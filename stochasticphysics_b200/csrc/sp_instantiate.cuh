@@ -3,6 +3,7 @@
 
 #include "sp_dispatch.h"
 #include "sp_kernels.cuh"
+#include "sp_kernels_x2.cuh"
 
 namespace sp {
 
@@ -10,6 +11,14 @@ template <int PROB, class R, int A, int SOLVER, bool INJ, int PPT>
 void launch_step_t(const EnsDev* e, const TileDesc* t, int ntiles, int grid, int block, cudaStream_t s) {
     step_kernel<PROB, R, A, SOLVER, INJ, PPT><<<grid, block / PPT, 0, s>>>(e, t, ntiles);
 }
+template <int PROB, int A, int SOLVER>
+void launch_step_x2_t(const EnsDev* e, const TileDesc* t, int ntiles, int grid, int block, cudaStream_t s) {
+    step_kernel_x2<PROB, A, SOLVER><<<grid, block / 2, 0, s>>>(e, t, ntiles);
+}
+// the paired FP32 form (sp_kernels_x2.cuh): Brown+Neel Euler/spherical, explicit steppers
+template <int PROB, int SOLVER>
+constexpr bool kPairedStep = PROB == kBrownNeelEuler && (SOLVER == kEulerMaruyama || SOLVER == kHeun ||
+                                                         SOLVER == kMillstein || SOLVER == kEulerMaruyamaNormalized);
 template <int PROB, class R, int A>
 void launch_init_t(const EnsDev* e, const RawParticles& rp, unsigned long long Np, cudaStream_t s) {
     init_kernel<PROB, R, A><<<static_cast<unsigned>(Np / kPad), kPad, 0, s>>>(e, rp);
@@ -41,8 +50,13 @@ KernelSet make_set() {
         k.step[0] = &launch_step_t<PROB, R, A, SOLVER, INJ, 1>;
         k.step_fn[0] = reinterpret_cast<const void*>(&step_kernel<PROB, R, A, SOLVER, INJ, 1>);
         if constexpr (sizeof(R) == 4 && !INJ) {  // two particles per thread: FP32, in-kernel noise
-            k.step[1] = &launch_step_t<PROB, R, A, SOLVER, INJ, 2>;
-            k.step_fn[1] = reinterpret_cast<const void*>(&step_kernel<PROB, R, A, SOLVER, INJ, 2>);
+            if constexpr (kPairedStep<PROB, SOLVER>) {  // in paired f32x2 arithmetic
+                k.step[1] = &launch_step_x2_t<PROB, A, SOLVER>;
+                k.step_fn[1] = reinterpret_cast<const void*>(&step_kernel_x2<PROB, A, SOLVER>);
+            } else {  // two interleaved scalar chains
+                k.step[1] = &launch_step_t<PROB, R, A, SOLVER, INJ, 2>;
+                k.step_fn[1] = reinterpret_cast<const void*>(&step_kernel<PROB, R, A, SOLVER, INJ, 2>);
+            }
         }
         k.reduce = &launch_reduce_t<Prob::OUT>;
         k.field = &launch_field_chunk_t<R>;

@@ -39,6 +39,8 @@ static __device__ __noinline__ SinCosD box_muller_pair_d(uint32_t a, uint32_t b)
 }
 
 template <> struct M<double> {
+    // rare paths (chart rotations, the mixed-chart drift) are called, not inlined
+    static constexpr bool kColdCalls = true;
     static __device__ __forceinline__ double sin(double x) { return ::sin(x); }
     static __device__ __forceinline__ double cos(double x) { return ::cos(x); }
     static __device__ __forceinline__ void sincos(double x, double* s, double* c) {
@@ -55,12 +57,14 @@ template <> struct M<double> {
     static __device__ __forceinline__ double inv_sin(double x) { return 1.0 / x; }
     static __device__ __forceinline__ double abs(double x) { return ::fabs(x); }
     static __device__ __forceinline__ bool isinf(double x) { return ::isinf(x); }
+    static __device__ __forceinline__ double zero_inf(double x) { return ::isinf(x) ? 0.0 : x; }
     static __device__ __forceinline__ bool finite(double x) { return ::isfinite(x); }
     static constexpr double two_pi = 6.283185307179586;
     static constexpr double eps = 2.220446049250313e-16;
 };
 
 template <> struct M<float> {
+    static constexpr bool kColdCalls = false;
     static __device__ __forceinline__ float sin(float x) { return __sinf(x); }
     static __device__ __forceinline__ float cos(float x) { return __cosf(x); }
     static __device__ __forceinline__ void sincos(float x, float* s, float* c) { __sincosf(x, s, c); }
@@ -78,6 +82,7 @@ template <> struct M<float> {
     }
     static __device__ __forceinline__ float abs(float x) { return ::fabsf(x); }
     static __device__ __forceinline__ bool isinf(float x) { return ::isinf(x); }
+    static __device__ __forceinline__ float zero_inf(float x) { return ::isinf(x) ? 0.0f : x; }
     static __device__ __forceinline__ bool finite(float x) { return ::isfinite(x); }
     static constexpr float two_pi = 6.283185307179586f;
     static constexpr float eps = 1.1920929e-7f;
@@ -104,7 +109,14 @@ template <class R>
 struct V3 {
     R x, y, z;
 };
-template <class R> __device__ __forceinline__ V3<R> v3(R a, R b, R c) { return V3<R>{a, b, c}; }
+// the value type an argument expression stands for (the paired form's unevaluated
+// products name their result type here)
+template <class T> struct real_of { using type = T; };
+template <class A, class B, class C>
+__device__ __forceinline__ V3<typename real_of<A>::type> v3(A a, B b, C c) {
+    using R = typename real_of<A>::type;
+    return V3<R>{R(a), R(b), R(c)};
+}
 template <class R> __device__ __forceinline__ V3<R> operator+(V3<R> a, V3<R> b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
 template <class R> __device__ __forceinline__ V3<R> operator-(V3<R> a, V3<R> b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
 template <class R> __device__ __forceinline__ V3<R> operator*(R s, V3<R> a) { return {s * a.x, s * a.y, s * a.z}; }

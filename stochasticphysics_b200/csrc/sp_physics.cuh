@@ -57,7 +57,7 @@ template <class R, bool INV>
 __device__ __noinline__ SphRot<R> sph_rotate_cold(R t0, R p0) { return sph_rotate_impl<R, INV>(t0, p0); }
 template <class R, bool INV>
 __device__ __forceinline__ SphRot<R> sph_rotate(R t0, R p0) {
-    if constexpr (sizeof(R) == 8) return sph_rotate_cold<R, INV>(t0, p0);
+    if constexpr (M<R>::kColdCalls) return sph_rotate_cold<R, INV>(t0, p0);
     else return sph_rotate_impl<R, INV>(t0, p0);
 }
 template <class R>
@@ -86,7 +86,7 @@ template <class R, bool INV>
 __device__ __noinline__ EulerRot<R> euler_rotate_cold(R a0, R a1, R a2) { return euler_rotate_impl<R, INV>(a0, a1, a2); }
 template <class R, bool INV>
 __device__ __forceinline__ EulerRot<R> euler_rotate(R a0, R a1, R a2) {
-    if constexpr (sizeof(R) == 8) return euler_rotate_cold<R, INV>(a0, a1, a2);
+    if constexpr (M<R>::kColdCalls) return euler_rotate_cold<R, INV>(a0, a1, a2);
     else return euler_rotate_impl<R, INV>(a0, a1, a2);
 }
 
@@ -377,8 +377,7 @@ struct NeelSph {
     }
     static __device__ __forceinline__ void cache_from(const Par& q, R st, R ct, R sp, R cp, Cache& c) {
         c.st = st; c.ct = ct;
-        R odst = M<R>::inv_sin(st);
-        if (M<R>::isinf(odst)) odst = R(0);
+        const R odst = M<R>::zero_inf(M<R>::inv_sin(st));
         c.odst = odst;
         if (!c.rot) {
             c.md = v3(st * cp, st * sp, ct);
@@ -536,19 +535,24 @@ struct BrownNeelEuler {
         R csc, odst;
         V3<R> md;
     };
-    static __device__ __forceinline__ Par load(const R* P, unsigned long long Np, unsigned long long p) {
+    // get(i): prefactor i of the particle (one lane each in the paired form)
+    template <class G>
+    static __device__ __forceinline__ Par load_with(G get) {
         Par q;
-        q.a = P[0 * Np + p]; q.bpd = P[1 * Np + p]; q.d = P[2 * Np + p]; q.cT = P[3 * Np + p];
-        q.pF = P[4 * Np + p]; q.cF = P[5 * Np + p]; q.dDN = P[6 * Np + p]; q.bpdDN = P[7 * Np + p];
-        q.aDN = P[8 * Np + p]; q.adDN2 = P[9 * Np + p]; q.d2fDN2 = P[10 * Np + p]; q.cF2h = P[11 * Np + p];
-        q.nd = P[12 * Np + p];
+        q.a = get(0); q.bpd = get(1); q.d = get(2); q.cT = get(3);
+        q.pF = get(4); q.cF = get(5); q.dDN = get(6); q.bpdDN = get(7);
+        q.aDN = get(8); q.adDN2 = get(9); q.d2fDN2 = get(10); q.cF2h = get(11);
+        q.nd = get(12);
         if constexpr (A == kUniaxialCubic) {
-            q.pF2 = P[13 * Np + p];
-            q.cT2 = P[14 * Np + p];
+            q.pF2 = get(13);
+            q.cT2 = get(14);
 #pragma unroll
-            for (int i = 0; i < 9; ++i) q.Rm[i] = P[(15 + i) * Np + p];
+            for (int i = 0; i < 9; ++i) q.Rm[i] = get(15 + i);
         }
         return q;
+    }
+    static __device__ __forceinline__ Par load(const R* P, unsigned long long Np, unsigned long long p) {
+        return load_with([&](int i) { return P[i * Np + p]; });
     }
     // :859-899
     static __device__ __forceinline__ void euler_rotate(R* e) {
@@ -585,9 +589,14 @@ struct BrownNeelEuler {
 #pragma unroll
         for (int i = 0; i < 5; ++i) M<R>::sincos(y[i], &t.S[i], &t.C[i]);
     }
-    static __device__ __forceinline__ void prepare_t(const Par&, const Rot<R>& r, R* y, Cache& c, const Trig& t) {
-        const R tb = M<R>::abs(y[1]);
-        c.br = r.rb && (tb < r.min1 || tb > r.max1);
+    static __device__ __forceinline__ void prepare_t(const Par& q, const Rot<R>& r, R* y, Cache& c, const Trig& t) {
+        const R tb = M<R>::abs(y[1]), tn = M<R>::abs(y[3]);
+        prepare_flags(q, y, c, t, r.rb && (tb < r.min1 || tb > r.max1), r.rn && (tn < r.min2 || tn > r.max2));
+    }
+    // prepare_t with the charts given: br (Euler angles rotated), nr (Neel angles rotated);
+    // the paired FP32 form decides them per particle and runs both lanes in one chart pair
+    static __device__ __forceinline__ void prepare_flags(const Par&, R* y, Cache& c, const Trig& t, bool br, bool nr) {
+        c.br = br;
         if (c.br) {
             const EulerRot<R> n = sp::euler_rotate<R, false>(y[0], y[1], y[2]);
             y[0] = n.e0; y[1] = n.e1; y[2] = n.e2;
@@ -596,8 +605,7 @@ struct BrownNeelEuler {
 #pragma unroll
             for (int i = 0; i < 3; ++i) { c.S[i] = t.S[i]; c.C[i] = t.C[i]; }
         }
-        const R tn = M<R>::abs(y[3]);
-        c.nr = r.rn && (tn < r.min2 || tn > r.max2);
+        c.nr = nr;
         if (c.nr) {
             const SphRot<R> n = sph_rotate<R, false>(y[3], y[4]);
             y[3] = n.t; y[4] = n.p;
@@ -609,12 +617,8 @@ struct BrownNeelEuler {
         cache_from(c);
     }
     static __device__ __forceinline__ void cache_from(Cache& c) {
-        R csc = M<R>::inv_sin(c.S[1]);
-        if (M<R>::isinf(csc)) csc = R(0);
-        c.csc = csc;
-        R odst = M<R>::inv_sin(c.S[3]);
-        if (M<R>::isinf(odst)) odst = R(0);
-        c.odst = odst;
+        c.csc = M<R>::zero_inf(M<R>::inv_sin(c.S[1]));
+        c.odst = M<R>::zero_inf(M<R>::inv_sin(c.S[3]));
         const R ct = c.C[3], cp = c.C[4], st = c.S[3], sp = c.S[4];
         c.md = c.nr ? v3(-ct, st * sp, st * cp) : v3(st * cp, st * sp, ct);
     }
@@ -734,7 +738,7 @@ struct BrownNeelEuler {
                      q.d2fDN2 * sin_t * (R(2) * cos_t * cotb * cph + (R(-1) + R(2) * csc * csc) * sin_t * s2));
         } else {
             V3<R> m;
-            if constexpr (sizeof(R) == 8)
+            if constexpr (M<R>::kColdCalls)
                 m = be_drift_mixed_cold<R>(c.br, q.adDN2, q.d2fDN2, q.cF2h, csc, ctheta, cpsi, spsi, cos_t, cos_p, sin_t, sin_p);
             else
                 m = be_drift_mixed_impl<R>(c.br, q.adDN2, q.d2fDN2, q.cF2h, csc, ctheta, cpsi, spsi, cos_t, cos_p, sin_t, sin_p);
@@ -944,12 +948,14 @@ struct Stepper {
     using Cache = typename P::Cache;
     using Trig = typename P::Trig;
 
-    // tr: sines and cosines of y (from the previous step's output), reused by prepare_t
-    static __device__ __forceinline__ void step(const Par& q, const Rot<R>& rot, R* y, const R* B, const R* w, R dt,
-                                                int max_iter, double tol, NewtonCount& nc, const Trig& tr) {
+    static constexpr bool kExplicit = SOLVER == kEulerMaruyama || SOLVER == kHeun ||
+                                      SOLVER == kEulerMaruyamaNormalized || SOLVER == kMillstein;
+
+    // one explicit step from y already prepared into the chart c (by prepare_t, or in the
+    // paired FP32 form by prepare_flags); ends with finishCalculations
+    static __device__ __forceinline__ void explicit_from(const Par& q, const Rot<R>& rot, R* y, Cache& c, const R* B,
+                                                         const R* w, R dt) {
         if constexpr (SOLVER == kEulerMaruyama) {
-            Cache c;
-            P::prepare_t(q, rot, y, c, tr);
             R a[D], d[D], bw[D];
             P::det(q, y, c, B, a);
             P::drift(q, y, c, d);
@@ -958,8 +964,6 @@ struct Stepper {
             for (int i = 0; i < D; ++i) y[i] = y[i] + ((a[i] + d[i]) * dt + bw[i]);
             P::finish(rot, y, c);
         } else if constexpr (SOLVER == kHeun) {
-            Cache c;
-            P::prepare_t(q, rot, y, c, tr);
             R a1[D], d[D], bw[D], s[D];
             P::det(q, y, c, B, a1);
             P::drift(q, y, c, d);
@@ -977,8 +981,6 @@ struct Stepper {
             for (int i = 0; i < D; ++i) y[i] = (y[i] + (R(0.5) * ((a2[i] + d[i]) + a1[i])) * dt) + bw[i];
             P::finish(rot, y, c);
         } else if constexpr (SOLVER == kEulerMaruyamaNormalized) {
-            Cache c;
-            P::prepare_t(q, rot, y, c, tr);
             R a[D], d[D], bw[D];
             P::det(q, y, c, B, a);
             P::drift(q, y, c, d);
@@ -988,8 +990,6 @@ struct Stepper {
             P::finish(rot, y, c);
             P::normalize(y);
         } else if constexpr (SOLVER == kMillstein) {
-            Cache c;
-            P::prepare_t(q, rot, y, c, tr);
             R a[D], d[D], bw[D];
             P::det(q, y, c, B, a);
             P::drift(q, y, c, d);
@@ -1000,6 +1000,16 @@ struct Stepper {
 #pragma unroll
             for (int i = 0; i < D; ++i) y[i] = ((y[i] + a[i] * dt) + bw[i]) + d[i] * ww;
             P::finish(rot, y, c);
+        }
+    }
+
+    // tr: sines and cosines of y (from the previous step's output), reused by prepare_t
+    static __device__ __forceinline__ void step(const Par& q, const Rot<R>& rot, R* y, const R* B, const R* w, R dt,
+                                                int max_iter, double tol, NewtonCount& nc, const Trig& tr) {
+        if constexpr (kExplicit) {
+            Cache c;
+            P::prepare_t(q, rot, y, c, tr);
+            explicit_from(q, rot, y, c, B, w, dt);
         } else {
             if constexpr (P::kHasJacobian) {
                 // Newton on f(yj) = finish(prepare((yj+yn)/2) + a dt + b dW) + yn/2 - 3yj/2,
