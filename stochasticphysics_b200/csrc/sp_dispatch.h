@@ -17,6 +17,11 @@ struct KernelSet {
     void (*reduce)(const EnsDev* e, int n_ens, int max_slots, int mode, cudaStream_t s) = nullptr;
     void (*field)(const EnsDev* e, int n_ens, unsigned long long chunk, int midpoint, cudaStream_t s) = nullptr;
     const void* step_fn[2] = {nullptr, nullptr};  // for cudaFuncGetAttributes / occupancy queries
+    // dynamic shared memory of a step launch of `threads` threads (injected increments'
+    // staging; 0 for in-kernel noise), and the once-per-device opt-in it needs above the
+    // default limit: call prepare() with the device current before the first launch
+    size_t (*dyn_smem)(int threads) = nullptr;
+    void (*prepare)() = nullptr;
 };
 
 // index: problem, anisotropy, solver slot (see solver_slot),

@@ -1,15 +1,37 @@
 // sp_instantiate.cuh — builds the KernelSet entries of one problem.
 #pragma once
 
+#include <mutex>
+
 #include "sp_dispatch.h"
 #include "sp_kernels.cuh"
 #include "sp_kernels_x2.cuh"
 
 namespace sp {
 
+template <int PROB, class R, int A>
+size_t inj_smem_t(int threads) {
+    return DwStream<R, ProblemOf<PROB, R, A>::type::Mn>::smem_bytes(threads);
+}
 template <int PROB, class R, int A, int SOLVER, bool INJ, int PPT>
 void launch_step_t(const EnsDev* e, const TileDesc* t, int ntiles, int grid, int block, cudaStream_t s) {
-    step_kernel<PROB, R, A, SOLVER, INJ, PPT><<<grid, block / PPT, 0, s>>>(e, t, ntiles);
+    const size_t dyn = INJ ? inj_smem_t<PROB, R, A>(block / PPT) : 0;
+    step_kernel<PROB, R, A, SOLVER, INJ, PPT><<<grid, block / PPT, dyn, s>>>(e, t, ntiles);
+}
+// the injected kernels' staging exceeds the default dynamic shared memory limit: raise it
+// once per device for the largest CTA
+template <int PROB, class R, int A, int SOLVER>
+void prepare_inj_t() {
+    static std::mutex mu;
+    static bool done[64] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return;
+    std::lock_guard<std::mutex> lk(mu);
+    if (done[dev]) return;
+    if (cudaFuncSetAttribute(reinterpret_cast<const void*>(&step_kernel<PROB, R, A, SOLVER, true, 1>),
+                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(inj_smem_t<PROB, R, A>(kMaxBlock))) == cudaSuccess)
+        done[dev] = true;
 }
 template <int PROB, int A, int SOLVER>
 void launch_step_x2_t(const EnsDev* e, const TileDesc* t, int ntiles, int grid, int block, cudaStream_t s) {
@@ -57,6 +79,10 @@ KernelSet make_set() {
                 k.step[1] = &launch_step_t<PROB, R, A, SOLVER, INJ, 2>;
                 k.step_fn[1] = reinterpret_cast<const void*>(&step_kernel<PROB, R, A, SOLVER, INJ, 2>);
             }
+        }
+        if constexpr (INJ) {
+            k.dyn_smem = &inj_smem_t<PROB, R, A>;
+            k.prepare = &prepare_inj_t<PROB, R, A, SOLVER>;
         }
         k.reduce = &launch_reduce_t<Prob::OUT>;
         k.field = &launch_field_chunk_t<R>;

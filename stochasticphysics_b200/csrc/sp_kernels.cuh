@@ -8,8 +8,8 @@
 //                   particles per thread: the state lives in registers, each warp
 //                   stages the chunk's B(t) table (computed once per step in FP64 by
 //                   field_chunk_kernel) in shared memory, the Wiener increments come
-//                   from in-kernel Philox (or from HBM in injection mode, a few steps
-//                   ahead through a register ring), each step's output sines and
+//                   from in-kernel Philox (or from HBM in injection mode, staged a few
+//                   steps ahead in shared memory by bulk copies), each step's output sines and
 //                   cosines carry to the next step's prepare, and each window's Kahan
 //                   mean is reduced per warp in FP64 and stored in one coalesced store
 //                   (SingleParticleSimulator.h:129-159, MeanSimulationResult.h:87-119)
@@ -20,6 +20,7 @@
 #pragma once
 
 #include "sp_physics.cuh"
+#include "sp_stage.cuh"
 
 namespace sp {
 
@@ -309,6 +310,17 @@ __global__ void __launch_bounds__(kMaxBlock / PPT) step_kernel(const EnsDev* __r
     // (a CTA-wide barrier every tile made fast warps wait for slow ones)
     __shared__ R sBw[kMaxBlock / 32][kFieldTile][3];
     R(*const sB)[3] = sBw[threadIdx.x >> 5];
+    // injection mode: each warp's ring of staged increments (dynamic shared memory)
+    using Stream = DwStream<R, Mn>;
+    static_assert(!INJECT || PPT == 1, "injected increments are staged for one particle per thread");
+    Stream dws;
+    if constexpr (INJECT) {
+        extern __shared__ __align__(128) unsigned char sp_dyn_smem[];
+        __shared__ uint64_t sbar[kMaxBlock / 32][Stream::kStages];
+        const int warp = threadIdx.x >> 5;
+        dws.init(reinterpret_cast<R*>(sp_dyn_smem + static_cast<size_t>(warp) * Stream::kStages * Stream::kStageBytes),
+                 sbar[warp]);
+    }
 
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
         const TileDesc td = tiles[t];
@@ -365,23 +377,10 @@ __global__ void __launch_bounds__(kMaxBlock / PPT) step_kernel(const EnsDev* __r
         // live in registers across the step loop.
         unsigned int wpos = static_cast<unsigned int>(s0 % W);
         const unsigned int W32 = static_cast<unsigned int>(W);
-        const R* dwp = static_cast<const R*>(e.dw);
-        static_assert(kFieldTile % 4 == 0, "the increment ring assumes tiles of whole ring turns");
-
-        // injected increments stream from HBM: a ring of the next PF steps' increments keeps
-        // PF steps of loads in flight per thread (the loads of one step alone cannot hide
-        // the memory latency); slot j of the ring holds the steps j, j + PF, ...
-        constexpr int PF = INJECT ? (Mn > 3 ? 2 : 4) : 1;
-        R ring[PPT][PF][Mn];
-        if constexpr (INJECT) {
-#pragma unroll
-            for (int k = 0; k < PPT; ++k)
-#pragma unroll
-                for (int j = 0; j < PF; ++j)
-                    if (active[k] && static_cast<unsigned long long>(j) < nsteps)
-#pragma unroll
-                        for (int m = 0; m < Mn; ++m) ring[k][j][m] = dwp[((s0 + j) * Mn + m) * Np + p[k]];
-        }
+        // injected increments stream from HBM: the warp's rows of the tile's first steps go
+        // in flight now (the warp's 32 particles start at the tile's first + 32 warp)
+        if constexpr (INJECT)
+            dws.begin(static_cast<const R*>(e.dw), Np, td.first + (threadIdx.x & ~31u), s0, nsteps);
 
         for (unsigned long long t0 = 0; t0 < nsteps; t0 += kFieldTile) {
             const int len = static_cast<int>(min(static_cast<unsigned long long>(kFieldTile), nsteps - t0));
@@ -451,28 +450,21 @@ __global__ void __launch_bounds__(kMaxBlock / PPT) step_kernel(const EnsDev* __r
                 }
             };
             if constexpr (INJECT) {
-                // kFieldTile is a multiple of PF, so step s0 + t0 + i sits in ring slot i % PF
-                for (int i0 = 0; i0 < len; i0 += PF) {
-#pragma unroll
-                    for (int j = 0; j < PF; ++j) {
-                        const int i = i0 + j;
-                        if (i < len) {  // uniform
-                            R cur[PPT][Mn];
-                            const unsigned long long gn = t0 + i + PF;  // steps after s0
-#pragma unroll
-                            for (int k = 0; k < PPT; ++k) {
-#pragma unroll
-                                for (int m = 0; m < Mn; ++m) cur[k][m] = ring[k][j][m];
-                                if (active[k] && gn < nsteps)
-#pragma unroll
-                                    for (int m = 0; m < Mn; ++m) ring[k][j][m] = dwp[((s0 + gn) * Mn + m) * Np + p[k]];
-                            }
-                            one_step(i, cur);
-                        }
-                    }
+                for (int i = 0; i < len; ++i) {
+                    R cur[PPT][Mn];
+                    if (!dws.next(cur[0])) break;  // a stage timed out (uniform across the warp)
+                    one_step(i, cur);
                 }
+                if (!dws.ok) break;
             } else {
                 for (int i = 0; i < len; ++i) one_step(i, nullptr);
+            }
+        }
+        if constexpr (INJECT) {
+            if (!dws.ok) {  // report, wait for the copies still in flight, leave the results unwritten
+                if ((threadIdx.x & 31) == 0) atomicExch(&e.ctl->fault, 1ull);
+                dws.drain();
+                return;
             }
         }
 #pragma unroll

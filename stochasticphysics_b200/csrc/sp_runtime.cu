@@ -271,9 +271,11 @@ Ensemble::Ensemble(sp_context* c, const sp_ensemble_desc& d, const LaunchConfig&
                "upload tiles");
     ppt = usable_ppt(*ks, launch.ppt, block);
     grid = ntiles;
+    if (ks->prepare) ks->prepare();
     if (launch.persistent) {
         int per_sm = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ks->step_fn[ppt - 1], block / ppt, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ks->step_fn[ppt - 1], block / ppt,
+                                                      ks->dyn_smem ? ks->dyn_smem(block / ppt) : 0);
         grid = std::min(ntiles, std::max(1, per_sm) * ctx->sms);
     }
 
@@ -458,6 +460,9 @@ void reference_times(unsigned long long K, unsigned long long W, double dt, doub
 
 void Ensemble::read(sp_result* out, sp_stats* st) {
     synchronize();
+    EnsCtl ctl;
+    check_cuda(cudaMemcpy(&ctl, d_ctl, sizeof(ctl), cudaMemcpyDeviceToHost), "read ctl");
+    if (ctl.fault) throw Error(SP_ERR_DEVICE_TIMEOUT, "a staged copy of injected increments did not arrive in time");
     const int OUT = L.OUT;
     std::vector<double> msum(L.K * OUT), wsum(OUT);
     check_cuda(cudaMemcpy(msum.data(), d_msum, msum.size() * 8, cudaMemcpyDeviceToHost), "read msum");
@@ -502,8 +507,6 @@ void Ensemble::read(sp_result* out, sp_stats* st) {
     if (st) {
         std::vector<unsigned char> status(L.Np);
         check_cuda(cudaMemcpy(status.data(), d_status, L.Np, cudaMemcpyDeviceToHost), "read status");
-        EnsCtl ctl;
-        check_cuda(cudaMemcpy(&ctl, d_ctl, sizeof(ctl), cudaMemcpyDeviceToHost), "read ctl");
         std::memset(st, 0, sizeof(*st));
         st->particle_steps = particle_steps;
         for (size_t p = 0; p < L.n; ++p) st->nonfinite_particles += status[p] != 0;

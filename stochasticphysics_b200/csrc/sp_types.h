@@ -72,6 +72,7 @@ struct EnsCtl {
     unsigned long long step_target;  // integrate up to this step
     unsigned long long newton_iterations;
     unsigned long long newton_unconverged;
+    unsigned long long fault;  // non-zero: a staged copy of injected increments did not arrive in time
 };
 
 struct EnsDev {
