@@ -184,7 +184,8 @@ void* Ensemble::dalloc(size_t bytes) {
     return p;
 }
 
-Ensemble::Ensemble(sp_context* c, const sp_ensemble_desc& d, const LaunchConfig& lc) : ctx(c), desc(d), launch(lc) {
+Ensemble::Ensemble(sp_context* c, const sp_ensemble_desc& d, const LaunchConfig& lc, bool chunk_graph)
+    : ctx(c), desc(d), launch(lc) {
     ks = &kernel_set(d.problem, d.anisotropy, solver_slot(d.solver, d.jacobian), d.precision,
                      d.noise == SP_NOISE_INJECTED ? 1 : 0);
     if (!ks->valid) throw Error(SP_ERR_UNSUPPORTED_COMBO, "no kernel for this problem/solver combination");
@@ -281,7 +282,7 @@ Ensemble::Ensemble(sp_context* c, const sp_ensemble_desc& d, const LaunchConfig&
 
     // raw particle properties -> init kernel
     upload_and_init(d);
-    build_graph();
+    if (chunk_graph) build_graph();
     check_cuda(cudaStreamSynchronize(stream), "ensemble init");
 }
 
@@ -419,6 +420,7 @@ void Ensemble::advance(unsigned long long nsteps, cudaStream_t s) {
     if (!s) s = stream;
     const unsigned long long target = std::min(steps_done + nsteps, L.S);
     if (target <= steps_done) return;
+    if (!gexec) build_graph();
     launch_set_target(d_ctl, target, s);
     const unsigned long long nchunks = (target - steps_done + L.chunk - 1) / L.chunk;
     check_cuda(cudaEventRecord(ev0, s), "event");

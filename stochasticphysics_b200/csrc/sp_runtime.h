@@ -111,7 +111,9 @@ struct Ensemble {
     TileDesc* d_tiles = nullptr;
     std::vector<void*> allocs;
 
-    Ensemble(sp_context* c, const sp_ensemble_desc& d, const LaunchConfig& lc);
+    // chunk_graph: capture the ensemble's own chunk graph now (the server launches its
+    // groups' graphs instead and passes false; advance() then captures it on first use)
+    Ensemble(sp_context* c, const sp_ensemble_desc& d, const LaunchConfig& lc, bool chunk_graph = true);
     ~Ensemble();
     Ensemble(const Ensemble&) = delete;
     Ensemble& operator=(const Ensemble&) = delete;

@@ -174,7 +174,7 @@ struct sp_server {
             queue.pop_front();
             try {
                 r->t_admit0 = Clock::now();
-                r->ens = std::make_unique<Ensemble>(ctx, r->desc, launch_for(r->desc, &r->chunks_per_round));
+                r->ens = std::make_unique<Ensemble>(ctx, r->desc, launch_for(r->desc, &r->chunks_per_round), false);
                 r->t_admit1 = Clock::now();
                 r->ens->last_stream = nullptr;
                 // the ensemble holds its inputs on the device now: drop the host copies
@@ -220,8 +220,9 @@ struct sp_server {
         check_cuda(cudaMallocFromPoolAsync(reinterpret_cast<void**>(&g.d_tiles), tiles.size() * sizeof(TileDesc),
                                            ctx->pool, g.stream), "cudaMallocFromPoolAsync");
         check_cuda(cudaMemcpyAsync(g.d_ens, ens.data(), ens.size() * sizeof(EnsDev), cudaMemcpyHostToDevice, g.stream), "copy");
+        // from pageable memory: each copy has taken its bytes when the call returns, and the
+        // group's launches follow them on g.stream
         check_cuda(cudaMemcpyAsync(g.d_tiles, tiles.data(), tiles.size() * sizeof(TileDesc), cudaMemcpyHostToDevice, g.stream), "copy");
-        check_cuda(cudaStreamSynchronize(g.stream), "group upload");
         const int n = static_cast<int>(ens.size());
         const int midpoint = g.members.front()->desc.solver == SP_SOLVER_IMPLICIT_MIDPOINT ? 1 : 0;
         cudaStream_t cs;
