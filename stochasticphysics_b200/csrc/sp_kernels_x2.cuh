@@ -7,43 +7,18 @@
 // add, multiply and fused multiply-add of the drift, diffusion, stepper and window sums
 // covers both particles in one instruction; Philox, Box-Muller and the sines and cosines
 // run per lane.  Each particle's chart (Euler and Neel coordinate rotations near a pole,
-// BrownAndNeelRelaxationEulerSpherical.h:141-361) is decided per lane: while neither
-// lane is rotated, both advance in one pass with the charts fixed at compile time; when
-// either is, a called routine runs the step once per distinct chart pair and keeps each
-// lane's own result, so a particle's arithmetic never depends on its partner.
+// BrownAndNeelRelaxationEulerSpherical.h:141-361) is decided per lane: when both lanes
+// share their charts one pass advances both; otherwise the step runs once per lane's
+// chart pair and each lane keeps the pass made in its own charts, so a particle's
+// arithmetic never depends on its partner.  The passes are one inlined copy of the step
+// in a loop (a called routine would take the addresses of the state and the prefactors
+// and keep them in local memory on every step).
 #pragma once
 
 #include "sp_kernels.cuh"
 #include "sp_pack.cuh"
 
 namespace sp {
-
-// one explicit step of both lanes in the charts (br, nr) of each lane; the rare path
-template <class PX, int SOLVER>
-__device__ __noinline__ void chart_step_x2(const typename PX::Par& q, F2* y, const F2* B, const F2* w, F2 dt,
-                                          const typename PX::Trig& tr, bool br0, bool nr0, bool br1, bool nr1) {
-    using St = Stepper<PX, F2, SOLVER>;
-    constexpr int D = PX::D;
-    const Rot<F2> rot{};
-    F2 ya[D];
-#pragma unroll
-    for (int i = 0; i < D; ++i) ya[i] = y[i];
-    {
-        typename PX::Cache c;
-        PX::prepare_flags(q, ya, c, tr, br0, nr0);
-        St::explicit_from(q, rot, ya, c, B, w, dt);
-    }
-    if (br1 == br0 && nr1 == nr0) {
-#pragma unroll
-        for (int i = 0; i < D; ++i) y[i] = ya[i];
-        return;
-    }
-    typename PX::Cache c;
-    PX::prepare_flags(q, y, c, tr, br1, nr1);
-    St::explicit_from(q, rot, y, c, B, w, dt);
-#pragma unroll
-    for (int i = 0; i < D; ++i) y[i] = F2(lane0(ya[i]), lane1(y[i]));
-}
 
 template <int PROB, int A, int SOLVER>
 __global__ void __launch_bounds__(kMaxBlock / 2) step_kernel_x2(const EnsDev* __restrict__ ensembles,
@@ -122,12 +97,20 @@ __global__ void __launch_bounds__(kMaxBlock / 2) step_kernel_x2(const EnsDev* __
                 const float tn0 = fabsf(lane0(y[3])), tn1 = fabsf(lane1(y[3]));
                 const bool br0 = rb && (tb0 < min1 || tb0 > max1), br1 = rb && (tb1 < min1 || tb1 > max1);
                 const bool nr0 = rn && (tn0 < min2 || tn0 > max2), nr1 = rn && (tn1 < min2 || tn1 > max2);
-                if (!(br0 || br1 || nr0 || nr1)) {
+                const int passes = (br0 == br1 && nr0 == nr1) ? 1 : 2;
+                F2 y0[D];
+#pragma unroll
+                for (int d = 0; d < D; ++d) y0[d] = y[d];
+#pragma unroll 1
+                for (int pass = 0; pass < passes; ++pass) {
+                    F2 yp[D];
+#pragma unroll
+                    for (int d = 0; d < D; ++d) yp[d] = y0[d];
                     typename PX::Cache c;
-                    PX::prepare_flags(q, y, c, tr, false, false);
-                    St::explicit_from(q, rot, y, c, B, w, dt);
-                } else {
-                    chart_step_x2<PX, SOLVER>(q, y, B, w, dt, tr, br0, nr0, br1, nr1);
+                    PX::prepare_flags(q, yp, c, tr, pass ? br1 : br0, pass ? nr1 : nr0);
+                    St::explicit_from(q, rot, yp, c, B, w, dt);
+#pragma unroll
+                    for (int d = 0; d < D; ++d) y[d] = pass ? F2(lane0(y[d]), lane1(yp[d])) : yp[d];
                 }
                 F2 o[OUT];
                 PX::out_t(y, o, tr);
