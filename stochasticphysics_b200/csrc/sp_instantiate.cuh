@@ -5,7 +5,6 @@
 
 #include "sp_dispatch.h"
 #include "sp_kernels.cuh"
-#include "sp_kernels_x2.cuh"
 
 namespace sp {
 
@@ -33,14 +32,6 @@ void prepare_inj_t() {
                              static_cast<int>(inj_smem_t<PROB, R, A>(kMaxBlock))) == cudaSuccess)
         done[dev] = true;
 }
-template <int PROB, int A, int SOLVER>
-void launch_step_x2_t(const EnsDev* e, const TileDesc* t, int ntiles, int grid, int block, cudaStream_t s) {
-    step_kernel_x2<PROB, A, SOLVER><<<grid, block / 2, 0, s>>>(e, t, ntiles);
-}
-// the paired FP32 form (sp_kernels_x2.cuh): Brown+Neel Euler/spherical, explicit steppers
-template <int PROB, int SOLVER>
-constexpr bool kPairedStep = PROB == kBrownNeelEuler && (SOLVER == kEulerMaruyama || SOLVER == kHeun ||
-                                                         SOLVER == kMillstein || SOLVER == kEulerMaruyamaNormalized);
 template <int PROB, class R, int A>
 void launch_init_t(const EnsDev* e, const RawParticles& rp, unsigned long long Np, cudaStream_t s) {
     init_kernel<PROB, R, A><<<static_cast<unsigned>(Np / kPad), kPad, 0, s>>>(e, rp);
@@ -72,13 +63,8 @@ KernelSet make_set() {
         k.step[0] = &launch_step_t<PROB, R, A, SOLVER, INJ, 1>;
         k.step_fn[0] = reinterpret_cast<const void*>(&step_kernel<PROB, R, A, SOLVER, INJ, 1>);
         if constexpr (sizeof(R) == 4 && !INJ) {  // two particles per thread: FP32, in-kernel noise
-            if constexpr (kPairedStep<PROB, SOLVER>) {  // in paired f32x2 arithmetic
-                k.step[1] = &launch_step_x2_t<PROB, A, SOLVER>;
-                k.step_fn[1] = reinterpret_cast<const void*>(&step_kernel_x2<PROB, A, SOLVER>);
-            } else {  // two interleaved scalar chains
-                k.step[1] = &launch_step_t<PROB, R, A, SOLVER, INJ, 2>;
-                k.step_fn[1] = reinterpret_cast<const void*>(&step_kernel<PROB, R, A, SOLVER, INJ, 2>);
-            }
+            k.step[1] = &launch_step_t<PROB, R, A, SOLVER, INJ, 2>;
+            k.step_fn[1] = reinterpret_cast<const void*>(&step_kernel<PROB, R, A, SOLVER, INJ, 2>);
         }
         if constexpr (INJ) {
             k.dyn_smem = &inj_smem_t<PROB, R, A>;

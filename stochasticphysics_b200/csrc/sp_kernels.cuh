@@ -201,6 +201,8 @@ __global__ void __launch_bounds__(kMaxBlock) init_kernel(const EnsDev* __restric
     for (int i = 0; i < P; ++i) prm[i * Np + p] = static_cast<R>(pd[i]);
     const_cast<double*>(e.moment)[p] = moment;
     for (int c = 0; c < OUT; ++c) { ks[c * Np + p] = R(0); kc[c * Np + p] = R(0); }
+    if (e.slo)
+        for (int i = 0; i < D; ++i) static_cast<R*>(e.slo)[i * Np + p] = R(0);
     e.status[p] = 0;
     R o[OUT];
     Prob::out(y, o);
@@ -348,6 +350,7 @@ __global__ void __launch_bounds__(kMaxBlock / PPT) step_kernel(const EnsDev* __r
         rot.min2 = static_cast<R>(e.min2); rot.max2 = static_cast<R>(e.max2);
 
         R y[PPT][D];
+        R lo[PPT][D];  // FP32 form: the carried rounding errors of the slowly moving components
         WindowSum<R, OUT> acc[PPT];
         typename Prob::Par q[PPT];
         typename Prob::Trig tr[PPT];  // sincos of y, carried from each step's output to the next prepare
@@ -370,6 +373,9 @@ __global__ void __launch_bounds__(kMaxBlock / PPT) step_kernel(const EnsDev* __r
                 q[k] = Prob::load(static_cast<const R*>(e.params), Np, td.first);  // any valid slot; results are discarded
             }
             Prob::trig(y[k], tr[k]);
+            const R* slo = static_cast<const R*>(e.slo);
+#pragma unroll
+            for (int i = 0; i < D; ++i) lo[k][i] = (slo && active[k]) ? slo[i * Np + p[k]] : R(0);
         }
         NewtonCount nc{0u, 0u};
         // W < 2^31 (validated); the window position fits 32 bits.  Values used only
@@ -414,7 +420,8 @@ __global__ void __launch_bounds__(kMaxBlock / PPT) step_kernel(const EnsDev* __r
                         if constexpr (SOLVER == kWeakTest) St::step_weak(q[k], rot, y[k], B, w, An, dt, sqdt, tr[k]);
                         else St::step_es1(q[k], rot, y[k], B, w, An, dt, sqdt, tr[k]);
                     } else {
-                        St::step(q[k], rot, y[k], B, w, dt, e.max_iter, e.tol, nc, tr[k]);
+                        St::step(q[k], rot, y[k], B, w, dt, e.max_iter, e.tol, nc, tr[k],
+                                 M<R>::kCompensatedState ? lo[k] : nullptr);
                     }
                     R o[OUT];
                     Prob::out_t(y[k], o, tr[k]);
@@ -475,7 +482,15 @@ __global__ void __launch_bounds__(kMaxBlock / PPT) step_kernel(const EnsDev* __r
                 R* kc = static_cast<R*>(e.kcomp);
                 bool finite = true;
 #pragma unroll
-                for (int i = 0; i < D; ++i) { state[i * Np + p[k]] = y[k][i]; finite = finite && M<R>::finite(y[k][i]); }
+                for (int i = 0; i < D; ++i) {
+                    state[i * Np + p[k]] = y[k][i];
+                    finite = finite && M<R>::finite(y[k][i]);
+                }
+                if (e.slo) {
+                    R* slo = static_cast<R*>(e.slo);
+#pragma unroll
+                    for (int i = 0; i < D; ++i) slo[i * Np + p[k]] = lo[k][i];
+                }
 #pragma unroll
                 for (int c = 0; c < OUT; ++c) { ks[c * Np + p[k]] = acc[k].get_sum(c); kc[c * Np + p[k]] = acc[k].get_comp(c); }
                 if (!finite) e.status[p[k]] = 1;

@@ -41,6 +41,7 @@ static __device__ __noinline__ SinCosD box_muller_pair_d(uint32_t a, uint32_t b)
 template <> struct M<double> {
     // rare paths (chart rotations, the mixed-chart drift) are called, not inlined
     static constexpr bool kColdCalls = true;
+    static constexpr bool kCompensatedState = false;  // FP64 resolves every increment
     static __device__ __forceinline__ double sin(double x) { return ::sin(x); }
     static __device__ __forceinline__ double cos(double x) { return ::cos(x); }
     static __device__ __forceinline__ void sincos(double x, double* s, double* c) {
@@ -65,6 +66,8 @@ template <> struct M<double> {
 
 template <> struct M<float> {
     static constexpr bool kColdCalls = false;
+    // the slowly moving state components carry their rounding error (Stepper::explicit_from)
+    static constexpr bool kCompensatedState = true;
     static __device__ __forceinline__ float sin(float x) { return __sinf(x); }
     static __device__ __forceinline__ float cos(float x) { return __cosf(x); }
     static __device__ __forceinline__ void sincos(float x, float* s, float* c) { __sincosf(x, s, c); }

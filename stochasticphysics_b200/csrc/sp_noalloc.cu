@@ -115,6 +115,7 @@ extern "C" SP_API sp_status sp_simulate_noalloc(const sp_ensemble_desc* desc, co
         auto take = [&](size_t bytes) { const size_t at = off; off += align256(bytes); return at; };
         const size_t o_ens = take(sizeof(EnsDev)), o_ctl = take(sizeof(EnsCtl)), o_tiles = take(ntiles * sizeof(TileDesc));
         const size_t o_state = take(L.Np * L.D * R), o_ksum = take(L.Np * L.OUT * R), o_kcomp = take(L.Np * L.OUT * R);
+        const size_t o_slo = R == 4 ? take(L.Np * L.D * R) : 0;
         const size_t o_params = take(L.Np * L.P * R), o_moment = take(L.Np * 8), o_status = take(L.Np);
         const size_t o_partial = take((L.Np / 32) * L.slots * L.OUT * 8), o_ftab = take(L.chunk * 3 * R);
         if (off > kNoAllocScratchBytes)
@@ -147,6 +148,7 @@ extern "C" SP_API sp_status sp_simulate_noalloc(const sp_ensemble_desc* desc, co
         }
         e.slots = L.slots;
         e.state = base + o_state; e.ksum = base + o_ksum; e.kcomp = base + o_kcomp; e.params = base + o_params;
+        e.slo = R == 4 ? base + o_slo : nullptr;
         e.moment = reinterpret_cast<double*>(base + o_moment); e.status = base + o_status;
         e.partial = reinterpret_cast<double*>(base + o_partial); e.ftab = base + o_ftab;
         e.msum = device_mean; e.wsum = device_weight; e.traj = nullptr; e.dw = nullptr;

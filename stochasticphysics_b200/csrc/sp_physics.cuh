@@ -187,6 +187,7 @@ struct NeelCart {
     static __device__ __forceinline__ void prepare(const Par&, const Rot<R>&, R*, Cache&) {}
     static __device__ __forceinline__ void recompute(const Par&, const R*, Cache&) {}
     static __device__ __forceinline__ void finish(const Rot<R>&, R*, const Cache&) {}
+    static __device__ __forceinline__ int compensated(const Cache&) { return 0; }  // Neel increments are many ulp
     static __device__ __forceinline__ void det(const Par& q, const R* y, const Cache&, const R* B, R* a) {
         const V3<R> m = v3(y[0], y[1], y[2]);
         const V3<R> H = heff(q, m, B);
@@ -399,6 +400,7 @@ struct NeelSph {
         if (c.rot) unrotate(y);
         else { y[0] = wrap_two_pi(y[0]); y[1] = wrap_two_pi(y[1]); }
     }
+    static __device__ __forceinline__ int compensated(const Cache&) { return 0; }
     static __device__ __forceinline__ void det(const Par& q, const R*, const Cache& c, const R* B, R* a) {
         const V3<R> H = heff(q, c.md, B);
         a[0] = dot(c.P0, H);
@@ -593,8 +595,7 @@ struct BrownNeelEuler {
         const R tb = M<R>::abs(y[1]), tn = M<R>::abs(y[3]);
         prepare_flags(q, y, c, t, r.rb && (tb < r.min1 || tb > r.max1), r.rn && (tn < r.min2 || tn > r.max2));
     }
-    // prepare_t with the charts given: br (Euler angles rotated), nr (Neel angles rotated);
-    // the paired FP32 form decides them per particle and runs both lanes in one chart pair
+    // prepare_t with the charts given: br (Euler angles rotated), nr (Neel angles rotated)
     static __device__ __forceinline__ void prepare_flags(const Par&, R* y, Cache& c, const Trig& t, bool br, bool nr) {
         c.br = br;
         if (c.br) {
@@ -691,6 +692,9 @@ struct BrownNeelEuler {
             return heff_uniaxial_cubic(q.pF, rot_apply_t(q, z), q.pF2, m, x, y, z, v3(B[0], B[1], B[2]));
         else return Aniso<R, A>::heff(q.pF, m, x, y, z, v3(B[0], B[1], B[2]));
     }
+    // the Euler angles of the particle (Brown rotation: a few ulp of FP32 angles per step),
+    // while their chart is not rotated
+    static __device__ __forceinline__ int compensated(const Cache& c) { return c.br ? 0 : 3; }
     static __device__ __forceinline__ void finish(const Rot<R>&, R* y, const Cache& c) {
         if (c.br) euler_unrotate(y);
         else { y[0] = wrap_two_pi(y[0]); y[1] = wrap_two_pi(y[1]); y[2] = wrap_two_pi(y[2]); }
@@ -790,6 +794,7 @@ struct BrownNeelCart {
     static __device__ __forceinline__ void prepare(const Par&, const Rot<R>&, R*, Cache&) {}
     static __device__ __forceinline__ void recompute(const Par&, const R*, Cache&) {}
     static __device__ __forceinline__ void finish(const Rot<R>&, R*, const Cache&) {}
+    static __device__ __forceinline__ int compensated(const Cache&) { return 3; }  // the particle axis n
     // .inl:222-271 (the reference returns zero for cubic anisotropy, .inl:225-229)
     static __device__ __forceinline__ void det(const Par& q, const R* y, const Cache&, const R* B, R* a) {
         if constexpr (A == kCubic) {
@@ -951,17 +956,45 @@ struct Stepper {
     static constexpr bool kExplicit = SOLVER == kEulerMaruyama || SOLVER == kHeun ||
                                       SOLVER == kEulerMaruyamaNormalized || SOLVER == kMillstein;
 
-    // one explicit step from y already prepared into the chart c (by prepare_t, or in the
-    // paired FP32 form by prepare_flags); ends with finishCalculations
+    // y + inc with the update's rounding error carried in lo (Fast2Sum: exact when
+    // |y| >= |inc + lo|, which holds for the small increments it is used for)
+    static __device__ __forceinline__ void add_compensated(R& y, R& lo, R inc) {
+        const R t = inc + lo;
+        const R s = y + t;
+        lo = t - (s - y);
+        y = s;
+    }
+    // whether component i of the update in chart c keeps its rounding error: in the FP32
+    // form the components a problem names (P::compensated), whose per-step increments are
+    // only a few ulp (the particle's Brown rotation: rounded plainly, they would pick up a
+    // spurious diffusion of several per cent and bias the ensemble mean); lo of the other
+    // components is cleared (a rotated chart re-parameterises the angles)
+    static __device__ __forceinline__ bool keep_error(const Cache& c, R* lo, int i) {
+        if constexpr (!M<R>::kCompensatedState || !(SOLVER == kEulerMaruyama || SOLVER == kHeun || SOLVER == kMillstein)) {
+            return false;
+        } else {
+            if (!lo) return false;
+            if (i < P::compensated(c)) return true;
+            lo[i] = R(0);
+            return false;
+        }
+    }
+
+    // one explicit step from y already prepared into the chart c by prepare_t; ends with
+    // finishCalculations.  lo: the FP32 form's carried rounding errors of y (or nullptr)
     static __device__ __forceinline__ void explicit_from(const Par& q, const Rot<R>& rot, R* y, Cache& c, const R* B,
-                                                         const R* w, R dt) {
+                                                         const R* w, R dt, R* lo = nullptr) {
         if constexpr (SOLVER == kEulerMaruyama) {
             R a[D], d[D], bw[D];
             P::det(q, y, c, B, a);
             P::drift(q, y, c, d);
             P::bdw(q, y, c, w, bw);
 #pragma unroll
-            for (int i = 0; i < D; ++i) y[i] = y[i] + ((a[i] + d[i]) * dt + bw[i]);
+            for (int i = 0; i < D; ++i) {
+                const R inc = (a[i] + d[i]) * dt + bw[i];
+                if (keep_error(c, lo, i)) add_compensated(y[i], lo[i], inc);
+                else y[i] = y[i] + inc;
+            }
             P::finish(rot, y, c);
         } else if constexpr (SOLVER == kHeun) {
             R a1[D], d[D], bw[D], s[D];
@@ -978,7 +1011,10 @@ struct Stepper {
             P::det(q, s, c, B, a2);
             P::drift(q, s, c, d);
 #pragma unroll
-            for (int i = 0; i < D; ++i) y[i] = (y[i] + (R(0.5) * ((a2[i] + d[i]) + a1[i])) * dt) + bw[i];
+            for (int i = 0; i < D; ++i) {
+                if (keep_error(c, lo, i)) add_compensated(y[i], lo[i], (R(0.5) * ((a2[i] + d[i]) + a1[i])) * dt + bw[i]);
+                else y[i] = (y[i] + (R(0.5) * ((a2[i] + d[i]) + a1[i])) * dt) + bw[i];
+            }
             P::finish(rot, y, c);
         } else if constexpr (SOLVER == kEulerMaruyamaNormalized) {
             R a[D], d[D], bw[D];
@@ -998,18 +1034,22 @@ struct Stepper {
 #pragma unroll
             for (int j = 0; j < Mn; ++j) ww = ww + w[j] * w[j];
 #pragma unroll
-            for (int i = 0; i < D; ++i) y[i] = ((y[i] + a[i] * dt) + bw[i]) + d[i] * ww;
+            for (int i = 0; i < D; ++i) {
+                if (keep_error(c, lo, i)) add_compensated(y[i], lo[i], (a[i] * dt + bw[i]) + d[i] * ww);
+                else y[i] = ((y[i] + a[i] * dt) + bw[i]) + d[i] * ww;
+            }
             P::finish(rot, y, c);
         }
     }
 
     // tr: sines and cosines of y (from the previous step's output), reused by prepare_t
     static __device__ __forceinline__ void step(const Par& q, const Rot<R>& rot, R* y, const R* B, const R* w, R dt,
-                                                int max_iter, double tol, NewtonCount& nc, const Trig& tr) {
+                                                int max_iter, double tol, NewtonCount& nc, const Trig& tr,
+                                                R* lo = nullptr) {
         if constexpr (kExplicit) {
             Cache c;
             P::prepare_t(q, rot, y, c, tr);
-            explicit_from(q, rot, y, c, B, w, dt);
+            explicit_from(q, rot, y, c, B, w, dt, lo);
         } else {
             if constexpr (P::kHasJacobian) {
                 // Newton on f(yj) = finish(prepare((yj+yn)/2) + a dt + b dW) + yn/2 - 3yj/2,

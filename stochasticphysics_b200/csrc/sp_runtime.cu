@@ -167,7 +167,8 @@ EnsembleLayout layout_of(const sp_ensemble_desc& d, const LaunchConfig& lc) {
     L.chunk = std::max<unsigned long long>(1, std::min<unsigned long long>(lc.chunk, std::max<unsigned long long>(L.S, 1)));
     L.slots = static_cast<int>(L.chunk / L.W + 2);
     const unsigned long long nw = L.Np / 32;
-    L.bytes = L.Np * (L.D + 2ull * L.OUT + L.P) * L.real + L.Np * 8 + L.Np + nw * L.slots * L.OUT * 8 +
+    L.bytes = L.Np * ((L.real == 4 ? 2ull : 1ull) * L.D + 2ull * L.OUT + L.P) * L.real + L.Np * 8 + L.Np +
+              nw * L.slots * L.OUT * 8 +
               L.K * L.OUT * 8 + L.OUT * 8 + L.K * 3 * 8 + L.chunk * 3 * L.real + sizeof(EnsCtl) + sizeof(EnsDev) +
               ((L.Np + 31) / 32 + 1) * sizeof(TileDesc);
     if (d.record_trajectories > 0) L.bytes += L.K * L.OUT * (L.n / d.record_trajectories) * 8;
@@ -199,6 +200,7 @@ Ensemble::Ensemble(sp_context* c, const sp_ensemble_desc& d, const LaunchConfig&
     d_state = dalloc(L.Np * L.D * R);
     d_ksum = dalloc(L.Np * L.OUT * R);
     d_kcomp = dalloc(L.Np * L.OUT * R);
+    if (L.real == 4) d_slo = dalloc(L.Np * L.D * R);
     d_params = dalloc(L.Np * L.P * R);
     d_moment = static_cast<double*>(dalloc(L.Np * 8));
     d_status = static_cast<unsigned char*>(dalloc(L.Np));
@@ -256,7 +258,7 @@ Ensemble::Ensemble(sp_context* c, const sp_ensemble_desc& d, const LaunchConfig&
         e.max2 = kPi - e.min2;
     }
     e.slots = L.slots;
-    e.state = d_state; e.ksum = d_ksum; e.kcomp = d_kcomp; e.params = d_params; e.moment = d_moment;
+    e.state = d_state; e.ksum = d_ksum; e.kcomp = d_kcomp; e.slo = d_slo; e.params = d_params; e.moment = d_moment;
     e.dw = d_dw; e.partial = d_partial; e.msum = d_msum; e.wsum = d_wsum; e.traj = d_traj; e.ftab = d_ftab;
     e.traj_stride = traj_stride ? traj_stride : 1; e.traj_n = traj_n;
     e.status = d_status; e.ctl = d_ctl;

@@ -101,7 +101,7 @@ struct Ensemble {
     int block = 128, grid = 1, ntiles = 0, ppt = 1;
     unsigned long long traj_stride = 0, traj_n = 0;  // recorded particles: every traj_stride-th, traj_n of them
     EnsDev hdev;
-    void *d_state = nullptr, *d_ksum = nullptr, *d_kcomp = nullptr, *d_params = nullptr, *d_dw = nullptr,
+    void *d_state = nullptr, *d_ksum = nullptr, *d_kcomp = nullptr, *d_slo = nullptr, *d_params = nullptr, *d_dw = nullptr,
          *d_ftab = nullptr;
     double *d_moment = nullptr, *d_partial = nullptr, *d_msum = nullptr, *d_wsum = nullptr, *d_traj = nullptr,
            *d_field = nullptr;

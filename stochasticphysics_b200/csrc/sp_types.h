@@ -5,6 +5,7 @@
 //   state   [D][Np]      Real   SDE state y (D = 3, 2, 5, 6)
 //   ksum    [OUT][Np]    Real   Kahan running window sum of the outputs
 //   kcomp   [OUT][Np]    Real   Kahan compensation (persists across windows)
+//   slo     [D][Np]      float  FP32 form only: rounding errors the state update carries
 //   params  [P][Np]      Real   derived per-particle prefactors (see kParams*)
 //   moment  [Np]         double Ms*V, the reference's getWeighting
 //   partial [warps][slots][OUT] double  per-warp weighted window means of one chunk
@@ -95,6 +96,7 @@ struct EnsDev {
     void* state;
     void* ksum;
     void* kcomp;
+    void* slo;      // FP32 form: [D][Np] carried rounding errors of the state (nullptr in FP64)
     const void* params;
     const double* moment;
     const void* dw;
