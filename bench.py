@@ -25,8 +25,11 @@ Heun) on the device-resident state, i.e. 2 x 65536 x 10000 particle-steps.
                Lissajous field) through sp_server_*, FP32; p50/p99 latency,
                aggregate particle-steps/s, and the same requests one at a time in
                FP64 as the serial baseline
-  batched      256 Neel parameter sets (uneven N and S) submitted at once, batched
-               per kernel key into shared launches (N=1)
+  batched      256 Neel parameter sets (uneven N and S, the stated sizes: about 8e12
+               particle-steps) submitted at once, batched per kernel key into shared
+               launches (N=1)
+  serving_overload  the serving arrivals with full-length requests for a fixed window:
+               saturated rate, requests in flight over time, latency of those finished
   plain_neel_1024  the 1024-particle FP64 Neel run of 1e6 steps (latency-bound small
                ensemble), whole run on the device and end to end, beside the CPU
   stiff        the cubic ImplicitMidpoint workload (262144 particles, dt = 1e-10 s):
@@ -307,7 +310,7 @@ def overload_leg(ctx, arrival_s=2.0, observe_s=30.0, rate=50.0, seed=0x5EED0005)
                         "Heun / Millstein, FP32, Lissajous 12 mT at 25.25 / 26.04 kHz, dt = 1e-11 s"}
 
 
-def batched_leg(ctx, count, step_scale, seed=0x5EED0004, serial_sample=32):
+def batched_leg(ctx, count, step_scale, seed=0x5EED0004, serial_sample=16):
     """Parameter-set batch: `count` Neel ensembles with the batched-set distributions
     (N ~ logU[1e3, 6.4e4], S ~ logU[1e5, 1e7] x step_scale, Heun / Millstein
     alternating, FP32), all submitted at once to the server, which runs each kernel
@@ -335,6 +338,7 @@ def batched_leg(ctx, count, step_scale, seed=0x5EED0004, serial_sample=32):
         ctx.simulate(s)
     serial_s = time.perf_counter() - t
     return {"sets": count, "value": ps / wall, "unit": UNIT, "wall_s": wall, "particle_steps": ps,
+            "step_scale": step_scale,
             "max_latency_ms": max(lat),
             "launch_shapes": {s.solver.name: ctx.launch_config(s) for s in specs[:2]},
             "one_at_a_time": {"value": sum(s.n * s.integrated_steps for s in sample) / serial_s, "sets": len(sample)},
@@ -703,7 +707,7 @@ def main():
     ap.add_argument("--no-stiff", action="store_true", help="skip the stiff ImplicitMidpoint leg")
     ap.add_argument("--no-injected", action="store_true", help="skip the injected-noise (HBM) leg")
     ap.add_argument("--no-sizes", action="store_true", help="skip the ensemble-size sweep")
-    ap.add_argument("--batched-step-scale", type=float, default=0.02,
+    ap.add_argument("--batched-step-scale", type=float, default=1.0,
                     help="scale of the batched sets' step counts (S ~ logU[1e5, 1e7] x scale)")
     ap.add_argument("--overload-seconds", type=float, default=30.0,
                     help="observation window of the full-size serving overload leg (0: skip)")

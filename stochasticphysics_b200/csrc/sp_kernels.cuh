@@ -309,8 +309,10 @@ __global__ void __launch_bounds__(kMaxBlock / PPT) step_kernel(const EnsDev* __r
     using St = Stepper<Prob, R, SOLVER>;
     constexpr int D = Prob::D, Mn = Prob::Mn, OUT = Prob::OUT;
     // per-warp copy of the chunk's field table: warps never wait on each other
-    // (a CTA-wide barrier every tile made fast warps wait for slow ones)
-    __shared__ R sBw[kMaxBlock / 32][kFieldTile][3];
+    // (a CTA-wide barrier every tile made fast warps wait for slow ones).  Injected kernels
+    // stage 32 steps at a time, leaving shared memory to the increments' ring.
+    constexpr int FT = INJECT ? 32 : kFieldTile;
+    __shared__ R sBw[kMaxBlock / 32][FT][3];
     R(*const sB)[3] = sBw[threadIdx.x >> 5];
     // injection mode: each warp's ring of staged increments (dynamic shared memory)
     using Stream = DwStream<R, Mn>;
@@ -388,8 +390,8 @@ __global__ void __launch_bounds__(kMaxBlock / PPT) step_kernel(const EnsDev* __r
         if constexpr (INJECT)
             dws.begin(static_cast<const R*>(e.dw), Np, td.first + (threadIdx.x & ~31u), s0, nsteps);
 
-        for (unsigned long long t0 = 0; t0 < nsteps; t0 += kFieldTile) {
-            const int len = static_cast<int>(min(static_cast<unsigned long long>(kFieldTile), nsteps - t0));
+        for (unsigned long long t0 = 0; t0 < nsteps; t0 += FT) {
+            const int len = static_cast<int>(min(static_cast<unsigned long long>(FT), nsteps - t0));
             __syncwarp();
             for (int i = threadIdx.x & 31; i < 3 * len; i += 32) (&sB[0][0])[i] = ftab[3 * t0 + i];
             __syncwarp();

@@ -6,7 +6,9 @@
 // shared, completion counted in bytes on an mbarrier) of 32 consecutive increments,
 // kStep steps per stage and kStages stages in a ring, so about (kStages - 1) kStep Mn
 // rows per warp are in flight while the warp computes, without holding any of them in
-// registers.  The copies read this GPU's own memory only and use no multicast.
+// registers.  The ring is sized so that four 128-thread CTAs fit an SM (FP64, noise
+// dimension 3: 9 KB per warp).  The copies read this GPU's own memory only and use no
+// multicast.
 //
 // Every wait on a stage is bounded by a clock budget.  A stage that does not arrive in
 // time sets EnsCtl::fault, the warp waits (bounded again) for the copies it still has in
@@ -60,7 +62,7 @@ __device__ __forceinline__ void bulk_copy_g2s(uint32_t dst, const void* src, uin
 template <class R, int Mn>
 struct DwStream {
     static constexpr int kStep = 4;    // steps per stage
-    static constexpr int kStages = 4;  // stages in the ring
+    static constexpr int kStages = 3;  // stages in the ring
     static constexpr int kRow = 32 * static_cast<int>(sizeof(R));
     static constexpr int kStageBytes = kStep * Mn * kRow;
     static_assert(kRow % 16 == 0, "bulk copies move multiples of 16 bytes");

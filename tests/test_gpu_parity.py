@@ -12,7 +12,8 @@ Bars (stated per test):
       which it stays at or below 1e-7 (asserted; the bar and horizon are printed).
   in-kernel Philox, FP64: the same 32-bit Philox words as the oracle; normals
       within 1e-14 relative, trajectories within 1e-9
-  FP32 form: ensemble mean within 1e-3 of the FP64 kernel on the same noise
+  FP32 form: ensemble mean within 1e-3 of the FP64 kernel on the same noise, with a
+      standard error of at most 3e-4 and no bias beyond 4 standard errors
 """
 import dataclasses
 import math
@@ -396,27 +397,50 @@ def test_chunked_advance_equals_one_shot(ctx):
     np.testing.assert_array_equal(r.trajectories, one.trajectories)
 
 
-def test_fp32_form_close_to_fp64(ctx):
-    """FP32 stepping with FP64 time/phase/sums vs the FP64 kernel on the same Philox noise.
+FP32_CASES = [(Problem.Neel, Solver.Heun_Strong, 65536, 21000), (Problem.Neel, Solver.Millstein, 65536, 21000),
+              (Problem.NeelSpherical, Solver.Heun_Strong, 65536, 21000),
+              (Problem.NeelSpherical, Solver.EulerMaruyama, 65536, 21000),
+              (Problem.BrownAndNeelEulerSpherical, Solver.Millstein, 262144, 31000),
+              (Problem.BrownAndNeelEulerSpherical, Solver.Heun_Strong, 262144, 31000),
+              (Problem.BrownAndNeel, Solver.EulerMaruyama_Normalized, 65536, 21000)]
 
-    Pathwise, the two agree closely until the stochastic dynamics amplify the FP32
-    round-off (the FP64 kernel with its increments merely rounded to float diverges from
-    itself equally fast); afterwards the FP32 ensemble is a statistically equivalent sample.
-    Checks: the first window within 1e-4, and every window within 4 standard errors of the
-    difference of two N-particle means (|m_i| <= 1, so sigma^2 <= 1/3 per component)."""
-    for problem, solver in ((Problem.Neel, Solver.Heun_Strong), (Problem.Neel, Solver.Millstein),
-                            (Problem.NeelSpherical, Solver.Heun_Strong), (Problem.NeelSpherical, Solver.EulerMaruyama),
-                            (Problem.BrownAndNeelEulerSpherical, Solver.Millstein),
-                            (Problem.BrownAndNeelEulerSpherical, Solver.Heun_Strong),
-                            (Problem.BrownAndNeel, Solver.Heun_Strong)):
-        n = 4096
-        spec = small_spec(problem, solver, n=n, steps=20000, W=1000)
-        r64 = ctx.simulate(spec)
-        r32 = ctx.simulate(dataclasses.replace(spec, precision=Precision.FP32))
-        d = np.abs(r32.mean[:, -3:] - r64.mean[:, -3:])
-        assert np.max(d[1]) < 1e-4, f"{problem.name}/{solver.name}: first-window FP32 error {np.max(d[1]):.2e}"
-        bound = 4 * math.sqrt(2.0 / (3.0 * n))
-        assert np.nanmax(d) < bound, f"{problem.name}/{solver.name}: FP32 mean error {np.nanmax(d):.2e}"
+
+@pytest.mark.parametrize("problem,solver,n,steps", FP32_CASES,
+                         ids=[f"{p.name}-{s.name}-{n}" for p, s, n, _ in FP32_CASES])
+def test_fp32_ensemble_mean_within_1e_3(ctx, problem, solver, n, steps):
+    """The FP32 form against the FP64 kernel on the same Philox noise, the qualifier of the
+    headline metric: the moment-weighted mean magnetisation (saturation value 1) of the FP32
+    ensemble within 1e-3 of the FP64 one in every window and component.  The ensemble runs
+    as 8 shards with global particle ids, merged (sp_merge_shards); the spread of the shards'
+    differences gives the standard error, which must be at most 3e-4 so that a 1e-3 error
+    is resolved, and the difference averaged over the windows must be within 4 standard
+    errors of zero (no bias; a plainly rounded FP32 state update of the slow Brown angles
+    gave -4e-4, about 5 standard errors, on the headline workload).  The first window
+    agrees pathwise (1e-4).  The coupled Cartesian problem runs EulerMaruyama_Normalized:
+    its other explicit steppers let |m| run away to overflow within these horizons, as the
+    reference's do."""
+    shards = 8
+    spec = small_spec(problem, solver, n=n, steps=steps, W=1000)
+    k = n // shards
+    parts = [spec.subset(i * k, (i + 1) * k) for i in range(shards)]
+    res = {}
+    for prec in (Precision.FP64, Precision.FP32):
+        with ctx.server() as srv:
+            ids = srv.submit_many([dataclasses.replace(p, precision=prec) for p in parts])
+            res[prec] = [srv.wait(i)[0] for i in ids]
+    merged = {prec: sp.merge_shards([r.weighted_sum for r in rs], [r.weight for r in rs])[0] for prec, rs in res.items()}
+    cols = slice(spec.dims[2] - 3, spec.dims[2])
+    d = (merged[Precision.FP32] - merged[Precision.FP64])[1:, cols]
+    per_shard = np.stack([(a.mean - b.mean)[1:, cols] for a, b in zip(res[Precision.FP32], res[Precision.FP64])])
+    se = per_shard.std(axis=0, ddof=1) / math.sqrt(shards)
+    bias, bias_se = d.mean(axis=0), per_shard.mean(axis=1).std(axis=0, ddof=1) / math.sqrt(shards)
+    label = f"{problem.name}/{solver.name}"
+    print(f"{label}: max {np.abs(d).max():.2e}, max se {se.max():.2e}, bias {bias} +- {bias_se}")
+    assert np.isfinite(d).all(), f"{label}: non-finite mean"
+    assert np.abs(d[0]).max() < 1e-4, f"{label}: first-window FP32 error {np.abs(d[0]).max():.2e}"
+    assert np.abs(d).max() <= 1e-3, f"{label}: FP32 mean error {np.abs(d).max():.2e}"
+    assert se.max() <= 3e-4, f"{label}: standard error {se.max():.2e} cannot resolve 1e-3"
+    assert np.all(np.abs(bias) <= 4 * bias_se + 1e-5), f"{label}: FP32 bias {bias} (se {bias_se})"
 
 
 def test_fp32_difference_is_unbiased_path_noise(ctx):
