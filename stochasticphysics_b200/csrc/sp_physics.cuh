@@ -188,8 +188,6 @@ struct NeelCart {
     static __device__ __forceinline__ void recompute(const Par&, const R*, Cache&) {}
     static __device__ __forceinline__ void finish(const Rot<R>&, R*, const Cache&) {}
     static __device__ __forceinline__ int compensated(const Cache&) { return 0; }  // Neel increments are many ulp
-    static constexpr bool kCharts = false;  // Cartesian: no coordinate rotations
-    static __device__ __forceinline__ bool plain_chart(const Cache&) { return true; }
     static __device__ __forceinline__ void det(const Par& q, const R* y, const Cache&, const R* B, R* a) {
         const V3<R> m = v3(y[0], y[1], y[2]);
         const V3<R> H = heff(q, m, B);
@@ -403,8 +401,6 @@ struct NeelSph {
         else { y[0] = wrap_two_pi(y[0]); y[1] = wrap_two_pi(y[1]); }
     }
     static __device__ __forceinline__ int compensated(const Cache&) { return 0; }
-    static constexpr bool kCharts = true;
-    static __device__ __forceinline__ bool plain_chart(const Cache& c) { return !c.rot; }  // not rotated
     static __device__ __forceinline__ void det(const Par& q, const R*, const Cache& c, const R* B, R* a) {
         const V3<R> H = heff(q, c.md, B);
         a[0] = dot(c.P0, H);
@@ -699,8 +695,6 @@ struct BrownNeelEuler {
     // the Euler angles of the particle (Brown rotation: a few ulp of FP32 angles per step),
     // while their chart is not rotated
     static __device__ __forceinline__ int compensated(const Cache& c) { return c.br ? 0 : 3; }
-    static constexpr bool kCharts = true;
-    static __device__ __forceinline__ bool plain_chart(const Cache& c) { return !c.br && !c.nr; }  // neither rotated
     static __device__ __forceinline__ void finish(const Rot<R>&, R* y, const Cache& c) {
         if (c.br) euler_unrotate(y);
         else { y[0] = wrap_two_pi(y[0]); y[1] = wrap_two_pi(y[1]); y[2] = wrap_two_pi(y[2]); }
@@ -801,8 +795,6 @@ struct BrownNeelCart {
     static __device__ __forceinline__ void recompute(const Par&, const R*, Cache&) {}
     static __device__ __forceinline__ void finish(const Rot<R>&, R*, const Cache&) {}
     static __device__ __forceinline__ int compensated(const Cache&) { return 3; }  // the particle axis n
-    static constexpr bool kCharts = false;
-    static __device__ __forceinline__ bool plain_chart(const Cache&) { return true; }
     // .inl:222-271 (the reference returns zero for cubic anisotropy, .inl:225-229)
     static __device__ __forceinline__ void det(const Par& q, const R* y, const Cache&, const R* B, R* a) {
         if constexpr (A == kCubic) {
@@ -1057,16 +1049,6 @@ struct Stepper {
         if constexpr (kExplicit) {
             Cache c;
             P::prepare_t(q, rot, y, c, tr);
-            // The FP32 form gives the common chart (no coordinate rotation) an inlined copy of
-            // its own, in which every chart branch folds away and the step is straight-line
-            // code the scheduler can interleave; the FP64 form keeps one copy, its step loop
-            // being bound by the instruction cache.
-            if constexpr (P::kCharts && !M<R>::kColdCalls) {
-                if (P::plain_chart(c)) {
-                    explicit_from(q, rot, y, c, B, w, dt, lo);
-                    return;
-                }
-            }
             explicit_from(q, rot, y, c, B, w, dt, lo);
         } else {
             if constexpr (P::kHasJacobian) {
