@@ -233,6 +233,23 @@ def serving_leg(ctx, seconds, rate, step_scale, seed=0x5EED0005, serial_sample=4
     }
 
 
+def plain_fp64_rate(ctx, specs, max_steps):
+    """The plain FP64 drop-in on the given requests one at a time (sp_simulate, FP64, each
+    run cut to at most max_steps integrated steps in whole windows: a long request's rate
+    does not depend on its length): particle-steps/s of the whole sample."""
+    from stochasticphysics_b200._abi import Precision
+    ps, sec = 0, 0.0
+    for s in specs:
+        W = s.oversampling
+        steps = min(s.number_of_steps, (max_steps // W + 1) * W)
+        r = dataclasses.replace(s, precision=Precision.FP64, number_of_steps=steps)
+        t = time.perf_counter()
+        ctx.simulate(r)
+        sec += time.perf_counter() - t
+        ps += r.n * r.integrated_steps
+    return ps / sec
+
+
 def overload_leg(ctx, arrival_s=2.0, observe_s=30.0, rate=50.0, seed=0x5EED0005):
     """The serving workload at its stated size: Poisson arrivals at `rate`/s for `arrival_s`
     seconds of full-length requests (N ~ logU[1e3, 6.4e4], S ~ logU[1e5, 1e7], Neel or
@@ -295,6 +312,7 @@ def overload_leg(ctx, arrival_s=2.0, observe_s=30.0, rate=50.0, seed=0x5EED0005)
                 pass
     completed = sum(work[i] for i in done)
     lat_s = sorted(lat)
+    plain64 = plain_fp64_rate(ctx, specs[:12], 100000)
     return {"requests": len(specs), "arrival_rate_per_s": rate, "arrival_window_s": arrival_s,
             "observe_window_s": observe_s, "wall_s": t_end,
             "offered_particle_steps_per_s": sum(work) / arrival_s,
@@ -303,6 +321,10 @@ def overload_leg(ctx, arrival_s=2.0, observe_s=30.0, rate=50.0, seed=0x5EED0005)
             "p50_ms_completed": float(np.percentile(lat_s, 50)) if lat_s else None,
             "p99_ms_completed": float(np.percentile(lat_s, 99)) if lat_s else None,
             "in_flight_over_time": depth, "memory_budget_bytes": budget,
+            "plain_fp64": {"value": plain64, "unit": UNIT,
+                           "note": "the first 12 requests one at a time through sp_simulate in FP64, each cut "
+                                   "to 1e5 steps"},
+            "served_over_plain_fp64": completed / t_end / plain64,
             "note": "completed_particle_steps counts finished requests only (the cancelled ones' partial "
                     "work is not included), so saturated_value is a lower bound on the integration rate",
             "workload": f"Poisson {rate}/s for {arrival_s} s, full-length requests (step_scale 1.0): "
@@ -337,7 +359,12 @@ def batched_leg(ctx, count, step_scale, seed=0x5EED0004, serial_sample=16):
     for s in sample:
         ctx.simulate(s)
     serial_s = time.perf_counter() - t
+    plain64 = plain_fp64_rate(ctx, sample, 100000)
     return {"sets": count, "value": ps / wall, "unit": UNIT, "wall_s": wall, "particle_steps": ps,
+            "plain_fp64": {"value": plain64, "unit": UNIT, "sets": len(sample),
+                           "note": "the same sampled sets one at a time through sp_simulate in FP64, each cut "
+                                   "to 1e5 steps"},
+            "batched_over_plain_fp64": ps / wall / plain64,
             "step_scale": step_scale,
             "max_latency_ms": max(lat),
             "launch_shapes": {s.solver.name: ctx.launch_config(s) for s in specs[:2]},
@@ -900,6 +927,13 @@ def main():
             "fp64_plain": {"value": v64, "unit": UNIT, "ms_per_step": results["FP64"]["total_ms"] / args.steps,
                            "clocks": results["FP64"]["clocks"]},
             "fp32_over_fp64": v32 / v64,
+            "fp32_served_over_fp64_plain": {
+                "co_scheduled_pair": v32 / v64,
+                "batched_sets": None if not batched else batched["batched_over_plain_fp64"],
+                "serving_overload": None if not overload else overload["served_over_plain_fp64"],
+                "note": "co_scheduled_pair: both forms on the timed workload, launched the same way; "
+                        "batched_sets / serving_overload: the FP32 batched or served run against the same "
+                        "requests one at a time through the plain FP64 kernel"},
             "sequential_ensembles": {"fp32": world * ps_per_step * args.steps / (results["FP32"]["seq_ms"] / 1e3),
                                      "fp64": world * ps_per_step * args.steps / (results["FP64"]["seq_ms"] / 1e3)},
             "fp32_vs_fp64_mean_m": {
