@@ -159,6 +159,20 @@ def profiled_instructions(prefix=""):
     return ((float(m.group(1)), float(h.group(1))) if m and h else None), path.name
 
 
+def profiled_pipes():
+    """FP64-pipe and FP32 FMA-pipe utilisation of the step kernels (ncu
+    sm__pipe_fp64_cycles_active / sm__inst_executed_pipe_fma, pct of peak) from the
+    committed ncu summary, keyed "<precision>_<solver>"."""
+    import re
+    path = ROOT / "profiles" / "step_kernel_brown_neel_euler_65536.md"
+    try:
+        text = path.read_text()
+    except OSError:
+        return None
+    out = {m.group(1): float(m.group(2)) for m in re.finditer(r"pipe_pct_(\w+):\s*([0-9.]+)", text)}
+    return out or None
+
+
 def serving_leg(ctx, seconds, rate, step_scale, seed=0x5EED0005, serial_sample=48, chunk_steps=0):
     """Poisson arrivals of mixed Neel / BrownAndNeelEulerSpherical requests with the
     batched-set distributions and the 2D Lissajous field, served by the continuous-
@@ -953,6 +967,7 @@ def main():
                          "peak_source": "measured in bench.py: FMA-chain kernel on this GPU",
                          "flops_per_particle_step": {"Millstein": flops_step[0], "Heun": flops_step[1]},
                          "fp64": {"achieved": sum(ach64) / 2, "peak": peak64, "frac": (sum(ach64) / 2) / peak64},
+                         "pipe_utilisation_pct": profiled_pipes(),
                          "issue": issue},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "api": "sp_server_submit_many / sp_server_wait: each step's pair submitted (host arrays in) "
