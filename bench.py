@@ -474,13 +474,16 @@ def stiff_leg(ctx, torch, n=262144, timed_steps=2000):
     return out
 
 
-def injected_leg(ctx, torch, n=65536, timed_steps=1000, warm_steps=100):
+def injected_leg(ctx, torch, peaks, rows=((65536, 1000), (1048576, 200)), warm_steps=50):
     """Injection mode (Wiener increments supplied by the caller and read from HBM every
-    step, the parity mode): Neel Cartesian Heun, 65536 particles, FP64 (24 B of dW per
-    particle-step) and FP32 (12 B).  The dW array (steps x 3 x particles) is far larger
-    than L2, so each increment comes from HBM once.  Device-resident, CUDA-event timed
-    after a warm-up chunk; reports particle-steps/s and the dW read rate against the
-    measured HBM copy bandwidth."""
+    step, the parity mode): Neel Cartesian Heun, FP64 (24 B of dW per particle-step) and
+    FP32 (12 B), at the bench's 65536 particles and at 1048576 particles, which fill the
+    GPU's resident warps.  The dW arrays (steps x 3 x particles) are far larger than L2,
+    so each increment comes from HBM once.  Device-resident, CUDA-event timed after a
+    warm-up chunk; reports particle-steps/s, the dW read rate against the measured HBM
+    copy bandwidth, and the ceiling the step's arithmetic puts on that fraction: with F
+    flops per particle-step (FMA = 2) and B bytes of dW, a kernel running at the
+    measured FMA peak P reads at most P B / F bytes/s."""
     from stochasticphysics_b200 import provider
     from stochasticphysics_b200._abi import Precision
 
@@ -491,30 +494,40 @@ def injected_leg(ctx, torch, n=65536, timed_steps=1000, warm_steps=100):
         pass
     if not hbm:  # no measured peaks file: an earlier copy-bandwidth measurement on B200
         hbm, hbm_src = 6650.0, "fallback: 6.65 TB/s, an earlier copy-bandwidth measurement on B200"
-    base = provider.neel_relaxation(n=n, steps=timed_steps + warm_steps + 100, oversampling=100)
-    base = provider.with_injected_noise(base, seed=7)
-    out = {}
+    flops = json.loads((ROOT / "stochasticphysics_b200" / "flops_table.json").read_text())["table"][
+        "Neel/Uniaxial/Heun_Strong"]["flops"]
     st = torch.cuda.Stream()
-    for prec in (Precision.FP64, Precision.FP32):
-        spec = dataclasses.replace(base, precision=prec)
-        with ctx.ensemble(spec) as e:
-            e.advance(warm_steps, st.cuda_stream)
-            torch.cuda.synchronize()
-            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            a.record(st)
-            e.advance(timed_steps, st.cuda_stream)
-            b.record(st)
-            torch.cuda.synchronize()
-        sec = a.elapsed_time(b) / 1e3
-        ps = n * timed_steps / sec
-        dw_bytes = 3 * (8 if prec == Precision.FP64 else 4)
-        gbs = ps * dw_bytes / 1e9
-        out[prec.name] = {"value": ps, "unit": UNIT, "dw_bytes_per_particle_step": dw_bytes, "dw_read_gbs": gbs,
-                          "hbm_frac": None if not hbm else gbs / hbm}
-    out["hbm_peak_gbs"] = hbm
-    out["hbm_peak_source"] = hbm_src
-    out["workload"] = (f"neel_relaxation with injected dW: Neel, Heun, {n} particles, {timed_steps} timed steps "
-                       f"({3 * n * (timed_steps + warm_steps) * 8 / 1e9:.2f} GB of FP64 dW on the device)")
+    out = {"hbm_peak_gbs": hbm, "hbm_peak_source": hbm_src, "flops_per_particle_step": flops, "rows": []}
+    for n, timed_steps in rows:
+        base = provider.neel_relaxation(n=n, steps=timed_steps + warm_steps + 100, oversampling=100)
+        base = provider.with_injected_noise(base, seed=7)
+        row = {"particles": n, "timed_steps": timed_steps,
+               "fp64_dw_gb": 3 * n * base.integrated_steps * 8 / 1e9}
+        for prec in (Precision.FP64, Precision.FP32):
+            with ctx.ensemble(dataclasses.replace(base, precision=prec)) as e:
+                e.advance(warm_steps, st.cuda_stream)
+                torch.cuda.synchronize()
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(st)
+                e.advance(timed_steps, st.cuda_stream)
+                b.record(st)
+                torch.cuda.synchronize()
+            sec = a.elapsed_time(b) / 1e3
+            ps = n * timed_steps / sec
+            dw_bytes = 3 * (8 if prec == Precision.FP64 else 4)
+            gbs = ps * dw_bytes / 1e9
+            peak = peaks[prec.name]
+            ceiling = peak * 1e12 * dw_bytes / flops / 1e9
+            row[prec.name] = {"value": ps, "unit": UNIT, "dw_bytes_per_particle_step": dw_bytes,
+                              "dw_read_gbs": gbs, "hbm_frac": gbs / hbm,
+                              "fma_frac": ps * flops / (peak * 1e12),
+                              "hbm_frac_ceiling_at_fma_peak": min(1.0, ceiling / hbm)}
+        out["rows"].append(row)
+        del base
+    first = out["rows"][0]
+    out["FP64"], out["FP32"] = first["FP64"], first["FP32"]  # the bench workload's size
+    out["workload"] = ("neel_relaxation with injected dW: Neel, Heun, uniaxial; rows at 65536 and 1048576 "
+                       "particles (the first is the FP64/FP32 entry above)")
     return out
 
 
@@ -905,7 +918,7 @@ def main():
             ctx, shards=args.accuracy_shards, steps=args.accuracy_steps)
         merged = merged_shards_check(ctx, torch, dist, world, rank) if world > 1 else None
         stiff = None if (world > 1 or args.no_stiff) else stiff_leg(ctx, torch)
-        injected = None if (world > 1 or args.no_injected) else injected_leg(ctx, torch)
+        injected = None if (world > 1 or args.no_injected) else injected_leg(ctx, torch, {"FP64": peak64, "FP32": peak32})
         sizes = None if (world > 1 or args.no_sizes) else sizes_leg(ctx, torch)
         plain_neel = None if (world > 1 or args.no_cpu_baseline) else plain_neel_leg(ctx, torch)
 
