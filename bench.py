@@ -209,13 +209,14 @@ def serving_leg(ctx, seconds, rate, step_scale, seed=0x5EED0005, serial_sample=4
         th = threading.Thread(target=submitter)
         t_start = time.perf_counter()
         th.start()
-        lat, served = [], []
+        lat, served, phases = [], [], []
         for i in range(len(specs)):
             while ids[i] is None:
                 time.sleep(0.0005)
             res, ms = srv.wait(ids[i])
             lat.append(ms)
             served.append(res.mean)
+            phases.append([res.stats[k] for k in ("queue_ms", "setup_ms", "run_ms", "readback_ms")])
         t_end = time.perf_counter()
         th.join()
     ps = [s.n * s.integrated_steps for s in specs]
@@ -231,10 +232,23 @@ def serving_leg(ctx, seconds, rate, step_scale, seed=0x5EED0005, serial_sample=4
         d = float(np.max(np.abs(served[i][:, cols] - r64.mean[:, cols])))
         errs.append((d, d / math.sqrt(2.0 / (3.0 * specs[i].n))))
     lat_s = sorted(lat)
+    ph = np.array(phases)
+    slowest = np.argsort(lat)[::-1][:max(1, len(lat) // 100)]
+    breakdown = {
+        "p50_ms": {k: float(np.percentile(ph[:, j], 50)) for j, k in enumerate(("queue", "setup", "run", "readback"))},
+        "p99_ms": {k: float(np.percentile(ph[:, j], 99)) for j, k in enumerate(("queue", "setup", "run", "readback"))},
+        "slowest_1pct": [{"latency_ms": float(lat[i]), "queue_ms": float(ph[i, 0]), "setup_ms": float(ph[i, 1]),
+                          "run_ms": float(ph[i, 2]), "readback_ms": float(ph[i, 3]), "particles": int(specs[i].n),
+                          "steps": int(specs[i].integrated_steps), "problem": specs[i].problem.name}
+                         for i in slowest],
+        "note": "server host clock per request: queue = submit -> admission, setup = upload and init, run = the "
+                "rounds until its last window, readback = result copy; run covers the rounds the request shares "
+                "with the others in flight",
+    }
     return {
         "requests": len(specs), "arrival_rate_per_s": rate, "arrival_window_s": seconds,
         "p50_ms": float(np.percentile(lat_s, 50)), "p99_ms": float(np.percentile(lat_s, 99)),
-        "max_ms": float(lat_s[-1]), "value": sum(ps) / (t_end - t_start), "unit": UNIT,
+        "max_ms": float(lat_s[-1]), "latency_breakdown": breakdown, "value": sum(ps) / (t_end - t_start), "unit": UNIT,
         "offered_particle_steps_per_s": sum(ps) / seconds, "memory_budget_bytes": budget,
         "serial_fp64": {"value": sum(ps[i] for i in sample) / serial_s, "unit": UNIT, "requests": len(sample),
                         "note": "same requests one at a time through sp_simulate in FP64 (every k-th request)"},
