@@ -66,6 +66,7 @@ struct DwStream {
     static constexpr int kRow = 32 * static_cast<int>(sizeof(R));
     static constexpr int kStageBytes = kStep * Mn * kRow;
     static_assert(kRow % 16 == 0, "bulk copies move multiples of 16 bytes");
+    static_assert(kStep * Mn <= 32, "one lane issues each row of a stage");
 
     // dynamic shared memory of a CTA of `threads` threads
     static constexpr size_t smem_bytes(int threads) { return static_cast<size_t>(threads / 32) * kStages * kStageBytes; }
