@@ -9,10 +9,12 @@
 // group runs ONE batched launch per chunk over a shared work list of particle
 // tiles (step_kernel reads the tile -> ensemble map), captured once per group
 // membership as a CUDA graph.  Groups run on separate streams so different
-// kernels overlap on the device; a round replays each group's chunk graph a few
-// times, so one group's next chunk fills the SMs another's draining chunk frees.
-// Finished ensembles are read back and freed at the next round boundary, which
-// makes room for queued requests.
+// kernels overlap on the device, each at its own pace: a group's round replays
+// its chunk graph a few times, and when it ends (an event the scheduler polls)
+// the group's finished ensembles are read back and freed, queued requests join,
+// and its next round starts while the other groups' rounds are still running.
+// One group's next chunk thus fills the SMs another's draining chunk frees, and
+// no group waits for a slower one at a round boundary.
 //
 // Every particle's arithmetic, noise stream and per-warp reduction order are
 // independent of which other ensembles share the launch, so a request's
@@ -66,7 +68,10 @@ struct Group {
     cudaStream_t stream = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t gexec = nullptr;
+    cudaEvent_t round_end = nullptr;  // recorded after the group's current round
     bool dirty = true;
+    bool running = false;              // a round is in flight on `stream`
+    unsigned long long round_launches = 0;  // chunk launches of the round in flight
 
     void release() {
         if (gexec) cudaGraphExecDestroy(gexec);
@@ -100,8 +105,8 @@ struct sp_server {
                (d.noise == SP_NOISE_INJECTED);
     }
 
-    // Requests join and leave a group only between rounds, so the round bounds how long a
-    // new request waits behind a running group: cfg.chunk_steps steps, or else the tuned
+    // Requests join and leave a group only between its rounds, so the round bounds how long
+    // a new request waits behind a running group of its key: cfg.chunk_steps steps, or else the tuned
     // (throughput) chunk capped at kServeChunk steps, in whole windows.  A round runs as
     // chunk launches of at most kSliceSteps (whole windows where a window fits): each
     // launch ends with its CTAs draining, and with several groups in flight the others'
@@ -243,6 +248,38 @@ struct sp_server {
         g.dirty = false;
     }
 
+    // waits for every round in flight (stop, or an error that fails every request)
+    void drain() {
+        for (auto& kv : groups) {
+            if (kv.second.running && kv.second.stream) cudaStreamSynchronize(kv.second.stream);
+            kv.second.running = false;
+        }
+    }
+
+    // Polls until a running group ends its round (appended to `ended`), an idle group has
+    // members to start, or the server stops; queued requests are admitted (uploaded) while
+    // the rounds run.
+    void wait_round(std::vector<Group*>& ended) {
+        for (;;) {
+            for (auto& kv : groups) {
+                Group& g = kv.second;
+                if (!g.running) continue;
+                const cudaError_t q = cudaEventQuery(g.round_end);
+                if (q == cudaSuccess) ended.push_back(&g);
+                else if (q != cudaErrorNotReady) check_cuda(q, "round");
+            }
+            if (!ended.empty()) return;
+            {
+                std::lock_guard<std::mutex> lk(mu);
+                admit_locked();
+                if (stop) return;
+                for (const auto& kv : groups)
+                    if (!kv.second.running && !kv.second.members.empty()) return;
+            }
+            std::this_thread::sleep_for(std::chrono::microseconds(50));
+        }
+    }
+
     void run() {
         check_cuda(cudaSetDevice(ctx->device), "cudaSetDevice");
         for (;;) {
@@ -250,27 +287,31 @@ struct sp_server {
                 std::unique_lock<std::mutex> lk(mu);
                 for (;;) {
                     admit_locked();
-                    if (stop) return;
+                    if (stop) {
+                        drain();
+                        return;
+                    }
                     if (!active.empty()) break;
                     cv_work.wait(lk);
                 }
             }
+            std::vector<Group*> ended;
             try {
-                // one round for every group: its chunk graph chunks_per_round times, the
-                // groups' launches interleaved and the longest group first, so the others'
-                // CTAs fill the SMs it leaves free instead of it running alone at the end.
-                // Length = particle-steps of the round over the key's tuned rate (the
-                // particle-steps alone while any key is untuned).
+                // a round for every idle group with members: its chunk graph chunks_per_round
+                // times on its own stream.  Groups that start together go longest first
+                // (particle-steps of the round over the key's tuned rate; particle-steps alone
+                // while any key is untuned), so the others' CTAs fill the SMs it leaves free
+                // instead of it running alone at the end.
                 std::vector<std::pair<double, Group*>> order;
                 bool all_tuned = true;
                 for (auto& kv : groups)
-                    if (!kv.second.members.empty() && tuned_rate(kv.second.members.front()->desc) <= 0.0) all_tuned = false;
-                unsigned long long launches = 0;
+                    if (!kv.second.running && !kv.second.members.empty() &&
+                        tuned_rate(kv.second.members.front()->desc) <= 0.0)
+                        all_tuned = false;
                 for (auto& kv : groups) {
                     Group& g = kv.second;
-                    if (g.members.empty()) continue;
+                    if (g.running || g.members.empty()) continue;
                     if (g.dirty) rebuild(g);
-                    launches = std::max(launches, g.chunks_per_round);
                     double work = 0.0;
                     for (Request* r : g.members) {
                         const Ensemble* e = r->ens.get();
@@ -280,8 +321,16 @@ struct sp_server {
                     order.emplace_back(all_tuned ? work / tuned_rate(g.members.front()->desc) : work, &g);
                 }
                 std::stable_sort(order.begin(), order.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
-                for (auto& og : order)
-                    for (Request* r : og.second->members) r->in_round = true;
+                unsigned long long launches = 0;
+                for (auto& og : order) launches = std::max(launches, og.second->chunks_per_round);
+                for (auto& og : order) {
+                    Group& g = *og.second;
+                    for (Request* r : g.members) r->in_round = true;
+                    if (!g.round_end)
+                        check_cuda(cudaEventCreateWithFlags(&g.round_end, cudaEventDisableTiming), "round event");
+                    g.round_launches = g.chunks_per_round;
+                    g.running = true;
+                }
                 for (unsigned long long j = 0; j < launches; ++j)
                     for (auto& og : order) {
                         Group& g = *og.second;
@@ -289,15 +338,11 @@ struct sp_server {
                         check_cuda(cudaGraphLaunch(g.gexec, g.stream), "graph launch");
                         g_launch_count += 5;
                     }
-                {
-                    // requests that arrived meanwhile are uploaded while the round runs and
-                    // join at the next one
-                    std::lock_guard<std::mutex> lk(mu);
-                    admit_locked();
-                }
-                for (auto& og : order) check_cuda(cudaStreamSynchronize(og.second->stream), "chunk");
+                for (auto& og : order) check_cuda(cudaEventRecord(og.second->round_end, og.second->stream), "round event");
+                wait_round(ended);
             } catch (const Error& e) {
                 std::lock_guard<std::mutex> lk(mu);
+                drain();
                 for (Request* r : active) { r->ens.reset(); finish(r, SP_REQUEST_FAILED, e.status, e.what()); }
                 active.clear();
                 used_bytes = 0;
@@ -305,24 +350,24 @@ struct sp_server {
                 cv_done.notify_all();
                 continue;
             }
-            // host mirror of the device counters; retire finished or cancelled ensembles
+            // host mirror of the device counters of the groups whose round ended; retire
+            // their finished or cancelled ensembles
             std::lock_guard<std::mutex> lk(mu);
-            std::vector<Request*> still;
-            for (Request* r : active) {
-                if (!r->in_round) {
-                    still.push_back(r);
-                    continue;
-                }
-                r->in_round = false;
-                Ensemble* e = r->ens.get();
-                // each launch advances the ensemble by min(chunk, steps left) (bump, commit)
-                const unsigned long long nl = groups[key_of(r->desc)].chunks_per_round;
-                const unsigned long long step = std::min(nl * e->L.chunk, e->L.S - e->steps_done);
-                e->steps_done += step;
-                e->particle_steps += step * e->L.n;
-                e->launches += 5 * nl;
-                const bool done = e->steps_done >= e->L.S;
-                if (done || r->cancel) {
+            for (Group* g : ended) {
+                g->running = false;
+                const std::vector<Request*> members = g->members;  // retiring edits g->members
+                for (Request* r : members) {
+                    if (!r->in_round) continue;  // admitted during the round: joins the next one
+                    r->in_round = false;
+                    Ensemble* e = r->ens.get();
+                    // each launch advances the ensemble by min(chunk, steps left) (bump, commit)
+                    const unsigned long long nl = g->round_launches;
+                    const unsigned long long step = std::min(nl * e->L.chunk, e->L.S - e->steps_done);
+                    e->steps_done += step;
+                    e->particle_steps += step * e->L.n;
+                    e->launches += 5 * nl;
+                    const bool done = e->steps_done >= e->L.S;
+                    if (!done && !r->cancel) continue;
                     r->t_run_end = Clock::now();
                     try {
                         if (done) retire(r);
@@ -334,14 +379,11 @@ struct sp_server {
                         finish(r, SP_REQUEST_FAILED, ex.status, ex.what());
                     }
                     used_bytes -= r->bytes;
-                    Group& g = groups[key_of(r->desc)];
-                    g.members.erase(std::find(g.members.begin(), g.members.end(), r));
-                    g.dirty = true;
-                } else {
-                    still.push_back(r);
+                    g->members.erase(std::find(g->members.begin(), g->members.end(), r));
+                    g->dirty = true;
+                    active.erase(std::find(active.begin(), active.end(), r));
                 }
             }
-            active.swap(still);
             cv_done.notify_all();
         }
     }
@@ -546,6 +588,7 @@ sp_status sp_server_destroy(sp_server* s) {
     for (Request* r : s->active) r->ens.reset();
     for (auto& kv : s->groups) {
         kv.second.release();
+        if (kv.second.round_end) cudaEventDestroy(kv.second.round_end);
         if (kv.second.stream) cudaStreamDestroy(kv.second.stream);
     }
     delete s;
