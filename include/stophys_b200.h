@@ -357,11 +357,14 @@ SP_API sp_status sp_ensemble_footprint(const sp_ensemble_desc* desc, uint64_t* b
 typedef struct sp_server_config {
     uint64_t memory_budget_bytes; /* admission limit on device bytes of admitted requests */
     uint64_t chunk_steps;         /* steps per scheduling round; 0 = the tuned chunk
-                                     capped at 4000 steps (whole windows): requests join
-                                     and leave only between rounds, so the round bounds
-                                     how long a new request waits behind running ones.
-                                     A round runs as chunk launches of at most 1000
-                                     steps (whole windows where a window fits)           */
+                                     capped at 4000 steps (whole windows).  Admitted
+                                     requests are grouped by kernel; each group runs its
+                                     rounds on its own stream at its own pace, and
+                                     requests join and leave a group only between its
+                                     rounds, so the round bounds how long a new request
+                                     waits behind running ones of its kind.  A round runs
+                                     as chunk launches of at most 1000 steps (whole
+                                     windows where a window fits)                        */
     int32_t max_active;           /* cap on concurrently admitted requests (0 = none)     */
     int32_t reserved;
 } sp_server_config;
