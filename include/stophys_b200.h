@@ -34,7 +34,7 @@
 extern "C" {
 #endif
 
-#define SP_ABI_VERSION 8u
+#define SP_ABI_VERSION 9u
 
 #if defined(_WIN32)
 #define SP_API __declspec(dllexport)
@@ -359,14 +359,19 @@ typedef struct sp_server_config {
     uint64_t chunk_steps;         /* steps per scheduling round; 0 = the tuned chunk
                                      capped at 4000 steps (whole windows).  Admitted
                                      requests are grouped by kernel; each group runs its
-                                     rounds on its own stream at its own pace, and
+                                     rounds on its own stream at its own pace;
                                      requests join and leave a group only between its
-                                     rounds, so the round bounds how long a new request
-                                     waits behind running ones of its kind.  A round runs
-                                     as chunk launches of at most 1000 steps (whole
-                                     windows where a window fits)                        */
+                                     rounds (a request whose kind's group is mid-round
+                                     starts a second group of its kind), so the round
+                                     bounds how long a request that finishes mid-round
+                                     waits to be read back.  A round runs as chunk
+                                     launches of at most 1000 steps (whole windows where
+                                     a window fits)                                      */
     int32_t max_active;           /* cap on concurrently admitted requests (0 = none)     */
-    int32_t reserved;
+    int32_t groups_per_kind;      /* (ABI 9) groups of one kernel kind that may run at
+                                     once (0 = 2): a request whose kind has that many
+                                     groups mid-round joins the least full at its next
+                                     round; below the cap it starts a group at once     */
 } sp_server_config;
 
 typedef enum sp_request_state {

@@ -13,7 +13,7 @@ from typing import Optional
 
 import numpy as np
 
-ABI_VERSION = 8
+ABI_VERSION = 9
 
 
 class Status(IntEnum):
@@ -243,7 +243,7 @@ class sp_server_config(C.Structure):
         ("memory_budget_bytes", C.c_uint64),
         ("chunk_steps", C.c_uint64),
         ("max_active", C.c_int32),
-        ("reserved", C.c_int32),
+        ("groups_per_kind", C.c_int32),
     ]
 
 

@@ -8,8 +8,10 @@
 // kernel key (problem, anisotropy, solver, precision, noise mode) and each
 // group runs ONE batched launch per chunk over a shared work list of particle
 // tiles (step_kernel reads the tile -> ensemble map), captured once per group
-// membership as a CUDA graph.  Groups run on separate streams so different
-// kernels overlap on the device, each at its own pace: a group's round replays
+// membership as a CUDA graph.  A request joins an idle group of its key; when
+// its key's group is mid-round it starts a second group of that key at once.
+// Groups run on separate streams so different kernels overlap on the device,
+// each at its own pace: a group's round replays
 // its chunk graph a few times, and when it ends (an event the scheduler polls)
 // the group's finished ensembles are read back and freed, queued requests join,
 // and its next round starts while the other groups' rounds are still running.
@@ -24,7 +26,6 @@
 #include <condition_variable>
 #include <cstring>
 #include <deque>
-#include <map>
 #include <memory>
 #include <mutex>
 #include <thread>
@@ -58,6 +59,7 @@ struct Request {
 };
 
 struct Group {
+    int key = -1;  // kernel key of its members
     const KernelSet* ks = nullptr;
     std::vector<Request*> members;
     EnsDev* d_ens = nullptr;
@@ -98,18 +100,19 @@ struct sp_server {
     std::deque<Request*> queue;
     std::vector<Request*> active;
     std::unordered_map<uint64_t, std::unique_ptr<Request>> all;
-    std::map<int, Group> groups;  // key -> group
+    std::vector<std::unique_ptr<Group>> groups;  // several may share a kernel key
 
     static int key_of(const sp_ensemble_desc& d) {
         return (((d.problem * kAnisoSlots + d.anisotropy) * kSolverSlots + solver_slot(d.solver, d.jacobian)) * 2 + d.precision) * 2 +
                (d.noise == SP_NOISE_INJECTED);
     }
 
-    // Requests join and leave a group only between its rounds, so the round bounds how long
-    // a new request waits behind a running group of its key: cfg.chunk_steps steps, or else the tuned
-    // (throughput) chunk capped at kServeChunk steps, in whole windows.  A round runs as
-    // chunk launches of at most kSliceSteps (whole windows where a window fits): each
-    // launch ends with its CTAs draining, and with several groups in flight the others'
+    // Requests join and leave a group only between its rounds (a new request whose key's
+    // group is mid-round starts a second group of that key, group_for), so the round bounds how long a
+    // request that finishes or is cancelled mid-round waits to be read back: cfg.chunk_steps
+    // steps, or else the tuned (throughput) chunk capped at kServeChunk steps, in whole
+    // windows.  A round runs as chunk launches of at most kSliceSteps (whole windows where a
+    // window fits): each launch ends with its CTAs draining, and with several groups in flight the others'
     // next launches fill the SMs so freed (two 65536-particle Brown+Neel ensembles run
     // 15 % faster in 1000-step launches than in 10000-step ones).
     static constexpr unsigned long long kServeChunk = 4000;
@@ -165,6 +168,37 @@ struct sp_server {
         }
     }
 
+    // The group a newly admitted request of kernel key `key` joins: an idle group of that
+    // key (its next round starts at once); else, while the key has fewer than
+    // kGroupsPerKey groups, a group of its own (an idle empty group or a new one), so a
+    // request arriving while its key's group is mid-round starts at once instead of
+    // waiting for that round to end; else the key's running group with the fewest members,
+    // joining at its next round.  The cap (sp_server_config.groups_per_kind, default
+    // kGroupsPerKey) keeps a burst of arrivals batched in few launches.
+    static constexpr int kGroupsPerKey = 2;
+    Group& group_for(int key) {
+        Group* empty = nullptr;
+        Group* least_full = nullptr;
+        int of_key = 0;
+        for (auto& gp : groups) {
+            if (gp->key == key && !gp->members.empty()) {
+                if (!gp->running) return *gp;
+                ++of_key;
+                if (!least_full || gp->members.size() < least_full->members.size()) least_full = gp.get();
+            } else if (!gp->running && gp->members.empty() && (!empty || gp->key == key)) {
+                empty = gp.get();
+            }
+        }
+        if (of_key >= (cfg.groups_per_kind > 0 ? cfg.groups_per_kind : kGroupsPerKey)) return *least_full;
+        if (!empty) {
+            groups.push_back(std::make_unique<Group>());
+            empty = groups.back().get();
+        }
+        empty->key = key;
+        empty->dirty = true;
+        return *empty;
+    }
+
     void admit_locked() {
         while (!queue.empty()) {
             Request* r = queue.front();
@@ -189,7 +223,7 @@ struct sp_server {
                 r->state = SP_REQUEST_RUNNING;
                 used_bytes += r->bytes;
                 active.push_back(r);
-                Group& g = groups[key_of(r->desc)];
+                Group& g = group_for(key_of(r->desc));
                 g.members.push_back(r);
                 g.dirty = true;
             } catch (const Error& e) {
@@ -250,9 +284,9 @@ struct sp_server {
 
     // waits for every round in flight (stop, or an error that fails every request)
     void drain() {
-        for (auto& kv : groups) {
-            if (kv.second.running && kv.second.stream) cudaStreamSynchronize(kv.second.stream);
-            kv.second.running = false;
+        for (auto& gp : groups) {
+            if (gp->running && gp->stream) cudaStreamSynchronize(gp->stream);
+            gp->running = false;
         }
     }
 
@@ -261,8 +295,8 @@ struct sp_server {
     // the rounds run.
     void wait_round(std::vector<Group*>& ended) {
         for (;;) {
-            for (auto& kv : groups) {
-                Group& g = kv.second;
+            for (auto& gp : groups) {
+                Group& g = *gp;
                 if (!g.running) continue;
                 const cudaError_t q = cudaEventQuery(g.round_end);
                 if (q == cudaSuccess) ended.push_back(&g);
@@ -273,8 +307,8 @@ struct sp_server {
                 std::lock_guard<std::mutex> lk(mu);
                 admit_locked();
                 if (stop) return;
-                for (const auto& kv : groups)
-                    if (!kv.second.running && !kv.second.members.empty()) return;
+                for (const auto& gp : groups)
+                    if (!gp->running && !gp->members.empty()) return;
             }
             std::this_thread::sleep_for(std::chrono::microseconds(50));
         }
@@ -304,12 +338,11 @@ struct sp_server {
                 // instead of it running alone at the end.
                 std::vector<std::pair<double, Group*>> order;
                 bool all_tuned = true;
-                for (auto& kv : groups)
-                    if (!kv.second.running && !kv.second.members.empty() &&
-                        tuned_rate(kv.second.members.front()->desc) <= 0.0)
+                for (const auto& gp : groups)
+                    if (!gp->running && !gp->members.empty() && tuned_rate(gp->members.front()->desc) <= 0.0)
                         all_tuned = false;
-                for (auto& kv : groups) {
-                    Group& g = kv.second;
+                for (auto& gp : groups) {
+                    Group& g = *gp;
                     if (g.running || g.members.empty()) continue;
                     if (g.dirty) rebuild(g);
                     double work = 0.0;
@@ -346,7 +379,7 @@ struct sp_server {
                 for (Request* r : active) { r->ens.reset(); finish(r, SP_REQUEST_FAILED, e.status, e.what()); }
                 active.clear();
                 used_bytes = 0;
-                for (auto& kv : groups) { kv.second.members.clear(); kv.second.release(); }
+                for (auto& gp : groups) { gp->members.clear(); gp->release(); }
                 cv_done.notify_all();
                 continue;
             }
@@ -443,6 +476,7 @@ extern "C" {
 sp_status sp_server_create(sp_context* ctx, const sp_server_config* cfg, sp_server** out) {
     SP_GUARD_BEGIN
     if (!ctx || !out) return fail(SP_ERR_INVALID_ARG, "NULL argument");
+    if (cfg && cfg->groups_per_kind < 0) return fail(SP_ERR_INVALID_ARG, "groups_per_kind must be >= 0");
     auto* s = new sp_server();
     s->ctx = ctx;
     if (cfg) s->cfg = *cfg;
@@ -586,10 +620,10 @@ sp_status sp_server_destroy(sp_server* s) {
     if (s->worker.joinable()) s->worker.join();
     cudaSetDevice(s->ctx->device);
     for (Request* r : s->active) r->ens.reset();
-    for (auto& kv : s->groups) {
-        kv.second.release();
-        if (kv.second.round_end) cudaEventDestroy(kv.second.round_end);
-        if (kv.second.stream) cudaStreamDestroy(kv.second.stream);
+    for (auto& gp : s->groups) {
+        gp->release();
+        if (gp->round_end) cudaEventDestroy(gp->round_end);
+        if (gp->stream) cudaStreamDestroy(gp->stream);
     }
     delete s;
     return SP_OK;

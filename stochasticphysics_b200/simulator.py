@@ -222,13 +222,15 @@ class DeviceEnsemble:
 class Server:
     """Continuous-batching server (sp_server_*): submit at any time, wait for results."""
 
-    def __init__(self, ctx: Context, memory_budget_bytes: int = 0, chunk_steps: int = 0, max_active: int = 0):
+    def __init__(self, ctx: Context, memory_budget_bytes: int = 0, chunk_steps: int = 0, max_active: int = 0,
+                 groups_per_kind: int = 0):
         self.ctx = ctx
         self._lib = ctx._lib
         cfg = sp_server_config()
         cfg.memory_budget_bytes = int(memory_budget_bytes)
         cfg.chunk_steps = int(chunk_steps)
         cfg.max_active = int(max_active)
+        cfg.groups_per_kind = int(groups_per_kind)
         h = C.c_void_p()
         check(self._lib.sp_server_create(ctx.handle, C.byref(cfg), C.byref(h)))
         self.handle = h
