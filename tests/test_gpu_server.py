@@ -93,3 +93,27 @@ def test_submit_many_queues_all_or_nothing(ctx):
         with pytest.raises(sp.SPError, match="request 1") as e:
             srv.submit_many([small(n=100), small(n=200000)])
         assert e.value.status == Status.ADMISSION_REFUSED
+
+
+@pytest.mark.parametrize("groups_per_kind", [1, 2, 3])
+def test_groups_per_kind_leave_results_unchanged(ctx, groups_per_kind):
+    """Requests of one kind arriving while that kind's group is mid-round either start a
+    group of their own or join a running one at its next round (sp_server_config.
+    groups_per_kind); each result is bit-identical to the request run alone."""
+    import time
+    specs = [small(n=3000 + 500 * i, steps=40000, seed=10 + i) for i in range(4)]
+    with sp.Server(ctx, chunk_steps=2000, groups_per_kind=groups_per_kind) as srv:
+        ids = []
+        for s in specs:
+            ids.append(srv.submit(s))
+            time.sleep(0.003)  # the earlier requests' groups are mid-round
+        got = [srv.wait(i)[0] for i in ids]
+    for s, r in zip(specs, got):
+        np.testing.assert_array_equal(r.mean, ctx.simulate(s).mean)
+        np.testing.assert_array_equal(r.weight, ctx.simulate(s).weight)
+
+
+def test_negative_groups_per_kind_is_refused(ctx):
+    with pytest.raises(sp.SPError) as ei:
+        sp.Server(ctx, groups_per_kind=-1)
+    assert ei.value.status == Status.INVALID_ARG
