@@ -22,6 +22,9 @@ struct KernelSet {
     // default limit: call prepare() with the device current before the first launch
     size_t (*dyn_smem)(int threads) = nullptr;
     void (*prepare)() = nullptr;
+    // injected-noise sets of solvers with one draw per step: the pregenerated-noise kernel
+    // (the chunk's increments as the in-kernel path draws them) over `grid` x n_ens CTAs
+    void (*noise)(const EnsDev* e, int n_ens, int grid, cudaStream_t s) = nullptr;
 };
 
 // index: problem, anisotropy, solver slot (see solver_slot),

@@ -33,6 +33,10 @@ void prepare_inj_t() {
         done[dev] = true;
 }
 template <int PROB, class R, int A>
+void launch_noise_t(const EnsDev* e, int n_ens, int grid, cudaStream_t s) {
+    noise_chunk_kernel<PROB, R, A><<<dim3(static_cast<unsigned>(grid), static_cast<unsigned>(n_ens)), 256, 0, s>>>(e);
+}
+template <int PROB, class R, int A>
 void launch_init_t(const EnsDev* e, const RawParticles& rp, unsigned long long Np, cudaStream_t s) {
     init_kernel<PROB, R, A><<<static_cast<unsigned>(Np / kPad), kPad, 0, s>>>(e, rp);
 }
@@ -69,6 +73,7 @@ KernelSet make_set() {
         if constexpr (INJ) {
             k.dyn_smem = &inj_smem_t<PROB, R, A>;
             k.prepare = &prepare_inj_t<PROB, R, A, SOLVER>;
+            k.noise = &launch_noise_t<PROB, R, A>;
         }
         k.reduce = &launch_reduce_t<Prob::OUT>;
         k.field = &launch_field_chunk_t<R>;

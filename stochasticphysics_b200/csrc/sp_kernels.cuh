@@ -405,7 +405,7 @@ __global__ void __launch_bounds__(kMaxBlock / PPT, (step_min_blocks<PROB, R, SOL
         // injected increments stream from HBM: the warp's rows of the tile's first steps go
         // in flight now (the warp's 32 particles start at the tile's first + 32 warp)
         if constexpr (INJECT)
-            dws.begin(static_cast<const R*>(e.dw), Np, td.first + (threadIdx.x & ~31u), s0, nsteps);
+            dws.begin(static_cast<const R*>(e.dw), Np, td.first + (threadIdx.x & ~31u), e.dw_chunk ? 0ull : s0, nsteps);
 
         for (unsigned long long t0 = 0; t0 < nsteps; t0 += FT) {
             const int len = static_cast<int>(min(static_cast<unsigned long long>(FT), nsteps - t0));
@@ -576,6 +576,32 @@ __global__ void field_chunk_kernel(const EnsDev* __restrict__ ensembles, int mid
     field_eval(e.field, t, B);
     R* f = static_cast<R*>(e.ftab) + 3 * i;
     f[0] = static_cast<R>(B[0]); f[1] = static_cast<R>(B[1]); f[2] = static_cast<R>(B[2]);
+}
+
+// Pregenerated noise: the Wiener increments of the current chunk of each ensemble
+// (grid.y = ensemble), drawn exactly as the in-kernel path draws them (philox_increments:
+// the same Philox counters and the same arithmetic), into dw [chunk][Mn][Np]; the
+// injected step kernel then reads them instead of drawing them on its own step chain.
+// One thread per (step, particle), particles fastest (coalesced stores).
+template <int PROB, class R, int A>
+__global__ void __launch_bounds__(256) noise_chunk_kernel(const EnsDev* __restrict__ ensembles) {
+    using Prob = typename ProblemOf<PROB, R, A>::type;
+    constexpr int Mn = Prob::Mn;
+    const EnsDev& e = ensembles[blockIdx.y];
+    const unsigned long long s0 = e.ctl->step_done, tgt = e.ctl->step_target;
+    const unsigned long long nsteps = tgt > s0 ? min(e.chunk, tgt - s0) : 0ull;
+    const unsigned long long n = e.n, Np = e.Np, total = nsteps * n;
+    R* const dw = static_cast<R*>(e.dw);
+    const R sqdt = static_cast<R>(e.sqrt_dt);
+    const R m2dt = static_cast<R>(-2.0 * e.dt);
+    for (unsigned long long i = static_cast<unsigned long long>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
+         i += static_cast<unsigned long long>(gridDim.x) * blockDim.x) {
+        const unsigned long long j = i / n, p = i - j * n;
+        R w[Mn];
+        philox_increments<R, Mn, Prob::kCalledMath>(e.seed, e.pid_offset + p, s0 + j, sqdt, m2dt, w);
+#pragma unroll
+        for (int m = 0; m < Mn; ++m) dw[(j * Mn + m) * Np + p] = w[m];
+    }
 }
 
 template <class R, int Mn>

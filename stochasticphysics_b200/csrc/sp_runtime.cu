@@ -185,12 +185,37 @@ void* Ensemble::dalloc(size_t bytes) {
     return p;
 }
 
-Ensemble::Ensemble(sp_context* c, const sp_ensemble_desc& d, const LaunchConfig& lc, bool chunk_graph)
+// Pregenerated noise.  A small ensemble leaves most SMs idle and each step's time is the
+// latency of one thread's step chain, of which the FP64 Philox draw and Box-Muller (double
+// log, sqrt and sincospi) are about half (Neel Heun, 1024 particles: 0.94 us per step with
+// in-kernel noise, 0.43 with the increments read from memory).  With at most one warp per
+// SM scheduler, an FP64 ensemble with in-kernel noise therefore draws each chunk's
+// increments in a separate, fully parallel kernel (the same Philox counters and
+// arithmetic, so the results are bit-identical) into a chunk-sized buffer that the
+// injected step kernel stages like caller-supplied increments.
+constexpr unsigned long long kPregenWarpsPerSM = 4;
+constexpr unsigned long long kPregenBytes = 256ull << 20;  // cap on the chunk's increments buffer
+
+static bool pregen_wanted(const sp_context* ctx, const sp_ensemble_desc& d) {
+    if (d.noise != SP_NOISE_PHILOX || d.precision != SP_PRECISION_FP64) return false;
+    if (d.n_particles > kPregenWarpsPerSM * 32ull * static_cast<unsigned long long>(ctx->sms)) return false;
+    const KernelSet& inj = kernel_set(d.problem, d.anisotropy, solver_slot(d.solver, d.jacobian), d.precision, 1);
+    return inj.valid && inj.noise;
+}
+
+Ensemble::Ensemble(sp_context* c, const sp_ensemble_desc& d, const LaunchConfig& lc, bool chunk_graph, bool pregen_ok)
     : ctx(c), desc(d), launch(lc) {
+    pregen = pregen_ok && pregen_wanted(c, d);
     ks = &kernel_set(d.problem, d.anisotropy, solver_slot(d.solver, d.jacobian), d.precision,
-                     d.noise == SP_NOISE_INJECTED ? 1 : 0);
+                     (d.noise == SP_NOISE_INJECTED || pregen) ? 1 : 0);
     if (!ks->valid) throw Error(SP_ERR_UNSUPPORTED_COMBO, "no kernel for this problem/solver combination");
-    L = layout_of(d, lc);
+    if (pregen) {  // the chunk's increments buffer stays within kPregenBytes
+        const unsigned long long row = static_cast<unsigned long long>(noise_dim(d.problem)) *
+                                       round_up(d.n_particles, kPad) * 8ull;
+        launch.chunk = std::max<unsigned long long>(1, std::min(launch.chunk, kPregenBytes / row));
+    }
+    L = layout_of(d, launch);
+    if (pregen) L.bytes += L.chunk * L.Mn * L.Np * L.real;
     check_cuda(cudaSetDevice(ctx->device), "cudaSetDevice");
     check_cuda(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
     check_cuda(cudaEventCreate(&ev0), "cudaEventCreate");
@@ -217,6 +242,7 @@ Ensemble::Ensemble(sp_context* c, const sp_ensemble_desc& d, const LaunchConfig&
     check_cuda(cudaMemsetAsync(d_msum, 0, L.K * L.OUT * 8, stream), "memset");
     check_cuda(cudaMemsetAsync(d_ctl, 0, sizeof(EnsCtl), stream), "memset");
 
+    if (pregen) d_dw = dalloc(L.chunk * L.Mn * L.Np * R);  // [chunk][M][Np], written per chunk
     // injected increments: [S][M][n] FP64 host -> [S][M][Np] Real device
     if (d.noise == SP_NOISE_INJECTED && L.S > 0) {
         d_dw = dalloc(L.S * L.Mn * L.Np * R);
@@ -259,7 +285,7 @@ Ensemble::Ensemble(sp_context* c, const sp_ensemble_desc& d, const LaunchConfig&
     }
     e.slots = L.slots;
     e.state = d_state; e.ksum = d_ksum; e.kcomp = d_kcomp; e.slo = d_slo; e.params = d_params; e.moment = d_moment;
-    e.dw = d_dw; e.partial = d_partial; e.msum = d_msum; e.wsum = d_wsum; e.traj = d_traj; e.ftab = d_ftab;
+    e.dw = d_dw; e.dw_chunk = pregen ? 1 : 0; e.partial = d_partial; e.msum = d_msum; e.wsum = d_wsum; e.traj = d_traj; e.ftab = d_ftab;
     e.traj_stride = traj_stride ? traj_stride : 1; e.traj_n = traj_n;
     e.status = d_status; e.ctl = d_ctl;
     check_cuda(cudaMemcpyAsync(d_ens, &e, sizeof(EnsDev), cudaMemcpyHostToDevice, stream), "upload EnsDev");
@@ -274,6 +300,9 @@ Ensemble::Ensemble(sp_context* c, const sp_ensemble_desc& d, const LaunchConfig&
                "upload tiles");
     ppt = usable_ppt(*ks, launch.ppt, block);
     grid = ntiles;
+    if (pregen)
+        noise_grid = static_cast<int>(std::min<unsigned long long>((L.chunk * L.n + 255) / 256,
+                                                                   8ull * static_cast<unsigned long long>(ctx->sms)));
     if (ks->prepare) ks->prepare();
     if (launch.persistent) {
         int per_sm = 0;
@@ -400,6 +429,7 @@ void Ensemble::upload_and_init(const sp_ensemble_desc& d) {
 void Ensemble::enqueue_chunk(cudaStream_t s) {
     const int midpoint = desc.solver == SP_SOLVER_IMPLICIT_MIDPOINT ? 1 : 0;
     ks->field(d_ens, 1, L.chunk, midpoint, s);
+    if (pregen) ks->noise(d_ens, 1, noise_grid, s);
     ks->step[ppt - 1](d_ens, d_tiles, ntiles, grid, block, s);
     ks->reduce(d_ens, 1, L.slots, 0, s);
     launch_commit(d_ens, 1, s);
@@ -429,8 +459,9 @@ void Ensemble::advance(unsigned long long nsteps, cudaStream_t s) {
     for (unsigned long long i = 0; i < nchunks; ++i) check_cuda(cudaGraphLaunch(gexec, s), "graph launch");
     check_cuda(cudaEventRecord(ev1, s), "event");
     pending_timing = true;
-    launches += 1 + 4 * nchunks;
-    g_launch_count += 1 + 4 * nchunks;
+    const unsigned long long per_chunk = pregen ? 5 : 4;
+    launches += 1 + per_chunk * nchunks;
+    g_launch_count += 1 + per_chunk * nchunks;
     particle_steps += (target - steps_done) * L.n;
     steps_done = target;
     last_stream = s;

@@ -99,6 +99,8 @@ struct Ensemble {
     unsigned long long launches = 0, particle_steps = 0, steps_done = 0;
     unsigned long long h2d_bytes = 0, d2h_bytes = 0;
     int block = 128, grid = 1, ntiles = 0, ppt = 1;
+    bool pregen = false;  // pregenerated noise: a noise kernel per chunk, the injected step kernel
+    int noise_grid = 1;
     unsigned long long traj_stride = 0, traj_n = 0;  // recorded particles: every traj_stride-th, traj_n of them
     EnsDev hdev;
     void *d_state = nullptr, *d_ksum = nullptr, *d_kcomp = nullptr, *d_slo = nullptr, *d_params = nullptr, *d_dw = nullptr,
@@ -112,8 +114,11 @@ struct Ensemble {
     std::vector<void*> allocs;
 
     // chunk_graph: capture the ensemble's own chunk graph now (the server launches its
-    // groups' graphs instead and passes false; advance() then captures it on first use)
-    Ensemble(sp_context* c, const sp_ensemble_desc& d, const LaunchConfig& lc, bool chunk_graph = true);
+    // groups' graphs instead and passes false; advance() then captures it on first use).
+    // pregen_ok: a small FP64 ensemble with in-kernel noise may pregenerate each chunk's
+    // increments (pregen_wanted); the server's groups and the autotuner's probes pass false.
+    Ensemble(sp_context* c, const sp_ensemble_desc& d, const LaunchConfig& lc, bool chunk_graph = true,
+             bool pregen_ok = true);
     ~Ensemble();
     Ensemble(const Ensemble&) = delete;
     Ensemble& operator=(const Ensemble&) = delete;

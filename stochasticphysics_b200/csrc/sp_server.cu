@@ -213,7 +213,7 @@ struct sp_server {
             queue.pop_front();
             try {
                 r->t_admit0 = Clock::now();
-                r->ens = std::make_unique<Ensemble>(ctx, r->desc, launch_for(r->desc, &r->chunks_per_round), false);
+                r->ens = std::make_unique<Ensemble>(ctx, r->desc, launch_for(r->desc, &r->chunks_per_round), false, false);
                 r->t_admit1 = Clock::now();
                 r->ens->last_stream = nullptr;
                 // the ensemble holds its inputs on the device now: drop the host copies

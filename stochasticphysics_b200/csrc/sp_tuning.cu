@@ -90,7 +90,7 @@ namespace {
 // particle-steps/s of one shape on the probe: one warm-up chunk (first graph
 // launch, caches), then `timed` steps between CUDA events on the probe's stream
 double time_shape(sp_context* ctx, const sp_ensemble_desc& probe, const LaunchConfig& lc, unsigned long long timed) {
-    Ensemble e(ctx, probe, lc);
+    Ensemble e(ctx, probe, lc, true, false);  // the in-kernel noise path the shape is tuned for
     e.advance(e.L.chunk, nullptr);
     e.synchronize();
     e.device_ms = 0.0;

@@ -99,7 +99,8 @@ struct EnsDev {
     void* slo;      // FP32 form: [D][Np] carried rounding errors of the state (nullptr in FP64)
     const void* params;
     const double* moment;
-    const void* dw;
+    void* dw;       // Wiener increments [rows][Mn][Np]: injected (every step) or pregenerated
+    int dw_chunk;   // 1: dw holds only the current chunk's increments (row 0 = its first step)
     double* partial;
     double* msum;   // [K][OUT] weighted ensemble sums
     double* wsum;   // [OUT] summed weights
