@@ -963,7 +963,7 @@ def main():
         line = {
             "metric": METRIC, "value": v32, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": results["FP32"]["total_ms"] / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded, BASELINE config distributions)",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded, the stated distributions of each workload)",
             "config": config_dict(args),
             "fp64_plain": {"value": v64, "unit": UNIT, "ms_per_step": results["FP64"]["total_ms"] / args.steps,
                            "clocks": results["FP64"]["clocks"]},
