@@ -448,7 +448,7 @@ SP_API sp_status sp_launch_config_for(sp_context* ctx, const sp_ensemble_desc* d
  * chunk launch ends with its CTAs draining, and the SMs they free go to the other
  * ensembles' CTAs only when those have launches in flight, where a lone ensemble is
  * fastest with the longer chunk the autotuner picks.
- * Small FP64 ensembles with SP_NOISE_PHILOX (at most 4 x 32 particles per SM) draw each
+ * Small FP64 ensembles with SP_NOISE_PHILOX (at most 8 x 32 particles per SM) draw each
  * chunk's increments in a separate parallel kernel before the step kernel (the same
  * Philox stream, bit-identical results, about half the per-step latency); their chunk
  * is shortened where needed so that this buffer stays within 256 MB.  sp_simulate and

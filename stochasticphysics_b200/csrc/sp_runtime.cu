@@ -188,12 +188,12 @@ void* Ensemble::dalloc(size_t bytes) {
 // Pregenerated noise.  A small ensemble leaves most SMs idle and each step's time is the
 // latency of one thread's step chain, of which the FP64 Philox draw and Box-Muller (double
 // log, sqrt and sincospi) are about half (Neel Heun, 1024 particles: 0.94 us per step with
-// in-kernel noise, 0.43 with the increments read from memory).  With at most one warp per
+// in-kernel noise, 0.43 with the increments read from memory).  With at most two warps per
 // SM scheduler, an FP64 ensemble with in-kernel noise therefore draws each chunk's
 // increments in a separate, fully parallel kernel (the same Philox counters and
 // arithmetic, so the results are bit-identical) into a chunk-sized buffer that the
 // injected step kernel stages like caller-supplied increments.
-constexpr unsigned long long kPregenWarpsPerSM = 4;
+constexpr unsigned long long kPregenWarpsPerSM = 8;  // measured crossover: between 7 and 10
 constexpr unsigned long long kPregenBytes = 256ull << 20;  // cap on the chunk's increments buffer
 
 static bool pregen_wanted(const sp_context* ctx, const sp_ensemble_desc& d) {

@@ -42,12 +42,12 @@ def test_pregenerated_noise_equals_in_kernel_noise(ctx, problem, solver):
 
 
 def test_only_small_ensembles_pregenerate(ctx):
-    """Up to four warps per SM, one per scheduler (4 x 32 x SMs particles), the ensemble
+    """Up to eight warps per SM, two per scheduler (8 x 32 x SMs particles), the ensemble
     runs one noise launch more per chunk; above it draws in the kernel.  Same kernel key, so the
     same chunk length for both sizes."""
     sms = 148
     small = small_spec(Problem.Neel, Solver.Heun_Strong, n=1000, steps=4000, W=200, seed=6)
-    large = small_spec(Problem.Neel, Solver.Heun_Strong, n=4 * 32 * sms + 32, steps=4000, W=200, seed=6)
+    large = small_spec(Problem.Neel, Solver.Heun_Strong, n=8 * 32 * sms + 32, steps=4000, W=200, seed=6)
     chunk = min(ctx.launch_config(small)["chunk_steps"], small.integrated_steps)
     chunks = -(-small.integrated_steps // chunk)
     a = ctx.simulate(small)
