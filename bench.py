@@ -890,7 +890,11 @@ def main():
         # awaited, so its upload and set-up overlap the rounds still running (every step
         # still uploads its inputs from host memory and reads its results back)
         with sp.Server(ctx) as srv:
-            for i in srv.submit_many(e2e_specs):
+            # warm-up in the timed pattern (two pairs in flight), so the server's groups
+            # and their streams exist before the clock starts
+            first = srv.submit_many(e2e_specs)
+            second = srv.submit_many(e2e_specs)
+            for i in first + second:
                 srv.wait(i)
             if world > 1:
                 dist.barrier()
