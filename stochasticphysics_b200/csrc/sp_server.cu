@@ -169,8 +169,8 @@ struct sp_server {
     }
 
     // The group a newly admitted request of kernel key `key` joins: an idle group of that
-    // key (its next round starts at once); else, while the key has fewer than
-    // kGroupsPerKey groups, a group of its own (an idle empty group or a new one), so a
+    // key (its next round starts at once); else, while the key has fewer running groups
+    // than the cap, a group of its own (an idle empty group or a new one), so a
     // request arriving while its key's group is mid-round starts at once instead of
     // waiting for that round to end; else the key's running group with the fewest members,
     // joining at its next round.  The cap (sp_server_config.groups_per_kind, default
