@@ -305,16 +305,18 @@ struct WindowSum<float, OUT> {
 //
 // Resident CTAs of kMaxBlock threads the compiler must allow per SM (0: its own choice,
 // as without the bound; an explicit 1 lets it take up to 255 registers, which made the
-// FP32 kernels 25 % slower at 163-167 registers instead of 128).  The FP64 Brown+Neel
-// explicit steps use about 230-255 registers left alone (8 warps per SM, whose FP64
+// FP32 kernels 25 % slower at 163-167 registers instead of 128).  The FP64 explicit steps
+// of Brown+Neel Euler/spherical use about 230-255 registers left alone (8 warps per SM, whose FP64
 // dependency chains leave the issue slots idle: the leading stall is `wait`); held to 128
 // registers they spill some state to local memory, which L1 serves, and run 16 warps per
 // SM: 25-31 % more particle-steps/s for an ensemble that fills the GPU (FP64 Millstein,
 // 262144 particles: 9.2e9 against 7.0e9; caps of 96, 112, 144 and 200 registers were
-// slower).  Register allocation does not change the arithmetic.
+// slower).  The Brown+Neel Cartesian ones (168-182 registers left alone) gain 12-22 % the
+// same way (Heun, 262144 particles: 2.43e10 against 2.13e10); the Neel kernels need no more
+// than 128 registers anyway.  Register allocation does not change the arithmetic.
 template <int PROB, class R, int SOLVER, bool INJECT, int PPT>
 constexpr int step_min_blocks() {
-    return (PROB == kBrownNeelEuler && sizeof(R) == 8 && !INJECT && PPT == 1 &&
+    return (sizeof(R) == 8 && !INJECT && PPT == 1 &&
             (SOLVER == kEulerMaruyama || SOLVER == kHeun || SOLVER == kMillstein || SOLVER == kEulerMaruyamaNormalized))
                ? 2
                : 0;
