@@ -313,11 +313,15 @@ struct WindowSum<float, OUT> {
 // 262144 particles: 9.2e9 against 7.0e9; caps of 96, 112, 144 and 200 registers were
 // slower).  The Brown+Neel Cartesian ones (168-182 registers left alone) gain 12-22 % the
 // same way (Heun, 262144 particles: 2.43e10 against 2.13e10); the Neel kernels need no more
-// than 128 registers anyway.  Register allocation does not change the arithmetic.
+// than 128 registers anyway.  Of the implicit-midpoint kernels (222-235 registers left
+// alone) the exact-Jacobian one gains 16 % (cubic Neel, 262144 particles: 6.13e9 against
+// 5.27e9) and the reference-matrix one, whose 20 Newton iterations spill more, loses 5 %,
+// so only the former is bound.  Register allocation does not change the arithmetic.
 template <int PROB, class R, int SOLVER, bool INJECT, int PPT>
 constexpr int step_min_blocks() {
     return (sizeof(R) == 8 && !INJECT && PPT == 1 &&
-            (SOLVER == kEulerMaruyama || SOLVER == kHeun || SOLVER == kMillstein || SOLVER == kEulerMaruyamaNormalized))
+            (SOLVER == kEulerMaruyama || SOLVER == kHeun || SOLVER == kMillstein || SOLVER == kEulerMaruyamaNormalized ||
+             SOLVER == kImplicitMidpointExact))
                ? 2
                : 0;
 }
